@@ -1,0 +1,261 @@
+"""hfmm_b200 -- Helmholtz KIFMM evaluate path on B200 (sm_100a).
+
+Drop-in for the reference's Python API (HFMM.py:55-91):
+
+    state = setup(positions, k, p=4, N_max=16, max_depth=None)
+    phi = evaluate(state, charges)            # real charges -> complex128 (N,)
+
+plus the complex-charge / field form the reference reaches only by combining
+four real evaluates (``kifmm.evaluate_setup(..., field=True)``,
+kifmm/setup.py:229-261):
+
+    phi, E = evaluate_field(state, charges)   # complex charges; E = -grad(phi), (N, 3)
+
+Positions, charges and results may be NumPy arrays or torch tensors; NumPy in,
+NumPy out. The tree, the interaction lists and every evaluate phase run as CUDA
+kernels of the in-tree library ``_lib/libhfmm_b200.so``; there is no CPU path.
+"""
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import check as _check, HFMMError, launch_count
+from .operators import level_tables, surface_pts, R_EQUIV, R_CHECK, n_surf
+
+__all__ = ["setup", "evaluate", "evaluate_field", "evaluate_into", "direct", "HFMMState",
+           "HFMMError", "launch_count", "PREC_FP64", "PREC_MIXED"]
+
+PREC_FP64 = _lib.HFMM_PREC_FP64
+PREC_MIXED = _lib.HFMM_PREC_MIXED
+
+
+def _device(device):
+    if device is None:
+        if not torch.cuda.is_available():
+            raise RuntimeError("hfmm_b200 needs a CUDA device (no CPU fallback)")
+        return torch.device("cuda", torch.cuda.current_device())
+    return torch.device(device)
+
+
+class HFMMState:
+    """A built plan: the octree, lists, operator tables and evaluate buffers on one GPU.
+
+    Plays the role of the reference's ``(real_state, imag_state)`` tuple
+    (HFMM.py:65-80). ``info`` holds the sizes the reference's setup dict reports
+    (max_depth, maxleaf, max_boxes, domain_extent, list lengths).
+    """
+
+    def __init__(self, handle, positions, k, p, N_max, device):
+        self._h = handle
+        self.positions = positions          # (N, 3) float64 on the device
+        self.n = positions.shape[0]
+        self.k = float(k)
+        self.p = int(p)
+        self.N_max = int(N_max)
+        self.device = device
+        self.n_families = 1 if self.k == 0 else 2
+        self._refresh()
+
+    def _refresh(self):
+        info = _lib.HfmmInfo()
+        _check(_lib.lib.hfmm_plan_info(self._h, info))
+        self.info = info.as_dict()
+        self.max_depth = self.info["max_depth"]
+
+    @property
+    def handle(self):
+        if self._h is None:
+            raise RuntimeError("HFMMState was closed")
+        return self._h
+
+    def close(self):
+        if getattr(self, "_h", None) is not None:
+            _lib.lib.hfmm_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---- inspection (tests) ----
+    def tree(self):
+        """Tree arrays of the active boxes, as NumPy (the build_fmm_tree outputs)."""
+        nb, n = self.info["n_boxes"], self.n
+        out = dict(m_id=np.empty(nb, np.uint64), p_id=np.empty(nb, np.int32),
+                   lvls=np.empty(nb, np.int32), counts=np.empty(nb, np.int32),
+                   is_leaf=np.empty(nb, np.uint8), sort_idx=np.empty(n, np.int32))
+        _check(_lib.lib.hfmm_export_tree(self.handle, *(out[k].ctypes.data for k in
+                                                         ("m_id", "p_id", "lvls", "counts",
+                                                          "is_leaf", "sort_idx"))))
+        out["is_leaf"] = out["is_leaf"].astype(bool)
+        return out
+
+    def pil(self):
+        nb, w = self.info["n_boxes"], self.info["maxleaf"]
+        out = np.empty((nb, w), np.int32)
+        _check(_lib.lib.hfmm_export_pil(self.handle, out.ctypes.data))
+        return out
+
+    def pairs(self, which):
+        """Interaction list as (len, 2) int32: 'V', 'U', 'W', 'X' or 'near'."""
+        idx = {"V": 0, "U": 1, "W": 2, "X": 3, "near": 4}[which]
+        n = self.info[{"V": "n_v", "U": "n_u", "W": "n_w", "X": "n_x", "near": "n_near"}[which]]
+        out = np.empty((max(n, 1), 2), np.int32)
+        _check(_lib.lib.hfmm_export_list(self.handle, idx, out.ctypes.data, max(n, 1)))
+        return out[:n]
+
+
+def _validate_setup(positions, k, p, N_max, max_depth):
+    """HFMM.py:14-16 and 57-64."""
+    if isinstance(positions, torch.Tensor):
+        x = positions.detach().to(torch.float64)
+        ok_shape = x.ndim == 2 and x.shape[1] == 3 and x.shape[0] > 0
+        if not ok_shape or not bool(torch.isfinite(x).all()):
+            raise ValueError("positions must be a nonempty finite (N,3) array")
+    else:
+        x = np.asarray(positions, dtype=np.float64)
+        if x.ndim != 2 or x.shape[1] != 3 or len(x) == 0 or not np.isfinite(x).all():
+            raise ValueError("positions must be a nonempty finite (N,3) array")
+    if p < 2 or int(p) != p or N_max < 1 or int(N_max) != N_max:
+        raise ValueError("p must be an integer >=2; N_max must be a positive integer")
+    if max_depth is not None and (max_depth < 1 or int(max_depth) != max_depth):
+        raise ValueError("max_depth must be a positive integer or None")
+    kf = float(k)
+    if not np.isfinite(kf):
+        raise ValueError("k must be a finite real number")
+    return x, kf
+
+
+def setup(positions, k, p=4, N_max=16, max_depth=None, device=None):
+    """Build the plan for ``positions`` and wavenumber ``k`` (HFMM.setup, HFMM.py:55-80).
+
+    ``p`` is the number of surface points per cube edge, ``N_max`` the leaf
+    size and ``max_depth`` an optional depth cap (``None``: the reference's
+    automatic depth with refinement, trees/cubic.py:577-600).
+    """
+    x, kf = _validate_setup(positions, k, p, N_max, max_depth)
+    dev = _device(device)
+    with torch.cuda.device(dev):
+        pos = torch.as_tensor(x, dtype=torch.float64).to(dev).contiguous()
+        h = _lib.ctypes.c_void_p()
+        _check(_lib.lib.hfmm_tree_build(pos.data_ptr(), pos.shape[0], int(N_max),
+                                        int(max_depth) if max_depth is not None else 0,
+                                        _lib.ctypes.byref(h)))
+        state = HFMMState(h.value, pos, kf, p, N_max, dev)
+        try:
+            _load_tables(state)
+            _check(_lib.lib.hfmm_plan_finalize(state.handle))
+        except Exception:
+            state.close()
+            raise
+        state._refresh()
+    return state
+
+
+def _load_tables(state):
+    p, md = state.p, state.max_depth
+    extent = state.info["domain_extent"]
+    eq = np.ascontiguousarray(surface_pts(p, R_EQUIV))
+    ch = np.ascontiguousarray(surface_pts(p, R_CHECK))
+    _check(_lib.lib.hfmm_plan_set_kernel(state.handle, state.k, p, state.n_families,
+                                         eq.ctypes.data, ch.ctypes.data))
+    for fam in range(state.n_families):
+        eps_rel = 1e-7 if fam == 0 else 1e-12          # HFMM.py:75-77
+        for level in range(2, md + 1):
+            t = level_tables(p, level, md, extent, state.k, fam == 1, eps_rel)
+            arrs = [t["F_up"][0], t["F_up"][1], t["F_up"][2], t["F_dn"][0], t["F_dn"][1],
+                    t["F_dn"][2], t["M2M_K"], t["L2L_K"], t["M2L_K"]]
+            arrs = [None if a is None else np.ascontiguousarray(a, dtype=np.float64) for a in arrs]
+            ptrs = [None if a is None else a.ctypes.data for a in arrs]
+            _check(_lib.lib.hfmm_plan_set_level(state.handle, fam, level, *ptrs))
+            del arrs, t
+
+
+def _as_device_f64(a, dev):
+    if isinstance(a, torch.Tensor):
+        return a.detach().to(device=dev, dtype=torch.float64).contiguous()
+    return torch.as_tensor(np.ascontiguousarray(a, dtype=np.float64)).to(dev)
+
+
+def evaluate_into(state, q_re, q_im, phi_out, field_out=None, precision=PREC_FP64, stream=None):
+    """Allocation-free evaluate on device tensors (float64 charges, complex128 outputs).
+
+    ``q_im`` may be None (real charges). ``stream`` is a torch.cuda.Stream or
+    None (the current stream). Asynchronous; call ``check_errors`` to read the
+    device error flag.
+    """
+    s = stream if stream is not None else torch.cuda.current_stream(state.device)
+    _check(_lib.lib.hfmm_evaluate(
+        state.handle, q_re.data_ptr(), None if q_im is None else q_im.data_ptr(),
+        phi_out.data_ptr(), None if field_out is None else field_out.data_ptr(),
+        int(precision), s.cuda_stream))
+
+
+def check_errors(state, stream=None):
+    s = stream if stream is not None else torch.cuda.current_stream(state.device)
+    _check(_lib.lib.hfmm_plan_check(state.handle, s.cuda_stream))
+
+
+def _run(state, charges, complex_ok, field, precision):
+    numpy_in = not isinstance(charges, torch.Tensor)
+    if numpy_in:
+        q = np.asarray(charges)
+        is_cplx = np.iscomplexobj(q)
+    else:
+        q = charges
+        is_cplx = q.is_complex()
+    if tuple(q.shape) != (state.n,) or (is_cplx and not complex_ok):
+        raise ValueError("charges must be a real array of shape (N,)")
+    dev = state.device
+    with torch.cuda.device(dev):
+        if is_cplx:
+            qt = torch.as_tensor(q).to(dev) if numpy_in else q.detach().to(dev)
+            q_re = qt.real.to(torch.float64).contiguous()
+            q_im = qt.imag.to(torch.float64).contiguous()
+        else:
+            q_re = _as_device_f64(q, dev)
+            q_im = None
+        phi = torch.empty(state.n, dtype=torch.complex128, device=dev)
+        E = torch.empty((state.n, 3), dtype=torch.complex128, device=dev) if field else None
+        evaluate_into(state, q_re, q_im, phi, E, precision)
+        check_errors(state)
+    if numpy_in:
+        phi = phi.cpu().numpy()
+        E = E.cpu().numpy() if E is not None else None
+    return (phi, E) if field else phi
+
+
+def evaluate(state, charges, precision=PREC_FP64):
+    """HFMM.evaluate (HFMM.py:83-91): real charges (N,) -> complex128 potential (N,)
+    in the input point order; complex charges raise ValueError."""
+    return _run(state, charges, complex_ok=False, field=False, precision=precision)
+
+
+def evaluate_field(state, charges, precision=PREC_FP64):
+    """Potential and field E = -grad(phi) for real or complex charges (N,).
+    Returns (phi (N,), E (N, 3)), both complex128."""
+    return _run(state, charges, complex_ok=True, field=True, precision=precision)
+
+
+def direct(state, charges, targets, field=False):
+    """GPU direct sum sum_{s: r>0} q_s e^{ikr}/r (and -grad) at ``targets`` (indices),
+    the referee of test.py:11-18. Returns NumPy complex arrays."""
+    dev = state.device
+    with torch.cuda.device(dev):
+        q = torch.as_tensor(np.asarray(charges)).to(dev) if not isinstance(charges, torch.Tensor) \
+            else charges.to(dev)
+        q_re = q.real.to(torch.float64).contiguous() if q.is_complex() else q.to(torch.float64).contiguous()
+        q_im = q.imag.to(torch.float64).contiguous() if q.is_complex() else None
+        tg = torch.as_tensor(np.asarray(targets, dtype=np.int32)).to(dev)
+        phi = torch.empty(tg.shape[0], dtype=torch.complex128, device=dev)
+        E = torch.empty((tg.shape[0], 3), dtype=torch.complex128, device=dev) if field else None
+        s = torch.cuda.current_stream(dev)
+        _check(_lib.lib.hfmm_direct(state.positions.data_ptr(), q_re.data_ptr(),
+                                    None if q_im is None else q_im.data_ptr(), state.n,
+                                    tg.data_ptr(), tg.shape[0], state.k, phi.data_ptr(),
+                                    None if E is None else E.data_ptr(), s.cuda_stream))
+        phi = phi.cpu().numpy()
+        E = E.cpu().numpy() if E is not None else None
+    return (phi, E) if field else phi

@@ -1,0 +1,96 @@
+"""ctypes binding of the hfmm_b200 C ABI (include/hfmm_b200.h).
+
+The shared library is built in-tree by ``hfmm_b200.build``. There is no CPU or
+pure-Python fallback: if the library is missing or fails to load, importing
+this module raises.
+"""
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_lib", "libhfmm_b200.so")
+
+HFMM_OK = 0
+HFMM_PREC_FP64 = 0
+HFMM_PREC_MIXED = 1
+
+_c_i32, _c_i64, _c_dbl, _c_vp = ctypes.c_int32, ctypes.c_int64, ctypes.c_double, ctypes.c_void_p
+
+
+class HfmmInfo(ctypes.Structure):
+    _fields_ = [
+        ("n_points", _c_i64), ("max_depth", _c_i32), ("maxleaf", _c_i32),
+        ("max_boxes", _c_i64), ("n_boxes", _c_i64), ("n_leaves", _c_i64),
+        ("adaptive", _c_i32), ("level_lo", _c_i32 * 16), ("level_hi", _c_i32 * 16),
+        ("domain_extent", _c_dbl), ("pmin", _c_dbl * 3),
+        ("n_v", _c_i64), ("n_u", _c_i64), ("n_w", _c_i64), ("n_x", _c_i64), ("n_near", _c_i64),
+        ("n_s", _c_i32), ("p", _c_i32),
+    ]
+
+    def as_dict(self):
+        md = self.max_depth
+        return dict(
+            n_points=self.n_points, max_depth=md, maxleaf=self.maxleaf,
+            max_boxes=self.max_boxes, n_boxes=self.n_boxes, n_leaves=self.n_leaves,
+            adaptive=bool(self.adaptive),
+            level_ranges={l: (self.level_lo[l], self.level_hi[l]) for l in range(1, md + 1)},
+            domain_extent=self.domain_extent, pmin=tuple(self.pmin),
+            n_v=self.n_v, n_u=self.n_u, n_w=self.n_w, n_x=self.n_x, n_near=self.n_near,
+            n_s=self.n_s, p=self.p)
+
+
+# (name, restype, argtypes) for every symbol of include/hfmm_b200.h
+SIGNATURES = [
+    ("hfmm_tree_build", _c_i32, [_c_vp, _c_i64, _c_i32, _c_i32, ctypes.POINTER(_c_vp)]),
+    ("hfmm_plan_info", _c_i32, [_c_vp, ctypes.POINTER(HfmmInfo)]),
+    ("hfmm_plan_set_kernel", _c_i32, [_c_vp, _c_dbl, _c_i32, _c_i32, _c_vp, _c_vp]),
+    ("hfmm_plan_set_level", _c_i32, [_c_vp, _c_i32, _c_i32] + [_c_vp] * 9),
+    ("hfmm_plan_finalize", _c_i32, [_c_vp]),
+    ("hfmm_evaluate", _c_i32, [_c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_i32, _c_vp]),
+    ("hfmm_plan_check", _c_i32, [_c_vp, _c_vp]),
+    ("hfmm_plan_destroy", None, [_c_vp]),
+    ("hfmm_export_tree", _c_i32, [_c_vp] * 7),
+    ("hfmm_export_pil", _c_i32, [_c_vp, _c_vp]),
+    ("hfmm_export_list", _c_i32, [_c_vp, _c_i32, _c_vp, _c_i64]),
+    ("hfmm_direct", _c_i32, [_c_vp, _c_vp, _c_vp, _c_i64, _c_vp, _c_i64, _c_dbl, _c_vp, _c_vp,
+                             _c_vp]),
+    ("hfmm_last_error", ctypes.c_char_p, []),
+    ("hfmm_launch_count", _c_i64, []),
+]
+
+
+class HFMMError(RuntimeError):
+    """A C-ABI call returned a non-zero status."""
+
+    def __init__(self, code, msg):
+        super().__init__(f"hfmm_b200 error {code}: {msg}")
+        self.code = code
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(
+            f"hfmm_b200: CUDA library not built ({LIB_PATH} missing); run "
+            "`python -m hfmm_b200.build` (there is no CPU fallback)")
+    lib = ctypes.CDLL(LIB_PATH)
+    for name, res, args in SIGNATURES:
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+lib = _load()
+
+
+def check(code):
+    """Raise HFMMError (or ValueError for argument errors) on a non-zero status."""
+    if code != HFMM_OK:
+        msg = lib.hfmm_last_error().decode(errors="replace")
+        if code == -1:
+            raise ValueError(msg)
+        raise HFMMError(code, msg)
+
+
+def launch_count():
+    return int(lib.hfmm_launch_count())

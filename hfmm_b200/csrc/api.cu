@@ -1,0 +1,633 @@
+// C ABI of hfmm_b200 (include/hfmm_b200.h): plan life cycle, operator-table
+// upload, schedules and the evaluate driver.
+//
+// The evaluate driver follows core.evaluate (jaxfmm/core.py:274-335) with the
+// leveled KIFMM closures (kifmm/assemble.py:15-89):
+//   S2M  P2M check potentials + level decode          (phases.py:79-125)
+//   M2M  child -> parent check + decode, bottom-up     (phases.py:128-173)
+//   M2L  V-list check, fused with P2L and L2L, decode  (phases.py:176-280, 1709-1770)
+//   L2P  + near field P2P + W-list M2P                 (phases.py:1533-1582, near.py:48-312,
+//                                                        phases.py:1064-1140)
+// Both Helmholtz components (cos, sin) and the R charge columns run together.
+// Levels 0 and 1 carry no far-field work: V, W and X pairs start at level 2, so
+// their equivalent and local densities are never read.
+#include "hfmm_internal.cuh"
+#include "particles.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+
+namespace hfmm {
+
+std::atomic<int64_t> g_launches{0};
+static thread_local std::string t_last_error;
+
+void set_error(int code, const std::string& msg) {
+    (void)code;
+    t_last_error = msg;
+}
+int fail(int code, const std::string& msg) {
+    set_error(code, msg);
+    return code;
+}
+
+namespace {
+
+// dst[c][k][m] = (transpose ? src[map[c]][m][k] : src[map[c]][k][m]), zero padded to ld
+__global__ void k_relayout(const double* __restrict__ src, const int32_t* __restrict__ map,
+                           int count, int n_s, int ld, int transpose, double* dst) {
+    __shared__ double tile[32][33];
+    const int c = blockIdx.z;
+    const int sc = map ? map[c] : c;
+    const int bx = blockIdx.x * 32, by = blockIdx.y * 32;   // bx: m (dst column), by: k (dst row)
+    const double* S = src + (int64_t)sc * n_s * n_s;
+    double* D = dst + (int64_t)c * ld * ld;
+    if (!transpose) {
+        for (int yy = threadIdx.y; yy < 32; yy += blockDim.y) {
+            int k = by + yy, m = bx + threadIdx.x;
+            tile[yy][threadIdx.x] = (k < n_s && m < n_s) ? S[(int64_t)k * n_s + m] : 0.0;
+        }
+    } else {
+        // read S[m][k] coalesced along k: rows m = bx + yy, cols k = by + tx
+        for (int yy = threadIdx.y; yy < 32; yy += blockDim.y) {
+            int m = bx + yy, k = by + threadIdx.x;
+            tile[threadIdx.x][yy] = (m < n_s && k < n_s) ? S[(int64_t)m * n_s + k] : 0.0;
+        }
+    }
+    __syncthreads();
+    for (int yy = threadIdx.y; yy < 32; yy += blockDim.y) {
+        int k = by + yy, m = bx + threadIdx.x;
+        if (k < ld && m < ld) D[(int64_t)k * ld + m] = tile[yy][threadIdx.x];
+    }
+}
+
+void relayout(const double* h_src, int src_count, const std::vector<int32_t>& map, int n_s,
+              int ld, bool transpose, DevBuf<double>& dst) {
+    int count = map.empty() ? src_count : (int)map.size();
+    dst.alloc((size_t)count * ld * ld);
+    DevBuf<double> staging;
+    staging.alloc((size_t)src_count * n_s * n_s);
+    HFMM_CUDA(cudaMemcpy(staging.p, h_src, (size_t)src_count * n_s * n_s * sizeof(double),
+                         cudaMemcpyHostToDevice));
+    DevBuf<int32_t> dmap;
+    if (!map.empty()) {
+        dmap.alloc(map.size());
+        HFMM_CUDA(cudaMemcpy(dmap.p, map.data(), map.size() * 4, cudaMemcpyHostToDevice));
+    }
+    dim3 grid((unsigned)ceil_div(ld, 32), (unsigned)ceil_div(ld, 32), (unsigned)count);
+    HFMM_LAUNCH(k_relayout, grid, dim3(32, 8), 0, 0, staging.p, map.empty() ? nullptr : dmap.p,
+                count, n_s, ld, transpose ? 1 : 0, dst.p);
+    HFMM_CUDA(cudaDeviceSynchronize());
+}
+
+void upload_vec(const double* h, int n_s, int ld, DevBuf<double>& dst) {
+    std::vector<double> v(ld, 0.0);
+    std::memcpy(v.data(), h, n_s * sizeof(double));
+    dst.alloc(ld);
+    HFMM_CUDA(cudaMemcpy(dst.p, v.data(), ld * sizeof(double), cudaMemcpyHostToDevice));
+}
+
+std::vector<int32_t> nonadjacent_map() {
+    std::vector<int32_t> m;
+    for (int d = 0; d < N_DISP; ++d) {
+        int dx = d / 49 - 3, dy = (d / 7) % 7 - 3, dz = d % 7 - 3;
+        if (std::max(std::abs(dx), std::max(std::abs(dy), std::abs(dz))) > 1) m.push_back(d);
+    }
+    return m;
+}
+
+// A-pointer sets of the GEMM calls: kind 0..3 decode (up U, up Vt, dn U, dn Vt),
+// kind 4 M2M (8 entries), kind 5 downward M2L+L2L (351 entries); per level, families adjacent.
+enum { K_UPU, K_UPV, K_DNU, K_DNV, K_M2M, K_DN, K_COUNT };
+const int k_entries[K_COUNT] = {1, 1, 1, 1, 8, M2L_ENTRIES};
+
+struct PtrIndex {
+    size_t off[K_COUNT][MAX_LEVELS];
+};
+
+void build_a_ptrs(hfmm_plan* P, PtrIndex& ix) {
+    std::vector<const double*> h;
+    const size_t mat = (size_t)P->ld * P->ld;
+    auto madj = nonadjacent_map();
+    std::vector<int32_t> compact(N_DISP, -1);
+    for (size_t i = 0; i < madj.size(); ++i) compact[madj[i]] = (int32_t)i;
+    for (int kind = 0; kind < K_COUNT; ++kind)
+        for (int l = 0; l < MAX_LEVELS; ++l) {
+            ix.off[kind][l] = h.size();
+            if (l < 2 || l > P->md) continue;
+            for (int f = 0; f < P->n_fam; ++f) {
+                LevelTables& T = P->tables[f][l];
+                switch (kind) {
+                    case K_UPU: h.push_back(T.up_U.p); break;
+                    case K_UPV: h.push_back(T.up_Vt.p); break;
+                    case K_DNU: h.push_back(T.dn_U.p); break;
+                    case K_DNV: h.push_back(T.dn_Vt.p); break;
+                    case K_M2M:
+                        for (int o = 0; o < 8; ++o) h.push_back(T.m2m.p ? T.m2m.p + o * mat : nullptr);
+                        break;
+                    case K_DN:
+                        for (int d = 0; d < N_DISP; ++d)
+                            h.push_back(compact[d] >= 0 ? T.m2l.p + compact[d] * mat : nullptr);
+                        for (int o = 0; o < 8; ++o) h.push_back(T.l2l.p ? T.l2l.p + o * mat : nullptr);
+                        break;
+                }
+            }
+        }
+    P->h_a_ptrs = h;
+    P->a_ptrs.alloc(h.size());
+    HFMM_CUDA(cudaMemcpy(P->a_ptrs.p, h.data(), h.size() * sizeof(void*), cudaMemcpyHostToDevice));
+}
+
+EvalView view(hfmm_plan* P) {
+    EvalView v;
+    v.n = P->n;
+    v.nb = P->nb;
+    v.n_s = P->n_s;
+    v.ld = P->ld;
+    v.k = P->k;
+    v.pos_s = P->pos_s.p;
+    v.q_s = P->q_s.p;
+    v.leaf_start = P->leaf_start.p;
+    v.counts = P->counts.p;
+    v.lvls = P->lvls.p;
+    v.centre = P->centre.p;
+    v.hbox = P->hbox.p;
+    v.rmax = P->rmax.p;
+    return v;
+}
+
+struct PlanExtra {
+    PtrIndex ix;
+};
+
+std::mutex g_extra_mu;
+std::vector<std::pair<hfmm_plan*, PlanExtra*>> g_extra;
+
+PlanExtra* extra(hfmm_plan* P, bool create) {
+    std::lock_guard<std::mutex> g(g_extra_mu);
+    for (auto& e : g_extra)
+        if (e.first == P) return e.second;
+    if (!create) return nullptr;
+    g_extra.push_back({P, new PlanExtra()});
+    return g_extra.back().second;
+}
+
+void drop_extra(hfmm_plan* P) {
+    std::lock_guard<std::mutex> g(g_extra_mu);
+    for (size_t i = 0; i < g_extra.size(); ++i)
+        if (g_extra[i].first == P) {
+            delete g_extra[i].second;
+            g_extra.erase(g_extra.begin() + i);
+            return;
+        }
+}
+
+}  // namespace
+
+void upload_level(hfmm_plan* P, int fam, int l, const double* const* h) {
+    LevelTables& T = P->tables[fam][l];
+    const int n_s = P->n_s, ld = P->ld;
+    std::vector<int32_t> none;
+    relayout(h[0], 1, none, n_s, ld, false, T.up_U);   // A = U^T  -> A^T = U
+    upload_vec(h[1], n_s, ld, T.up_d);
+    relayout(h[2], 1, none, n_s, ld, false, T.up_Vt);  // A = Vt^T -> A^T = Vt
+    relayout(h[3], 1, none, n_s, ld, false, T.dn_U);
+    upload_vec(h[4], n_s, ld, T.dn_d);
+    relayout(h[5], 1, none, n_s, ld, false, T.dn_Vt);
+    if (h[6] && l < P->md) relayout(h[6], 8, none, n_s, ld, true, T.m2m);
+    else T.m2m.release();
+    if (h[7] && l >= 3) relayout(h[7], 8, none, n_s, ld, true, T.l2l);
+    else T.l2l.release();
+    relayout(h[8], N_DISP, nonadjacent_map(), n_s, ld, true, T.m2l);
+    T.set = true;
+}
+
+void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double* phi, double* E,
+                   cudaStream_t s) {
+    const int R = q_im ? 2 : 1;
+    const int NF = P->n_fam;
+    const bool field = E != nullptr;
+    PlanExtra* X = extra(P, false);
+    const int64_t fs = P->nb * (int64_t)R * P->ld;   // family stride of expansion arrays
+    gather_charges(P->n, P->sort_idx.p, q_re, q_im, P->q_s.p, s);
+    EvalView v = view(P);
+
+    ParticlePass base;
+    base.v = v;
+    base.nf = NF;
+    base.R = R;
+    base.field = field;
+    base.fam_stride = fs;
+    base.pot = P->pot.p;
+    base.fld = P->fld.p;
+
+    auto gemm = [&](int kind, int l, const hfmm_plan::Tiles& tiles, const int32_t* src_tab,
+                    int src_ld, const double* B0, const double* B1, double* out,
+                    const double* scale_set) {
+        GemmCall c{};
+        c.tile_tgt = tiles.tgt.p;
+        c.ntiles = tiles.ntiles;
+        c.src_tab = src_tab;
+        c.src_ld = src_ld;
+        c.n_entries = k_entries[kind];
+        c.b_split = kind == K_DN ? N_DISP : c.n_entries;
+        c.A = P->a_ptrs.p + X->ix.off[kind][l];
+        c.B0 = B0;
+        c.B1 = B1;
+        c.out = out;
+        c.scale = scale_set;
+        c.accumulate = 0;
+        c.R = R;
+        c.ld = P->ld;
+        c.n_s = P->n_s;
+        c.fam_stride = fs;
+        c.a_fam_stride = k_entries[kind];
+        c.n_fam = NF;
+        c.nb = P->nb;
+        gemm_f64(c, P->d_err.p, s);
+    };
+    // The decode scale vector differs per family: run the first decode step once per family.
+    auto decode = [&](int l, bool up, const double* in, double* out) {
+        const hfmm_plan::Tiles& tiles = P->dec_tiles[l][R - 1];
+        for (int f = 0; f < NF; ++f) {
+            GemmCall c{};
+            c.tile_tgt = tiles.tgt.p;
+            c.ntiles = tiles.ntiles;
+            c.src_tab = nullptr;
+            c.src_ld = 0;
+            c.n_entries = 1;
+            c.b_split = 1;
+            c.A = P->a_ptrs.p + X->ix.off[up ? K_UPU : K_DNU][l] + f;
+            c.B0 = in + f * fs;
+            c.B1 = nullptr;
+            c.out = P->tmp.p + f * fs;
+            c.scale = up ? P->tables[f][l].up_d.p : P->tables[f][l].dn_d.p;
+            c.accumulate = 0;
+            c.R = R;
+            c.ld = P->ld;
+            c.n_s = P->n_s;
+            c.fam_stride = 0;
+            c.a_fam_stride = 0;
+            c.n_fam = 1;
+            c.nb = P->nb;
+            gemm_f64(c, P->d_err.p, s);
+        }
+        gemm(up ? K_UPV : K_DNV, l, tiles, nullptr, 0, P->tmp.p, nullptr, out, nullptr);
+    };
+
+    // ---- upward pass
+    {
+        ParticlePass p = base;
+        p.op = ParticleOp::P2M;
+        p.rows = P->leaves.p;
+        p.nrows = P->n_leaves;
+        p.surf = P->check_pts.p;
+        p.out = P->check.p;
+        particles_f64(p, s);
+    }
+    for (int l = P->md; l >= 2; --l) {
+        if (l < P->md)
+            gemm(K_M2M, l, P->m2m_tiles[l][R - 1], P->m2m_src.p, 8, P->equiv.p, nullptr,
+                 P->check.p, nullptr);
+        decode(l, true, P->check.p, P->equiv.p);
+    }
+    // ---- downward pass (M2L + L2L in one GEMM, then X-list P2L, then decode)
+    for (int l = 2; l <= P->md; ++l) {
+        gemm(K_DN, l, P->dn_tiles[l][R - 1], P->m2l_src.p, M2L_ENTRIES, P->equiv.p, P->loc.p,
+             P->check.p, nullptr);
+        if (P->nX) {
+            ParticlePass p = base;
+            p.op = ParticleOp::P2L;
+            p.rows = P->x_tgt.p;
+            p.nrows = P->n_x_tgt;
+            p.off = P->x_off.p;
+            p.srcs = P->x_src.p;
+            p.surf = P->equiv_pts.p;
+            p.out = P->check.p;
+            p.level = l;
+            particles_f64(p, s);
+        }
+        decode(l, false, P->check.p, P->loc.p);
+    }
+    // ---- particle outputs: near field stores, far field and W list add
+    {
+        ParticlePass p = base;
+        p.op = ParticleOp::P2P;
+        p.rows = P->leaves.p;
+        p.nrows = P->n_leaves;
+        p.off = P->near_off.p;
+        p.srcs = P->near_src.p;
+        particles_f64(p, s);
+        p = base;
+        p.op = ParticleOp::L2P;
+        p.rows = P->leaves.p;
+        p.nrows = P->n_leaves;
+        p.surf = P->check_pts.p;
+        p.dens = P->loc.p;
+        particles_f64(p, s);
+        if (P->nW) {
+            p = base;
+            p.op = ParticleOp::M2P;
+            p.rows = P->w_tgt.p;
+            p.nrows = P->n_w_tgt;
+            p.off = P->w_off.p;
+            p.srcs = P->w_src.p;
+            p.surf = P->equiv_pts.p;
+            p.dens = P->equiv.p;
+            particles_f64(p, s);
+        }
+        p = base;
+        p.op = ParticleOp::COMBINE;
+        p.rows = P->sort_idx.p;
+        p.phi = phi;
+        p.E = E;
+        particles_f64(p, s);
+    }
+}
+
+}  // namespace hfmm
+
+using namespace hfmm;
+
+#define API_BEGIN try {
+#define API_END                                              \
+    }                                                        \
+    catch (const hfmm::Error& e) {                           \
+        return fail(e.code, e.msg);                          \
+    }                                                        \
+    catch (const std::exception& e) {                        \
+        return fail(HFMM_ERR_STATE, e.what());               \
+    }                                                        \
+    catch (...) {                                            \
+        return fail(HFMM_ERR_STATE, "unknown error");        \
+    }
+
+extern "C" {
+
+const char* hfmm_last_error(void) { return t_last_error.c_str(); }
+
+int64_t hfmm_launch_count(void) { return g_launches.load(); }
+
+int hfmm_tree_build(const double* pos_dev, int64_t n, int32_t n_max, int32_t max_depth,
+                    hfmm_plan** out) {
+    if (!out) return fail(HFMM_ERR_ARG, "out is NULL");
+    *out = nullptr;
+    if (!pos_dev || n <= 0) return fail(HFMM_ERR_ARG, "positions must be a nonempty (N,3) array");
+    if (n_max < 1) return fail(HFMM_ERR_ARG, "N_max must be a positive integer");
+    if (n > (int64_t)INT32_MAX) return fail(HFMM_ERR_CAPACITY, "more than 2^31-1 points");
+    hfmm_plan* P = new hfmm_plan();
+    API_BEGIN
+    HFMM_CUDA(cudaGetDevice(&P->device));
+    require_device_ptr(pos_dev, "positions");
+    P->n = n;
+    P->n_max = n_max;
+    P->md_given = max_depth > 0;
+    P->md = max_depth;
+    P->d_err.alloc(1);
+    P->d_err.zero();
+    tree_build(P, pos_dev);
+    *out = P;
+    return HFMM_OK;
+    }
+    catch (const hfmm::Error& e) {
+        delete P;
+        return fail(e.code, e.msg);
+    }
+    catch (...) {
+        delete P;
+        return fail(HFMM_ERR_STATE, "tree build failed");
+    }
+}
+
+int hfmm_plan_info(const hfmm_plan* P, hfmm_info* o) {
+    if (!P || !o) return fail(HFMM_ERR_ARG, "NULL argument");
+    std::memset(o, 0, sizeof(*o));
+    o->n_points = P->n;
+    o->max_depth = P->md;
+    o->maxleaf = P->maxleaf;
+    o->max_boxes = P->ref_max_boxes;
+    o->n_boxes = P->nb;
+    o->n_leaves = P->n_leaves;
+    o->adaptive = P->adaptive ? 1 : 0;
+    for (int l = 0; l < MAX_LEVELS; ++l) {
+        o->level_lo[l] = P->level_lo[l];
+        o->level_hi[l] = P->level_hi[l];
+    }
+    o->domain_extent = P->extent;
+    for (int a = 0; a < 3; ++a) o->pmin[a] = P->pmin[a];
+    o->n_v = P->nV;
+    o->n_u = P->nU;
+    o->n_w = P->nW;
+    o->n_x = P->nX;
+    o->n_near = P->nNear;
+    o->n_s = P->n_s;
+    o->p = P->p;
+    return HFMM_OK;
+}
+
+int hfmm_plan_set_kernel(hfmm_plan* P, double k, int32_t p, int32_t n_families,
+                         const double* equiv_pts, const double* check_pts) {
+    if (!P) return fail(HFMM_ERR_ARG, "plan is NULL");
+    if (!std::isfinite(k)) return fail(HFMM_ERR_ARG, "k must be a finite real number");
+    if (p < 2) return fail(HFMM_ERR_ARG, "p must be an integer >= 2");
+    if (n_families != 1 && n_families != 2) return fail(HFMM_ERR_ARG, "n_families must be 1 or 2");
+    if (!equiv_pts || !check_pts) return fail(HFMM_ERR_ARG, "surfaces are NULL");
+    API_BEGIN
+    P->k = k;
+    P->p = p;
+    P->n_s = 6 * p * p - 12 * p + 8;
+    P->ld = round_up(P->n_s, 16);
+    P->n_fam = n_families;
+    for (int f = 0; f < 2; ++f)
+        for (int l = 0; l < MAX_LEVELS; ++l) P->tables[f][l].reset();
+    std::vector<double> soa(3 * P->n_s);
+    for (int which = 0; which < 2; ++which) {
+        const double* src = which == 0 ? equiv_pts : check_pts;
+        for (int j = 0; j < P->n_s; ++j)
+            for (int a = 0; a < 3; ++a) soa[a * P->n_s + j] = src[j * 3 + a];
+        DevBuf<double>& d = which == 0 ? P->equiv_pts : P->check_pts;
+        d.alloc(soa.size());
+        HFMM_CUDA(cudaMemcpy(d.p, soa.data(), soa.size() * 8, cudaMemcpyHostToDevice));
+    }
+    P->finalized = false;
+    return HFMM_OK;
+    API_END
+}
+
+int hfmm_plan_set_level(hfmm_plan* P, int32_t family, int32_t level, const double* F_up_U,
+                        const double* F_up_d, const double* F_up_Vt, const double* F_dn_U,
+                        const double* F_dn_d, const double* F_dn_Vt, const double* M2M_K,
+                        const double* L2L_K, const double* M2L_K) {
+    if (!P) return fail(HFMM_ERR_ARG, "plan is NULL");
+    if (P->n_s == 0) return fail(HFMM_ERR_STATE, "set the kernel first");
+    if (family < 0 || family >= P->n_fam) return fail(HFMM_ERR_ARG, "family out of range");
+    if (level < 2 || level > P->md) return fail(HFMM_ERR_ARG, "level must be in [2, max_depth]");
+    if (!F_up_U || !F_up_d || !F_up_Vt || !F_dn_U || !F_dn_d || !F_dn_Vt || !M2L_K)
+        return fail(HFMM_ERR_ARG, "decode and M2L tables are required");
+    if (level < P->md && !M2M_K) return fail(HFMM_ERR_ARG, "M2M_K required below max_depth");
+    if (level >= 3 && !L2L_K) return fail(HFMM_ERR_ARG, "L2L_K required from level 3");
+    API_BEGIN
+    const double* h[9] = {F_up_U, F_up_d, F_up_Vt, F_dn_U, F_dn_d, F_dn_Vt, M2M_K, L2L_K, M2L_K};
+    upload_level(P, family, level, h);
+    P->finalized = false;
+    return HFMM_OK;
+    API_END
+}
+
+int hfmm_plan_finalize(hfmm_plan* P) {
+    if (!P) return fail(HFMM_ERR_ARG, "plan is NULL");
+    if (P->n_s == 0) return fail(HFMM_ERR_STATE, "set the kernel first");
+    for (int f = 0; f < P->n_fam; ++f)
+        for (int l = 2; l <= P->md; ++l)
+            if (!P->tables[f][l].set)
+                return fail(HFMM_ERR_STATE, "tables missing for family " + std::to_string(f) +
+                                                " level " + std::to_string(l));
+    API_BEGIN
+    if (!P->V.p) {
+        lists_build(P);
+        schedules_build(P);
+    }
+    PlanExtra* X = extra(P, true);
+    build_a_ptrs(P, X->ix);
+    const size_t exp = (size_t)P->n_fam * P->nb * 2 * P->ld;
+    P->check.alloc(exp);
+    P->equiv.alloc(exp);
+    P->loc.alloc(exp);
+    P->tmp.alloc(exp);
+    P->check.zero();
+    P->equiv.zero();
+    P->loc.zero();
+    P->tmp.zero();
+    P->q_s.alloc(2 * P->n);
+    P->pot.alloc((size_t)P->n_fam * 2 * P->n);
+    P->fld.alloc((size_t)P->n_fam * 2 * 3 * P->n);
+    HFMM_CUDA(cudaDeviceSynchronize());
+    P->finalized = true;
+    return HFMM_OK;
+    API_END
+}
+
+int hfmm_evaluate(hfmm_plan* P, const double* q_re, const double* q_im, double* phi, double* E,
+                  int32_t precision, void* stream) {
+    if (!P) return fail(HFMM_ERR_ARG, "plan is NULL");
+    if (!P->finalized) return fail(HFMM_ERR_STATE, "plan not finalized");
+    if (!q_re || !phi) return fail(HFMM_ERR_ARG, "charges and output are required");
+    if (precision != HFMM_PREC_FP64)
+        return fail(HFMM_ERR_ARG, "precision mode not available in this build");
+    API_BEGIN
+    require_device_ptr(q_re, "q_re");
+    if (q_im) require_device_ptr(q_im, "q_im");
+    require_device_ptr(phi, "phi_out");
+    if (E) require_device_ptr(E, "field_out");
+    evaluate_fp64(P, q_re, q_im, phi, E, (cudaStream_t)stream);
+    return HFMM_OK;
+    API_END
+}
+
+int hfmm_plan_check(hfmm_plan* P, void* stream) {
+    if (!P) return fail(HFMM_ERR_ARG, "plan is NULL");
+    API_BEGIN
+    int v = 0;
+    HFMM_CUDA(cudaMemcpyAsync(&v, P->d_err.p, sizeof(int), cudaMemcpyDeviceToHost,
+                              (cudaStream_t)stream));
+    HFMM_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
+    if (v) {
+        HFMM_CUDA(cudaMemsetAsync(P->d_err.p, 0, sizeof(int), (cudaStream_t)stream));
+        HFMM_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
+        return fail(HFMM_ERR_DEVICE, "device error flag " + std::to_string(v) +
+                                         " (1 = index out of bounds, 2 = capacity)");
+    }
+    return HFMM_OK;
+    API_END
+}
+
+void hfmm_plan_destroy(hfmm_plan* P) {
+    if (!P) return;
+    drop_extra(P);
+    delete P;
+}
+
+int hfmm_export_tree(const hfmm_plan* P, uint64_t* m_id, int32_t* p_id, int32_t* lvls,
+                     int32_t* counts, uint8_t* is_leaf, int32_t* sort_idx) {
+    if (!P) return fail(HFMM_ERR_ARG, "plan is NULL");
+    API_BEGIN
+    const int64_t nb = P->nb;
+    if (m_id) HFMM_CUDA(cudaMemcpy(m_id, P->m_id.p, nb * 8, cudaMemcpyDeviceToHost));
+    if (p_id) HFMM_CUDA(cudaMemcpy(p_id, P->p_id.p, nb * 4, cudaMemcpyDeviceToHost));
+    if (lvls) HFMM_CUDA(cudaMemcpy(lvls, P->lvls.p, nb * 4, cudaMemcpyDeviceToHost));
+    if (counts) HFMM_CUDA(cudaMemcpy(counts, P->counts.p, nb * 4, cudaMemcpyDeviceToHost));
+    if (is_leaf) HFMM_CUDA(cudaMemcpy(is_leaf, P->is_leaf.p, nb, cudaMemcpyDeviceToHost));
+    if (sort_idx) HFMM_CUDA(cudaMemcpy(sort_idx, P->sort_idx.p, P->n * 4, cudaMemcpyDeviceToHost));
+    return HFMM_OK;
+    API_END
+}
+
+int hfmm_export_pil(const hfmm_plan* P, int32_t* pil) {
+    if (!P || !pil) return fail(HFMM_ERR_ARG, "NULL argument");
+    API_BEGIN
+    std::vector<int32_t> ls(P->nb), sidx(P->n);
+    HFMM_CUDA(cudaMemcpy(ls.data(), P->leaf_start.p, P->nb * 4, cudaMemcpyDeviceToHost));
+    HFMM_CUDA(cudaMemcpy(sidx.data(), P->sort_idx.p, P->n * 4, cudaMemcpyDeviceToHost));
+    const int w = P->maxleaf;
+    for (int64_t b = 0; b < P->nb; ++b) {
+        int32_t* row = pil + b * w;
+        for (int j = 0; j < w; ++j) row[j] = -1;
+        if (ls[b] < 0) continue;
+        int c = std::min(P->h_counts[b], w);
+        for (int j = 0; j < c; ++j) row[j] = sidx[ls[b] + j];
+    }
+    return HFMM_OK;
+    API_END
+}
+
+int hfmm_export_list(const hfmm_plan* P, int32_t which, int32_t* pairs, int64_t cap) {
+    if (!P || !pairs) return fail(HFMM_ERR_ARG, "NULL argument");
+    API_BEGIN
+    const DevBuf<int32_t>* b;
+    int64_t len;
+    switch (which) {
+        case 0: b = &P->V; len = P->nV; break;
+        case 1: b = &P->U; len = P->nU; break;
+        case 2: b = &P->W; len = P->nW; break;
+        case 3: b = &P->X; len = P->nX; break;
+        case 4: b = &P->near; len = P->nNear; break;
+        default: return fail(HFMM_ERR_ARG, "which must be 0..4");
+    }
+    if (cap < len) return fail(HFMM_ERR_CAPACITY, "pairs buffer too small");
+    if (len) HFMM_CUDA(cudaMemcpy(pairs, b->p, len * 8, cudaMemcpyDeviceToHost));
+    return HFMM_OK;
+    API_END
+}
+
+int hfmm_direct(const double* pos, const double* q_re, const double* q_im, int64_t n,
+                const int32_t* targets, int64_t n_t, double k, double* phi, double* fld,
+                void* stream) {
+    if (!pos || !q_re || !targets || !phi || n <= 0 || n_t < 0)
+        return fail(HFMM_ERR_ARG, "invalid direct-sum arguments");
+    if (!std::isfinite(k)) return fail(HFMM_ERR_ARG, "k must be finite");
+    API_BEGIN
+    require_device_ptr(pos, "positions");
+    require_device_ptr(q_re, "q_re");
+    if (q_im) require_device_ptr(q_im, "q_im");
+    require_device_ptr(targets, "targets");
+    require_device_ptr(phi, "phi_out");
+    if (fld) require_device_ptr(fld, "field_out");
+    int splits = direct_splits(n, n_t);
+    DevBuf<double> scratch;
+    scratch.alloc((size_t)splits * std::max<int64_t>(n_t, 1) * 8);
+    DevBuf<int> err;
+    err.alloc(1);
+    err.zero((cudaStream_t)stream);
+    direct_sum(pos, q_re, q_im, n, targets, n_t, k, phi, fld, scratch.p, splits,
+               (cudaStream_t)stream, err.p);
+    int h = 0;
+    HFMM_CUDA(cudaMemcpyAsync(&h, err.p, sizeof(int), cudaMemcpyDeviceToHost, (cudaStream_t)stream));
+    HFMM_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
+    if (h) return fail(HFMM_ERR_ARG, "target index out of range");
+    return HFMM_OK;
+    API_END
+}
+
+}  // extern "C"

@@ -1,0 +1,124 @@
+// Direct-sum referee: phi_t = sum_{s: r > 0} q_s e^{ikr} / r at sampled targets
+// (test.py:11-18), and the field -grad phi = sum q_s e^{ikr} (1 - ikr) / r^3 (x_t - x_s).
+//
+// Sources are split into n_split contiguous chunks; each (target block, chunk)
+// CTA writes its partial sums to scratch, and a second kernel adds the chunks
+// in a fixed order, so the result does not depend on scheduling.
+#include "hfmm_internal.cuh"
+
+#include <algorithm>
+
+namespace hfmm {
+
+namespace {
+
+constexpr int DT = 128;        // targets per CTA
+constexpr int DSTAGE = 256;    // sources staged per pass
+constexpr int NV = 8;          // phi re/im + field 3 x re/im
+
+__global__ void __launch_bounds__(DT) k_direct_partial(const double* __restrict__ pos,
+                                                       const double* __restrict__ q_re,
+                                                       const double* __restrict__ q_im, int64_t n,
+                                                       const int32_t* __restrict__ tg, int64_t n_t,
+                                                       double k, int field, int n_split,
+                                                       double* scratch, int* err) {
+    __shared__ double sx[DSTAGE], sy[DSTAGE], sz[DSTAGE], sqr[DSTAGE], sqi[DSTAGE];
+    const int64_t ti = blockIdx.x * (int64_t)DT + threadIdx.x;
+    const int split = blockIdx.y;
+    const int64_t chunk = (n + n_split - 1) / n_split;
+    const int64_t lo = split * chunk, hi = (lo + chunk < n) ? lo + chunk : n;
+    bool act = ti < n_t;
+    double x = 0, y = 0, z = 0;
+    if (act) {
+        int64_t t = tg[ti];
+        if (t < 0 || t >= n) {
+            atomicOr(err, ERRF_BOUNDS);
+            act = false;
+        } else {
+            x = pos[3 * t];
+            y = pos[3 * t + 1];
+            z = pos[3 * t + 2];
+        }
+    }
+    double acc[NV] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (int64_t p0 = lo; p0 < hi; p0 += DSTAGE) {
+        __syncthreads();
+        for (int i = threadIdx.x; i < DSTAGE; i += DT) {
+            int64_t s = p0 + i;
+            if (s < hi) {
+                sx[i] = pos[3 * s];
+                sy[i] = pos[3 * s + 1];
+                sz[i] = pos[3 * s + 2];
+                sqr[i] = q_re[s];
+                sqi[i] = q_im ? q_im[s] : 0.0;
+            }
+        }
+        __syncthreads();
+        if (!act) continue;
+        const int np = (int)((hi - p0 < DSTAGE) ? hi - p0 : DSTAGE);
+        for (int i = 0; i < np; ++i) {
+            double dx = x - sx[i], dy = y - sy[i], dz = z - sz[i];
+            double r2 = dx * dx + dy * dy + dz * dz;
+            if (!(r2 > 0.0)) continue;
+            double r = sqrt(r2), ir = 1.0 / r;
+            double kr = k * r, sn, cs;
+            sincos(kr, &sn, &cs);
+            // w = e^{ikr}/r; q w
+            double wr = cs * ir, wi = sn * ir;
+            acc[0] += sqr[i] * wr - sqi[i] * wi;
+            acc[1] += sqr[i] * wi + sqi[i] * wr;
+            if (field) {
+                // e^{ikr}(1 - ikr)/r^3 = ((cs + kr sn) + i (sn - kr cs)) / r^3
+                double ir3 = ir * ir * ir;
+                double fr = (cs + kr * sn) * ir3, fi = (sn - kr * cs) * ir3;
+                double gr = sqr[i] * fr - sqi[i] * fi, gi = sqr[i] * fi + sqi[i] * fr;
+                acc[2] += gr * dx;
+                acc[3] += gi * dx;
+                acc[4] += gr * dy;
+                acc[5] += gi * dy;
+                acc[6] += gr * dz;
+                acc[7] += gi * dz;
+            }
+        }
+    }
+    if (act)
+        for (int v = 0; v < NV; ++v) scratch[((int64_t)split * n_t + ti) * NV + v] = acc[v];
+}
+
+__global__ void k_direct_reduce(const double* __restrict__ scratch, int64_t n_t, int n_split,
+                                int field, double* phi, double* fld) {
+    int64_t ti = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (ti >= n_t) return;
+    double acc[NV] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (int s = 0; s < n_split; ++s)
+        for (int v = 0; v < NV; ++v) acc[v] += scratch[((int64_t)s * n_t + ti) * NV + v];
+    phi[2 * ti] = acc[0];
+    phi[2 * ti + 1] = acc[1];
+    if (field && fld)
+        for (int a = 0; a < 3; ++a) {
+            fld[(ti * 3 + a) * 2] = acc[2 + 2 * a];
+            fld[(ti * 3 + a) * 2 + 1] = acc[3 + 2 * a];
+        }
+}
+
+}  // namespace
+
+int direct_splits(int64_t n, int64_t n_t) {
+    int64_t tblocks = ceil_div(std::max<int64_t>(n_t, 1), DT);
+    int64_t want = ceil_div(4 * 148, tblocks);                 // about 4 CTAs per SM
+    int64_t by_work = ceil_div(std::max<int64_t>(n, 1), 2048);  // at least 2048 sources a split
+    return (int)std::max<int64_t>(1, std::min<int64_t>(want, by_work));
+}
+
+void direct_sum(const double* pos, const double* q_re, const double* q_im, int64_t n,
+                const int32_t* targets, int64_t n_t, double k, double* phi, double* fld,
+                double* scratch, int n_split, cudaStream_t s, int* err) {
+    if (n_t == 0) return;
+    dim3 grid((unsigned)ceil_div(n_t, DT), (unsigned)n_split);
+    HFMM_LAUNCH(k_direct_partial, grid, DT, 0, s, pos, q_re, q_im, n, targets, n_t, k,
+                fld ? 1 : 0, n_split, scratch, err);
+    HFMM_LAUNCH(k_direct_reduce, (unsigned)ceil_div(n_t, 256), 256, 0, s, scratch, n_t, n_split,
+                fld ? 1 : 0, phi, fld);
+}
+
+}  // namespace hfmm

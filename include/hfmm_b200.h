@@ -1,0 +1,136 @@
+/*
+ * hfmm_b200 -- C ABI of the B200 Helmholtz KIFMM evaluate path.
+ *
+ * The reference (a JAX package) has no native boundary: its entry points are the
+ * Python functions HFMM.setup / HFMM.evaluate (HFMM.py:55-91) and, one layer
+ * down, kifmm.setup / kifmm.evaluate_setup (jaxfmm/kifmm/setup.py:19-261). This
+ * header is the C-ABI those Python entry points bind through ctypes (see
+ * hfmm_b200/_lib.py). Every function returns HFMM_OK (0) or a negative status;
+ * hfmm_last_error() gives the message of the calling thread's last failure.
+ * Pointers named *_dev are device pointers owned by the caller; the plan owns
+ * every buffer it allocates. No C++ exception crosses this boundary.
+ *
+ * Life cycle of a plan (mirrors HFMM.setup, HFMM.py:55-80):
+ *   hfmm_tree_build        tree + particle layout     (trees/cubic.py:316-695)
+ *   hfmm_plan_info         depth, extent, sizes       (kifmm/setup.py:220-226 keys)
+ *   hfmm_plan_set_level    per-level operator tables  (kifmm/operators.py:572-641)
+ *   hfmm_plan_finalize     interaction lists + schedules (trees/lists.py:818-931)
+ *   hfmm_evaluate          potential [+ field]        (HFMM.py:83-91, core.py:214-335)
+ *   hfmm_plan_destroy
+ */
+#ifndef HFMM_B200_H
+#define HFMM_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HFMM_OK 0
+#define HFMM_ERR_ARG -1       /* invalid argument (shape, range, null pointer)      */
+#define HFMM_ERR_CUDA -2      /* a CUDA runtime call failed                          */
+#define HFMM_ERR_STATE -3     /* call out of order (e.g. evaluate before finalize)    */
+#define HFMM_ERR_CAPACITY -4  /* a size limit was exceeded                           */
+#define HFMM_ERR_DEVICE -5    /* a kernel raised its device error flag               */
+
+#define HFMM_PREC_FP64 0      /* plain path: every phase in float64                  */
+#define HFMM_PREC_MIXED 1     /* FP32 pair kernels, 3xTF32 M2L, FP64 final sums      */
+
+typedef struct hfmm_plan hfmm_plan;
+
+/* Sizes of a built plan. Box indices follow the reference's packing
+ * (finest level first, trees/cubic.py:371-372); boxes [0, n_boxes) are active. */
+typedef struct hfmm_info {
+    int64_t n_points;
+    int32_t max_depth;        /* realised depth (build_fmm_tree_auto, cubic.py:530-600) */
+    int32_t maxleaf;          /* largest leaf occupancy                                 */
+    int64_t max_boxes;        /* the reference's box buffer size after doubling         */
+    int64_t n_boxes;          /* active boxes                                           */
+    int64_t n_leaves;
+    int32_t adaptive;         /* leaves on more than one level (core.py:117)            */
+    int32_t level_lo[16];     /* boxes of level l occupy [level_lo[l], level_hi[l])     */
+    int32_t level_hi[16];
+    double domain_extent;
+    double pmin[3];
+    int64_t n_v, n_u, n_w, n_x, n_near;   /* list lengths (0 until finalize)           */
+    int32_t n_s;              /* surface points per box (0 until a kernel is set)       */
+    int32_t p;
+} hfmm_info;
+
+/* Build the octree of n points (pos_dev: n x 3 float64, row-major, device).
+ * n_max is the leaf size N_max; max_depth <= 0 selects the reference's automatic
+ * depth (cubic.py:583-600). Replaces build_fmm_tree_auto + assign_particles
+ * (trees/cubic.py:530-695) and core.setup_geometry's tree part (core.py:111-117). */
+int hfmm_tree_build(const double* pos_dev, int64_t n, int32_t n_max, int32_t max_depth,
+                    hfmm_plan** out);
+
+int hfmm_plan_info(const hfmm_plan* plan, hfmm_info* out);
+
+/* Kernel: wavenumber k, p points per cube edge, n_families = 2 (cos and sin
+ * components, HFMM.py:65-80) or 1 (k == 0, HFMM.py:71-72). equiv_pts and
+ * check_pts are the unit surfaces (n_s x 3, host, row-major) at radii 1.05 and
+ * 2.95 (kifmm/surfaces.py:20-85); n_s = 6p^2 - 12p + 8. */
+int hfmm_plan_set_kernel(hfmm_plan* plan, double k, int32_t p, int32_t n_families,
+                         const double* equiv_pts, const double* check_pts);
+
+/* Per-level tables of one kernel family (0 = cos, 1 = sin), host pointers, all
+ * float64 row-major as the reference stacks them (operators.py:620-641):
+ *   F_up_U, F_up_Vt, F_dn_U, F_dn_Vt : n_s x n_s;  F_up_d, F_dn_d : n_s
+ *   M2M_K : 8 x n_s x n_s, M2M_K_lv[level]  (may be NULL when level == max_depth)
+ *   L2L_K : 8 x n_s x n_s, L2L_K_lv[level-1] (may be NULL when level < 3)
+ *   M2L_K : 343 x n_s x n_s, M2L_K_lv[level] (adjacent entries ignored)
+ * Only levels 2..max_depth are consumed; the library copies and re-lays them out. */
+int hfmm_plan_set_level(hfmm_plan* plan, int32_t family, int32_t level,
+                        const double* F_up_U, const double* F_up_d, const double* F_up_Vt,
+                        const double* F_dn_U, const double* F_dn_d, const double* F_dn_Vt,
+                        const double* M2M_K, const double* L2L_K, const double* M2L_K);
+
+/* Build the V, U, W, X lists and the evaluate schedules on the device
+ * (trees/lists.py:818-931, core.py:119-140). */
+int hfmm_plan_finalize(hfmm_plan* plan);
+
+/* Evaluate for charges q_re (+ q_im, nullable for real charges) in the
+ * original point order. phi_out: n complex128 (interleaved re, im).
+ * field_out (nullable): n x 3 complex128, the field -grad(phi)
+ * (kifmm/setup.py:242-246). With q_im == NULL this is HFMM.evaluate
+ * (HFMM.py:83-91); with q_im the result follows by linearity,
+ * phi = E_cos(q_re) - E_sin(q_im) + i (E_sin(q_re) + E_cos(q_im)).
+ * precision: HFMM_PREC_FP64 or HFMM_PREC_MIXED. stream: a cudaStream_t or NULL.
+ * Allocates nothing; asynchronous on the stream. */
+int hfmm_evaluate(hfmm_plan* plan, const double* q_re_dev, const double* q_im_dev,
+                  double* phi_out_dev, double* field_out_dev, int32_t precision,
+                  void* stream);
+
+/* Read and clear the plan's device error flag (synchronises the stream). */
+int hfmm_plan_check(hfmm_plan* plan, void* stream);
+
+void hfmm_plan_destroy(hfmm_plan* plan);
+
+/* ---- inspection (tests compare these with the oracle bit for bit) ---- */
+/* Tree arrays of the active boxes: m_id (uint64), p_id, lvls, counts (int32),
+ * is_leaf (uint8), each of length n_boxes; sort_idx (int32, n). Host buffers. */
+int hfmm_export_tree(const hfmm_plan* plan, uint64_t* m_id, int32_t* p_id, int32_t* lvls,
+                     int32_t* counts, uint8_t* is_leaf, int32_t* sort_idx);
+/* Particles-in-leaf table (n_boxes x maxleaf, -1 padded), cubic.py:683-693. Host buffer. */
+int hfmm_export_pil(const hfmm_plan* plan, int32_t* pil);
+/* List `which` (0 = V, 1 = U, 2 = W, 3 = X, 4 = near pairs) as (len x 2) int32, host. */
+int hfmm_export_list(const hfmm_plan* plan, int32_t which, int32_t* pairs, int64_t cap);
+
+/* ---- referee ---- */
+/* Direct sum phi_t = sum_{s: r>0} q_s e^{ikr}/r (test.py:11-18) at n_t targets
+ * (indices into the n points), with the field when field_out_dev != NULL.
+ * Partial sums go to a scratch buffer the library allocates per call. */
+int hfmm_direct(const double* pos_dev, const double* q_re_dev, const double* q_im_dev,
+                int64_t n, const int32_t* targets_dev, int64_t n_t, double k,
+                double* phi_out_dev, double* field_out_dev, void* stream);
+
+/* ---- diagnostics ---- */
+const char* hfmm_last_error(void);
+/* Kernels this library has launched since load (all plans, all threads). */
+int64_t hfmm_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HFMM_B200_H */

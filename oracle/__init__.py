@@ -1,0 +1,34 @@
+"""CPU oracle for the Helmholtz KIFMM evaluate path (test infrastructure only).
+
+This package is a NumPy restatement of the reference's HFMM path (HFMM.py,
+jaxfmm/kifmm/*, jaxfmm/core.py, jaxfmm/near.py, jaxfmm/trees/*). It exists to
+check the CUDA product: only ``tests/``, ``__graft_entry__.smoke()`` and the
+CPU-baseline leg of ``bench.py`` may import it, and never as the thing that is
+measured or shipped.
+
+Pinning: the reference ships no golden vectors. The oracle is pinned against
+the reference's own known-answer checks (test.py:63-72: direct-sum error
+thresholds, linearity, exact-zero imaginary part at k=0, monotone improvement
+in p) on the reference's default test grid, and against an O(N^2) direct sum.
+Bit-exact parity of the oracle with the reference's JAX arrays is unpinned:
+JAX is not installed here, so the reference cannot be run.
+"""
+
+from .surfaces import n_surf, surface_pts, R_EQUIV, R_CHECK
+from .operators import (helmholtz_G_np, pinv_factors, build_operators,
+                        build_operators_leveled)
+from .tree import (morton_encode, morton_decode, build_fmm_tree, build_fmm_tree_auto,
+                   assign_particles, box_geometry, NEIGH_OFFSETS, ADJ_CHILD_MASK)
+from .lists import build_v, build_u, build_wx, near_pairs
+from .hfmm import (setup, evaluate, evaluate_setup, evaluate_complex, kifmm_setup,
+                   direct, direct_field, relative_error)
+
+__all__ = [
+    "n_surf", "surface_pts", "R_EQUIV", "R_CHECK",
+    "helmholtz_G_np", "pinv_factors", "build_operators", "build_operators_leveled",
+    "morton_encode", "morton_decode", "build_fmm_tree", "build_fmm_tree_auto",
+    "assign_particles", "box_geometry", "NEIGH_OFFSETS", "ADJ_CHILD_MASK",
+    "build_v", "build_u", "build_wx", "near_pairs",
+    "setup", "evaluate", "evaluate_setup", "evaluate_complex", "kifmm_setup",
+    "direct", "direct_field", "relative_error",
+]

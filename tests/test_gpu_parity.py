@@ -1,0 +1,118 @@
+"""Parity of the CUDA path with the oracle.
+
+Integer work (tree arrays, particle slots, interaction lists) must match bit
+for bit; potentials and fields must match to a relative L2 of 1e-12 (float64
+everywhere; the bar of the plain path). Cases: the committed golden fixtures
+and live oracle runs on further clouds (plane / depth refinement, tiny N,
+duplicates, explicit max_depth)."""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+import oracle as O
+from cases import uniform, clustered, plane, with_duplicates, complex_uniform, sphere_clusters
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-12
+GOLD = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "*.npz")))
+
+
+def load(path):
+    with np.load(path) as z:
+        return {k: z[k] for k in z.files}
+
+
+def _setup(pos, k, p, nmax, md):
+    import hfmm_b200
+    return hfmm_b200.setup(pos, k, p=p, N_max=nmax, max_depth=md)
+
+
+def _compare_tree(st, s_or_g, oracle_state=True):
+    t = st.tree()
+    nb = st.info["n_boxes"]
+    for key in ("m_id", "p_id", "lvls", "counts", "is_leaf"):
+        ref = s_or_g[key][:nb] if oracle_state else s_or_g[key]
+        assert len(ref) == nb and np.array_equal(t[key], ref), key
+    if oracle_state:
+        assert not (s_or_g["lvls"][nb:] > 0).any()
+    assert np.array_equal(t["sort_idx"], s_or_g["sort_idx"])
+    ref_pil = s_or_g["pil"][:nb]
+    assert np.array_equal(st.pil(), ref_pil)
+
+
+def _compare_lists(st, ref):
+    for key, rk in (("V", "V"), ("U", "U"), ("near", "near"), ("W", "W"), ("X", "X")):
+        r = ref[rk]
+        r = np.empty((0, 2), np.int32) if r is None else r
+        got = st.pairs(key)
+        assert got.shape == r.shape and np.array_equal(got, r), key
+
+
+@pytest.mark.parametrize("path", GOLD, ids=[os.path.basename(p)[:-4] for p in GOLD])
+def test_golden(path):
+    import hfmm_b200
+    g = load(path)
+    md = int(g["max_depth"])
+    st = _setup(g["positions"], float(g["k"]), int(g["p"]), int(g["N_max"]), None if md < 0 else md)
+    assert st.info["max_depth"] == int(g["realised_depth"])
+    assert st.info["maxleaf"] == int(g["maxleaf"])
+    assert st.info["max_boxes"] == int(g["max_boxes"])
+    assert st.info["domain_extent"] == float(g["domain_extent"])
+    _compare_tree(st, g, oracle_state=False)
+    _compare_lists(st, g)
+    q = g["charges"]
+    if "E" in g:
+        phi, E = hfmm_b200.evaluate_field(st, q)
+        assert O.relative_error(E, g["E"]) < TOL
+    else:
+        phi = hfmm_b200.evaluate(st, q)
+    assert phi.dtype == np.complex128
+    assert O.relative_error(phi, g["phi"]) < TOL
+
+
+LIVE = [
+    ("plane", plane, 3000, 3.0, 4, 16, None),
+    ("dups", with_duplicates, 1200, 2.0, 4, 16, None),
+    ("tiny1", uniform, 1, 1.0, 3, 16, None),
+    ("tiny2", uniform, 2, 1.0, 3, 16, None),
+    ("tiny17", uniform, 17, 1.0, 3, 16, None),
+    ("depth5", uniform, 3000, 4.0, 4, 8, 5),
+    ("clustered_d3", clustered, 2500, 6.0, 5, 32, 3),
+    ("sphere", sphere_clusters, 4000, 10.0, 4, 24, None),
+]
+
+
+@pytest.mark.parametrize("name,fn,n,k,p,nmax,md", LIVE, ids=[c[0] for c in LIVE])
+def test_live_oracle(name, fn, n, k, p, nmax, md):
+    import hfmm_b200
+    pos, q = fn(n)
+    ref = O.setup(pos, k, p=p, N_max=nmax, max_depth=md)
+    st = _setup(pos, k, p, nmax, md)
+    s = ref[0]
+    assert st.info["max_depth"] == s["max_depth"] and st.info["maxleaf"] == s["maxleaf"]
+    assert st.info["max_boxes"] == s["max_boxes"]
+    _compare_tree(st, s)
+    _compare_lists(st, dict(V=s["V"], U=s["U"], near=s["dir_cnct"], W=s["W"], X=s["X"]))
+    qc = q if np.iscomplexobj(q) else q + 0.5j * np.cos(np.arange(n))
+    phi_r = hfmm_b200.evaluate(st, qc.real)
+    assert O.relative_error(phi_r, O.evaluate(ref, qc.real)) < TOL
+    phi, E = hfmm_b200.evaluate_field(st, qc)
+    rphi, rE = O.evaluate_complex(ref, qc, field=True)
+    assert O.relative_error(phi, rphi) < TOL
+    assert O.relative_error(E, rE) < TOL
+
+
+def test_c1_shape_against_oracle():
+    """The CPU-runnable workload's shape at reduced N: complex charges, potential +
+    field, k = 2 pi, p = 8, leaf size 64 (depth 3)."""
+    import hfmm_b200
+    pos, q = complex_uniform(6000)
+    k = 2 * np.pi
+    ref = O.setup(pos, k, p=8, N_max=64, max_depth=3)
+    st = _setup(pos, k, 8, 64, 3)
+    phi, E = hfmm_b200.evaluate_field(st, q)
+    rphi, rE = O.evaluate_complex(ref, q, field=True)
+    assert O.relative_error(phi, rphi) < TOL
+    assert O.relative_error(E, rE) < TOL
