@@ -13,6 +13,9 @@ LIB_PATH = os.path.join(_HERE, "_lib", "libhfmm_b200.so")
 HFMM_OK = 0
 HFMM_PREC_FP64 = 0
 HFMM_PREC_MIXED = 1
+N_PHASES = 11
+PHASES = ("gather", "p2m", "m2m_gemm", "up_decode", "m2l_l2l_gemm", "p2l", "down_decode",
+          "p2p", "l2p", "m2p", "combine")
 
 _c_i32, _c_i64, _c_dbl, _c_vp = ctypes.c_int32, ctypes.c_int64, ctypes.c_double, ctypes.c_void_p
 
@@ -54,6 +57,8 @@ SIGNATURES = [
     ("hfmm_export_list", _c_i32, [_c_vp, _c_i32, _c_vp, _c_i64]),
     ("hfmm_direct", _c_i32, [_c_vp, _c_vp, _c_vp, _c_i64, _c_vp, _c_i64, _c_dbl, _c_vp, _c_vp,
                              _c_vp]),
+    ("hfmm_plan_set_profiling", _c_i32, [_c_vp, _c_i32]),
+    ("hfmm_plan_phase_times", _c_i32, [_c_vp, _c_vp]),
     ("hfmm_last_error", ctypes.c_char_p, []),
     ("hfmm_launch_count", _c_i64, []),
 ]
@@ -67,7 +72,11 @@ class HFMMError(RuntimeError):
         self.code = code
 
 
-def _load():
+def load():
+    """Load (once) and return the library; raises ImportError when it is missing."""
+    global _handle
+    if _handle is not None:
+        return _handle
     if not os.path.exists(LIB_PATH):
         raise ImportError(
             f"hfmm_b200: CUDA library not built ({LIB_PATH} missing); run "
@@ -77,10 +86,19 @@ def _load():
         fn = getattr(lib, name)
         fn.restype = res
         fn.argtypes = args
+    _handle = lib
     return lib
 
 
-lib = _load()
+class _Lazy:
+    """Resolves symbols on first use, so building the library never needs an old copy."""
+
+    def __getattr__(self, name):
+        return getattr(load(), name)
+
+
+_handle = None
+lib = _Lazy()
 
 
 def check(code):

@@ -160,6 +160,29 @@ EvalView view(hfmm_plan* P) {
 
 struct PlanExtra {
     PtrIndex ix;
+    bool profiling = false;
+    std::vector<cudaEvent_t> ev;     // pairs (start, end)
+    std::vector<int> ev_phase;
+    size_t used = 0;
+    ~PlanExtra() {
+        for (auto e : ev) cudaEventDestroy(e);
+    }
+};
+
+// Records a start/end event pair around one phase instance when profiling is on.
+struct PhaseTimer {
+    PlanExtra* X;
+    cudaStream_t s;
+    size_t slot = (size_t)-1;
+    PhaseTimer(PlanExtra* x, cudaStream_t st, int phase) : X(x), s(st) {
+        if (!X || !X->profiling || X->used >= X->ev_phase.size()) return;
+        slot = X->used++;
+        X->ev_phase[slot] = phase;
+        HFMM_CUDA(cudaEventRecord(X->ev[2 * slot], s));
+    }
+    ~PhaseTimer() {
+        if (slot != (size_t)-1) cudaEventRecord(X->ev[2 * slot + 1], s);
+    }
 };
 
 std::mutex g_extra_mu;
@@ -211,7 +234,10 @@ void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double*
     const bool field = E != nullptr;
     PlanExtra* X = extra(P, false);
     const int64_t fs = P->nb * (int64_t)R * P->ld;   // family stride of expansion arrays
-    gather_charges(P->n, P->sort_idx.p, q_re, q_im, P->q_s.p, s);
+    {
+        PhaseTimer pt(X, s, 0);
+        gather_charges(P->n, P->sort_idx.p, q_re, q_im, P->q_s.p, s);
+    }
     EvalView v = view(P);
 
     ParticlePass base;
@@ -226,6 +252,7 @@ void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double*
     auto gemm = [&](int kind, int l, const hfmm_plan::Tiles& tiles, const int32_t* src_tab,
                     int src_ld, const double* B0, const double* B1, double* out,
                     const double* scale_set) {
+        PhaseTimer pt(X, s, kind == K_M2M ? 2 : kind == K_DN ? 4 : (kind <= K_UPV ? 3 : 6));
         GemmCall c{};
         c.tile_tgt = tiles.tgt.p;
         c.ntiles = tiles.ntiles;
@@ -252,6 +279,7 @@ void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double*
     auto decode = [&](int l, bool up, const double* in, double* out) {
         const hfmm_plan::Tiles& tiles = P->dec_tiles[l][R - 1];
         for (int f = 0; f < NF; ++f) {
+            PhaseTimer pt(X, s, up ? 3 : 6);
             GemmCall c{};
             c.tile_tgt = tiles.tgt.p;
             c.ntiles = tiles.ntiles;
@@ -285,6 +313,7 @@ void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double*
         p.nrows = P->n_leaves;
         p.surf = P->check_pts.p;
         p.out = P->check.p;
+        PhaseTimer pt(X, s, 1);
         particles_f64(p, s);
     }
     for (int l = P->md; l >= 2; --l) {
@@ -307,6 +336,7 @@ void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double*
             p.surf = P->equiv_pts.p;
             p.out = P->check.p;
             p.level = l;
+            PhaseTimer pt(X, s, 5);
             particles_f64(p, s);
         }
         decode(l, false, P->check.p, P->loc.p);
@@ -319,14 +349,20 @@ void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double*
         p.nrows = P->n_leaves;
         p.off = P->near_off.p;
         p.srcs = P->near_src.p;
-        particles_f64(p, s);
+        {
+            PhaseTimer pt(X, s, 7);
+            particles_f64(p, s);
+        }
         p = base;
         p.op = ParticleOp::L2P;
         p.rows = P->leaves.p;
         p.nrows = P->n_leaves;
         p.surf = P->check_pts.p;
         p.dens = P->loc.p;
-        particles_f64(p, s);
+        {
+            PhaseTimer pt(X, s, 8);
+            particles_f64(p, s);
+        }
         if (P->nW) {
             p = base;
             p.op = ParticleOp::M2P;
@@ -336,6 +372,7 @@ void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double*
             p.srcs = P->w_src.p;
             p.surf = P->equiv_pts.p;
             p.dens = P->equiv.p;
+            PhaseTimer pt(X, s, 9);
             particles_f64(p, s);
         }
         p = base;
@@ -343,6 +380,7 @@ void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double*
         p.rows = P->sort_idx.p;
         p.phi = phi;
         p.E = E;
+        PhaseTimer pt(X, s, 10);
         particles_f64(p, s);
     }
 }
@@ -539,6 +577,39 @@ int hfmm_plan_check(hfmm_plan* P, void* stream) {
         return fail(HFMM_ERR_DEVICE, "device error flag " + std::to_string(v) +
                                          " (1 = index out of bounds, 2 = capacity)");
     }
+    return HFMM_OK;
+    API_END
+}
+
+int hfmm_plan_set_profiling(hfmm_plan* P, int32_t enable) {
+    if (!P) return fail(HFMM_ERR_ARG, "plan is NULL");
+    API_BEGIN
+    PlanExtra* X = extra(P, true);
+    if (enable && X->ev.empty()) {
+        const size_t slots = 8192;
+        X->ev.resize(2 * slots);
+        for (auto& e : X->ev) HFMM_CUDA(cudaEventCreate(&e));
+        X->ev_phase.assign(slots, -1);
+    }
+    X->profiling = enable != 0;
+    X->used = 0;
+    return HFMM_OK;
+    API_END
+}
+
+int hfmm_plan_phase_times(hfmm_plan* P, double* ms) {
+    if (!P || !ms) return fail(HFMM_ERR_ARG, "NULL argument");
+    API_BEGIN
+    for (int i = 0; i < HFMM_N_PHASES; ++i) ms[i] = 0.0;
+    PlanExtra* X = extra(P, false);
+    if (!X || !X->profiling) return fail(HFMM_ERR_STATE, "profiling is off");
+    for (size_t i = 0; i < X->used; ++i) {
+        HFMM_CUDA(cudaEventSynchronize(X->ev[2 * i + 1]));
+        float t = 0;
+        HFMM_CUDA(cudaEventElapsedTime(&t, X->ev[2 * i], X->ev[2 * i + 1]));
+        if (X->ev_phase[i] >= 0 && X->ev_phase[i] < HFMM_N_PHASES) ms[X->ev_phase[i]] += t;
+    }
+    X->used = 0;   // the next read covers the evaluates issued after this one
     return HFMM_OK;
     API_END
 }

@@ -125,6 +125,18 @@ int hfmm_direct(const double* pos_dev, const double* q_re_dev, const double* q_i
                 int64_t n, const int32_t* targets_dev, int64_t n_t, double k,
                 double* phi_out_dev, double* field_out_dev, void* stream);
 
+/* ---- phase timers ---- */
+/* With profiling on, hfmm_evaluate records CUDA events around each phase on its
+ * stream. hfmm_plan_phase_times synchronises and writes the milliseconds spent
+ * per phase, summed over every evaluate since profiling was enabled or the
+ * previous read (up to 8192 phase instances): 0 charge gather, 1 P2M, 2 M2M GEMM, 3 upward decode,
+ * 4 M2L+L2L GEMM, 5 X-list P2L, 6 downward decode, 7 P2P, 8 L2P, 9 W-list M2P,
+ * 10 combine. (Replaces the reference's wall-clock phase prints; it has no
+ * per-phase timers, util.py:692-724.) */
+#define HFMM_N_PHASES 11
+int hfmm_plan_set_profiling(hfmm_plan* plan, int32_t enable);
+int hfmm_plan_phase_times(hfmm_plan* plan, double* ms_out);
+
 /* ---- diagnostics ---- */
 const char* hfmm_last_error(void);
 /* Kernels this library has launched since load (all plans, all threads). */

@@ -128,7 +128,11 @@ def build_fmm_tree(positions, max_boxes, max_depth, N_max):
     pmin = pos.min(0)
     grid = 2 ** md
     extent = np.max(pmax - pmin)
-    scaled = (pos - pmin) / extent * grid
+    with np.errstate(invalid="ignore", divide="ignore"):
+        scaled = (pos - pmin) / extent * grid
+    # extent == 0 (all points equal) gives NaN; XLA's float->int conversion saturates
+    # and maps NaN to 0, which NumPy's cast does not guarantee, so apply it explicitly.
+    scaled = np.where(np.isnan(scaled), 0.0, scaled)
     gc = np.clip(scaled.astype(np.uint64), U64(0), U64(grid - 1))
     part_m = morton_encode(gc[:, 0], gc[:, 1], gc[:, 2])
     sort_idx = np.argsort(part_m, kind="stable").astype(np.int32)
