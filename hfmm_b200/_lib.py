@@ -57,6 +57,8 @@ SIGNATURES = [
     ("hfmm_export_list", _c_i32, [_c_vp, _c_i32, _c_vp, _c_i64]),
     ("hfmm_direct", _c_i32, [_c_vp, _c_vp, _c_vp, _c_i64, _c_vp, _c_i64, _c_dbl, _c_vp, _c_vp,
                              _c_vp]),
+    ("hfmm_direct_noalloc", _c_i32, [_c_vp, _c_vp, _c_vp, _c_i64, _c_vp, _c_i64, _c_dbl, _c_vp,
+                                     _c_vp, _c_vp]),
     ("hfmm_plan_set_profiling", _c_i32, [_c_vp, _c_i32]),
     ("hfmm_plan_phase_times", _c_i32, [_c_vp, _c_vp]),
     ("hfmm_last_error", ctypes.c_char_p, []),

@@ -125,6 +125,17 @@ int hfmm_direct(const double* pos_dev, const double* q_re_dev, const double* q_i
                 int64_t n, const int32_t* targets_dev, int64_t n_t, double k,
                 double* phi_out_dev, double* field_out_dev, void* stream);
 
+/* Same result as hfmm_direct without allocating anything, for callers that
+ * cannot allocate device memory (a JAX/XLA process that owns the GPU memory, a
+ * stream under CUDA-graph capture). No counterpart in the reference. The partial
+ * sums live in a fixed 8 MiB device array inside this library, so n_t is limited
+ * to 131072 targets (HFMM_ERR_CAPACITY above that). The first call on a device
+ * looks up that array's address; make it before any stream capture. All calls
+ * share the array: calls that overlap on the GPU race. Synchronises `stream`. */
+int hfmm_direct_noalloc(const double* pos_dev, const double* q_re_dev, const double* q_im_dev,
+                        int64_t n, const int32_t* targets_dev, int64_t n_t, double k,
+                        double* phi_out_dev, double* field_out_dev, void* stream);
+
 /* ---- phase timers ---- */
 /* With profiling on, hfmm_evaluate records CUDA events around each phase on its
  * stream. hfmm_plan_phase_times synchronises and writes the milliseconds spent
