@@ -13,6 +13,7 @@
 // their equivalent and local densities are never read.
 #include "hfmm_internal.cuh"
 #include "particles.cuh"
+#include "mixed.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -100,8 +101,8 @@ std::vector<int32_t> nonadjacent_map() {
 
 // A-pointer sets of the GEMM calls: kind 0..3 decode (up U, up Vt, dn U, dn Vt),
 // kind 4 M2M (8 entries), kind 5 downward M2L+L2L (351 entries); per level, families adjacent.
-enum { K_UPU, K_UPV, K_DNU, K_DNV, K_M2M, K_DN, K_COUNT };
-const int k_entries[K_COUNT] = {1, 1, 1, 1, 8, M2L_ENTRIES};
+enum { K_UPU, K_UPV, K_DNU, K_DNV, K_M2M, K_DN, K_L2L, K_COUNT };
+const int k_entries[K_COUNT] = {1, 1, 1, 1, 8, M2L_ENTRIES, 8};
 
 struct PtrIndex {
     size_t off[K_COUNT][MAX_LEVELS];
@@ -130,6 +131,9 @@ void build_a_ptrs(hfmm_plan* P, PtrIndex& ix) {
                     case K_DN:
                         for (int d = 0; d < N_DISP; ++d)
                             h.push_back(compact[d] >= 0 ? T.m2l.p + compact[d] * mat : nullptr);
+                        for (int o = 0; o < 8; ++o) h.push_back(T.l2l.p ? T.l2l.p + o * mat : nullptr);
+                        break;
+                    case K_L2L:
                         for (int o = 0; o < 8; ++o) h.push_back(T.l2l.p ? T.l2l.p + o * mat : nullptr);
                         break;
                 }
@@ -228,7 +232,7 @@ void upload_level(hfmm_plan* P, int fam, int l, const double* const* h) {
 }
 
 void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double* phi, double* E,
-                   cudaStream_t s) {
+                   cudaStream_t s, bool mixed) {
     const int R = q_im ? 2 : 1;
     const int NF = P->n_fam;
     const bool field = E != nullptr;
@@ -252,7 +256,7 @@ void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double*
     auto gemm = [&](int kind, int l, const hfmm_plan::Tiles& tiles, const int32_t* src_tab,
                     int src_ld, const double* B0, const double* B1, double* out,
                     const double* scale_set) {
-        PhaseTimer pt(X, s, kind == K_M2M ? 2 : kind == K_DN ? 4 : (kind <= K_UPV ? 3 : 6));
+        PhaseTimer pt(X, s, kind == K_M2M ? 2 : (kind == K_DN || kind == K_L2L) ? 4 : (kind <= K_UPV ? 3 : 6));
         GemmCall c{};
         c.tile_tgt = tiles.tgt.p;
         c.ntiles = tiles.ntiles;
@@ -260,12 +264,12 @@ void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double*
         c.src_ld = src_ld;
         c.n_entries = k_entries[kind];
         c.b_split = kind == K_DN ? N_DISP : c.n_entries;
+        c.accumulate = kind == K_L2L ? 1 : 0;
         c.A = P->a_ptrs.p + X->ix.off[kind][l];
         c.B0 = B0;
         c.B1 = B1;
         c.out = out;
         c.scale = scale_set;
-        c.accumulate = 0;
         c.R = R;
         c.ld = P->ld;
         c.n_s = P->n_s;
@@ -322,10 +326,41 @@ void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double*
                  P->check.p, nullptr);
         decode(l, true, P->check.p, P->equiv.p);
     }
+    const bool use_mx = mixed && P->mixed_ready;
+    if (use_mx) {   // TF32 hi/lo halves of every equivalent density (B operand of the M2L)
+        PhaseTimer pt(X, s, 11);
+        split_tf32(P->equiv.p, P->e_hi.p, P->e_lo.p, (int64_t)NF * fs, s);
+    }
     // ---- downward pass (M2L + L2L in one GEMM, then X-list P2L, then decode)
     for (int l = 2; l <= P->md; ++l) {
-        gemm(K_DN, l, P->dn_tiles[l][R - 1], P->m2l_src.p, M2L_ENTRIES, P->equiv.p, P->loc.p,
-             P->check.p, nullptr);
+        if (use_mx) {
+            PhaseTimer pt(X, s, 4);
+            MixedCall mc{};
+            mc.tile_tgt = P->mx_tiles[l][R - 1].tgt.p;
+            mc.ntiles = P->mx_tiles[l][R - 1].ntiles;
+            mc.src_tab = P->m2l_src.p;
+            mc.disp_compact = P->disp_compact.p;
+            mc.Bhi = P->e_hi.p;
+            mc.Blo = P->e_lo.p;
+            mc.Lhi = nullptr;
+            mc.Llo = nullptr;
+            mc.out = P->check.p;
+            mc.R = R;
+            mc.ld = P->ld;
+            mc.n_fam = NF;
+            mc.has_l2l = 0;   // L2L stays FP64 (below): the downward locals are ill-conditioned
+            mc.fam_stride = fs;
+            mc.out_fam_stride = fs;
+            mc.nb = P->nb;
+            mc.err = P->d_err.p;
+            m2l_tf32x3(static_cast<MixedMaps*>(P->mx_maps)[l], mc, s);
+            if (l >= 3)   // L2L (phases.py:273-278) in FP64, added to the check potential
+                gemm(K_L2L, l, P->dn_tiles[l][R - 1], P->m2l_src.p + N_DISP, M2L_ENTRIES, P->loc.p,
+                     nullptr, P->check.p, nullptr);
+        } else {
+            gemm(K_DN, l, P->dn_tiles[l][R - 1], P->m2l_src.p, M2L_ENTRIES, P->equiv.p, P->loc.p,
+                 P->check.p, nullptr);
+        }
         if (P->nX) {
             ParticlePass p = base;
             p.op = ParticleOp::P2L;
@@ -476,7 +511,7 @@ int hfmm_plan_set_kernel(hfmm_plan* P, double k, int32_t p, int32_t n_families,
     P->k = k;
     P->p = p;
     P->n_s = 6 * p * p - 12 * p + 8;
-    P->ld = round_up(P->n_s, 16);
+    P->ld = round_up(P->n_s, 32);
     P->n_fam = n_families;
     for (int f = 0; f < 2; ++f)
         for (int l = 0; l < MAX_LEVELS; ++l) P->tables[f][l].reset();
@@ -538,6 +573,34 @@ int hfmm_plan_finalize(hfmm_plan* P) {
     P->equiv.zero();
     P->loc.zero();
     P->tmp.zero();
+    // mixed path: TF32 hi/lo tables, tensor maps, split density buffers (needs ld >= 128)
+    P->mixed_ready = false;
+    if (P->ld >= 128) {
+        std::vector<int32_t> dc(N_DISP, -1);
+        auto madj = nonadjacent_map();
+        for (size_t i = 0; i < madj.size(); ++i) dc[madj[i]] = (int32_t)i;
+        P->disp_compact.alloc(N_DISP);
+        HFMM_CUDA(cudaMemcpy(P->disp_compact.p, dc.data(), N_DISP * 4, cudaMemcpyHostToDevice));
+        const size_t mat = (size_t)P->ld * P->ld;
+        if (!P->mx_maps) P->mx_maps = new MixedMaps[MAX_LEVELS];
+        MixedMaps* maps = static_cast<MixedMaps*>(P->mx_maps);
+        std::memset(maps, 0, sizeof(MixedMaps) * MAX_LEVELS);
+        for (int f = 0; f < P->n_fam; ++f)
+            for (int l = 2; l <= P->md; ++l) {
+                LevelTables& T = P->tables[f][l];
+                const int nm = (int)madj.size();
+                T.m2l_hi.alloc(nm * mat);
+                T.m2l_lo.alloc(nm * mat);
+                split_transpose_tables(T.m2l.p, T.m2l_hi.p, T.m2l_lo.p, P->ld, nm);
+                make_table_map(&maps[l].a_hi[f], T.m2l_hi.p, P->ld, nm);
+                make_table_map(&maps[l].a_lo[f], T.m2l_lo.p, P->ld, nm);
+            }
+        P->e_hi.alloc(exp);
+        P->e_lo.alloc(exp);
+        P->e_hi.zero();
+        P->e_lo.zero();
+        P->mixed_ready = true;
+    }
     P->q_s.alloc(2 * P->n);
     P->pot.alloc((size_t)P->n_fam * 2 * P->n);
     P->fld.alloc((size_t)P->n_fam * 2 * 3 * P->n);
@@ -552,14 +615,14 @@ int hfmm_evaluate(hfmm_plan* P, const double* q_re, const double* q_im, double* 
     if (!P) return fail(HFMM_ERR_ARG, "plan is NULL");
     if (!P->finalized) return fail(HFMM_ERR_STATE, "plan not finalized");
     if (!q_re || !phi) return fail(HFMM_ERR_ARG, "charges and output are required");
-    if (precision != HFMM_PREC_FP64)
-        return fail(HFMM_ERR_ARG, "precision mode not available in this build");
+    if (precision != HFMM_PREC_FP64 && precision != HFMM_PREC_MIXED)
+        return fail(HFMM_ERR_ARG, "precision must be HFMM_PREC_FP64 or HFMM_PREC_MIXED");
     API_BEGIN
     require_device_ptr(q_re, "q_re");
     if (q_im) require_device_ptr(q_im, "q_im");
     require_device_ptr(phi, "phi_out");
     if (E) require_device_ptr(E, "field_out");
-    evaluate_fp64(P, q_re, q_im, phi, E, (cudaStream_t)stream);
+    evaluate_fp64(P, q_re, q_im, phi, E, (cudaStream_t)stream, precision == HFMM_PREC_MIXED);
     return HFMM_OK;
     API_END
 }
@@ -617,6 +680,8 @@ int hfmm_plan_phase_times(hfmm_plan* P, double* ms) {
 void hfmm_plan_destroy(hfmm_plan* P) {
     if (!P) return;
     drop_extra(P);
+    delete[] static_cast<MixedMaps*>(P->mx_maps);
+    P->mx_maps = nullptr;
     delete P;
 }
 

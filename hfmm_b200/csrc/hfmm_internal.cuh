@@ -45,6 +45,7 @@ extern std::atomic<int64_t> g_launches;
 enum : int {
     ERRF_BOUNDS = 1,      // an index left its buffer (access skipped)
     ERRF_CAPACITY = 2,    // a device-side capacity was exceeded
+    ERRF_TIMEOUT = 4,     // a bounded wait gave up (the kernel drained and returned)
 };
 
 // ---------------------------------------------------------------- device memory
@@ -82,11 +83,14 @@ struct LevelTables {
     DevBuf<double> m2m;                 // 8 x (A^T) for this level as PARENT
     DevBuf<double> l2l;                 // 8 x (A^T) for this level as CHILD
     DevBuf<double> m2l;                 // 316 x (A^T), non-adjacent displacements
+    // mixed path: TF32 hi/lo halves of M2L and L2L as A[m][k] (fp32 containers)
+    DevBuf<float> m2l_hi, m2l_lo, l2l_hi, l2l_lo;
     bool set = false;
     void reset() {
         up_U.release(); up_d.release(); up_Vt.release();
         dn_U.release(); dn_d.release(); dn_Vt.release();
         m2m.release(); l2l.release(); m2l.release();
+        m2l_hi.release(); m2l_lo.release(); l2l_hi.release(); l2l_lo.release();
         set = false;
     }
 };
@@ -150,6 +154,11 @@ struct hfmm_plan {
     Tiles m2m_tiles[hfmm::MAX_LEVELS][2];   // [level][R-1]
     Tiles dn_tiles[hfmm::MAX_LEVELS][2];
     Tiles dec_tiles[hfmm::MAX_LEVELS][2];
+    Tiles mx_tiles[hfmm::MAX_LEVELS][2];    // mixed M2L tiles: 128 / R targets, by octant
+    hfmm::DevBuf<int32_t> disp_compact;     // 343 -> M2L table index or -1
+    hfmm::DevBuf<float> e_hi, e_lo, l_hi, l_lo;   // split densities [fam][box][R][ld]
+    void* mx_maps = nullptr;                // MixedMaps per level (host array)
+    bool mixed_ready = false;
     hfmm::DevBuf<const double*> a_ptrs;     // device arrays of A pointers per GEMM call
     std::vector<const double*> h_a_ptrs;
     size_t a_ptr_cursor = 0;
@@ -171,7 +180,7 @@ void lists_build(hfmm_plan* P);
 void schedules_build(hfmm_plan* P);
 void upload_level(hfmm_plan* P, int fam, int level, const double* const* h);
 void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double* phi,
-                   double* fld, cudaStream_t s);
+                   double* fld, cudaStream_t s, bool mixed = false);
 void direct_sum(const double* pos, const double* q_re, const double* q_im, int64_t n,
                 const int32_t* targets, int64_t n_t, double k, double* phi, double* fld,
                 double* scratch, int n_split, cudaStream_t s, int* err);

@@ -467,6 +467,18 @@ void schedules_build(hfmm_plan* P) {
             }
             P->dn_tiles[l][r].ntiles = (int)(byoct.size() / TT);
             upload(P->dn_tiles[l][r].tgt, byoct);
+            // mixed M2L tiles: 128 columns = 128 / R targets, same octant grouping
+            const int TTM = 128 / (r + 1);
+            std::vector<int32_t> mx;
+            for (int o = 0; o < 8; ++o) {
+                std::vector<int32_t> g;
+                for (int b = lo; b < hi; ++b)
+                    if ((int)(P->h_m_id[b] & 7ull) == o) g.push_back(b);
+                for (size_t i = 0; i < g.size(); i += TTM)
+                    for (int j = 0; j < TTM; ++j) mx.push_back(i + j < g.size() ? g[i + j] : -1);
+            }
+            P->mx_tiles[l][r].ntiles = (int)(mx.size() / TTM);
+            upload(P->mx_tiles[l][r].tgt, mx);
         }
     }
     HFMM_CUDA(cudaDeviceSynchronize());

@@ -1,0 +1,506 @@
+// Mixed-precision M2L (+ L2L) on the 5th-generation tensor cores: split 3xTF32.
+//
+// Same contraction as the FP64 output-stationary GEMM (gemm_f64.cu; M2L of
+// phases.py:211-236 and L2L of phases.py:273-278 summed into one check
+// potential), with every product A*B evaluated as
+//     A_hi*B_hi + A_hi*B_lo + A_lo*B_hi,   x_hi = tf32(x), x_lo = tf32(x - x_hi)
+// by tcgen05.mma kind::tf32 into one FP32 accumulator in tensor memory.
+//
+// CTA = one tile of target boxes (same level and octant) x one 128-row block of
+// the n_s check points x one kernel family; accumulator 128 lanes x 128 columns
+// (targets x charge columns) FP32 in TMEM. Per k-chunk of 32 (128-byte rows):
+//   * warp 4 (one lane) loads A_hi and A_lo with TMA (3-D tensor maps over the
+//     level's tables, SWIZZLE_128B, K-major) -> mbarrier complete_tx;
+//   * warps 0-3 gather the B columns (source boxes' equivalent densities) with
+//     16-byte cp.async into the same SWIZZLE_128B K-major layout, then fence the
+//     generic->async proxy and arrive on the stage's mbarrier;
+//   * warp 5 (one lane) issues 4 k-steps x 3 tcgen05.mma and commits the stage
+//     back to its "empty" mbarrier;
+// three stages in flight.
+// Accumulation precision: the error of an FP32 accumulator grows with the
+// length of its chain of MMAs (measured: about linearly), and the damped decode
+// amplifies it. So every FOLD k-chunks (24 MMAs) accumulate into a fresh FP32
+// buffer in TMEM (two buffers alternate), and warps 6-9 fold each finished
+// buffer into an FP64 running sum kept in TMEM (two 32-bit columns per double)
+// while the tensor core fills the other buffer. TMEM: 2 x 128 FP32 columns + 256 for the FP64
+// sums = 512 columns. The FP64 sums are stored as the check potentials.
+// Every mbarrier wait is bounded (2 s of %globaltimer); a timeout sets the
+// device error flag and every role drains and exits, TMEM is freed.
+#include "hfmm_internal.cuh"
+#include "mixed.cuh"
+
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <mutex>
+
+namespace hfmm {
+
+namespace {
+
+constexpr int BM = 128;          // UMMA M (check points per CTA)
+constexpr int BN = 128;          // UMMA N (target columns per CTA)
+constexpr int BK = 32;           // fp32 elements per k-chunk (128-byte rows)
+constexpr int STAGES = 3;
+constexpr int TILE_BYTES = BM * BK * 4;   // 16 KiB, one operand half
+constexpr int STAGE_BYTES = 4 * TILE_BYTES;
+constexpr int THREADS = 320;       // warps 0-3 gather, 4 TMA, 5 MMA, 6-9 accumulate
+constexpr int TMEM_COLS = 512;
+constexpr int FOLD = 2;            // k-chunks per FP32 accumulation unit
+constexpr uint64_t WAIT_NS = 2000000000ull;   // bounded waits: 2 s
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ uint64_t gtimer() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count));
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait: false on timeout or when another role has aborted.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int* abort_flag) {
+    if (mbar_try(bar, parity)) return true;
+    const uint64_t t0 = gtimer();
+    while (true) {
+        if (mbar_try(bar, parity)) return true;
+        if (*abort_flag) return false;
+        if (gtimer() - t0 > WAIT_NS) {
+            *abort_flag = 1;
+            return false;
+        }
+    }
+}
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, bool valid) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(dst), "l"(src),
+                 "r"(valid ? 16 : 0));
+}
+__device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap* map, int c0, int c1,
+                                            int c2, uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(bar)
+        : "memory");
+}
+// UMMA shared-memory descriptor: K-major, SWIZZLE_128B, 8-row groups 1024 B apart.
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t addr) {
+    return (uint64_t)((addr & 0x3FFFF) >> 4) | (1ull << 16) | (64ull << 32) | (1ull << 46) |
+           (2ull << 61);
+}
+__device__ __forceinline__ void umma_tf32(uint32_t tmem, uint64_t a, uint64_t b, uint32_t idesc,
+                                          uint32_t acc) {
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+        " tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
+        "l"(a), "l"(b), "r"(idesc), "r"(acc));
+}
+__device__ __forceinline__ void umma_commit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+                 : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t* v) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,"
+        "%14,%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+          "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
+          "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]),
+          "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]),
+          "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+        : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_st32(uint32_t taddr, const uint32_t* v) {
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,"
+        "%13,%14,%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,%32};" ::"r"(taddr),
+        "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7]),
+        "r"(v[8]), "r"(v[9]), "r"(v[10]), "r"(v[11]), "r"(v[12]), "r"(v[13]), "r"(v[14]),
+        "r"(v[15]), "r"(v[16]), "r"(v[17]), "r"(v[18]), "r"(v[19]), "r"(v[20]), "r"(v[21]),
+        "r"(v[22]), "r"(v[23]), "r"(v[24]), "r"(v[25]), "r"(v[26]), "r"(v[27]), "r"(v[28]),
+        "r"(v[29]), "r"(v[30]), "r"(v[31])
+        : "memory");
+}
+
+// Instruction descriptor: D = F32, A = B = TF32, both K-major, M = 128, N = BN.
+constexpr uint32_t IDESC = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(BN >> 3) << 17) |
+                           ((uint32_t)(BM >> 4) << 24);
+
+struct __align__(8) Ctl {
+    uint64_t full[STAGES];
+    uint64_t empty[STAGES];
+    uint64_t acc_full[2];    // a unit's FP32 sum is complete in buffer b (MMA commit)
+    uint64_t acc_empty[2];   // buffer b has been folded into the FP64 sum (128 arrivals)
+    uint64_t done;
+    uint32_t tmem;
+    int abort_flag;
+    int n_act;
+    int tgt[BN];
+    short act[M2L_ENTRIES + 1];
+};
+
+template <int R>
+__global__ void __launch_bounds__(THREADS, 1) k_m2l_tf32x3(const __grid_constant__ MixedMaps maps,
+                                                            MixedCall c) {
+    constexpr int TT = BN / R;
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    unsigned char* sm = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    Ctl& ctl = *reinterpret_cast<Ctl*>(sm + STAGES * STAGE_BYTES);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int tile = blockIdx.x, m0 = blockIdx.y * BM, fam = blockIdx.z;
+    volatile int* abort_flag = &ctl.abort_flag;
+
+    if (tid < TT) {
+        int t = c.tile_tgt[(int64_t)tile * TT + tid];
+        if (t >= c.nb) {
+            atomicOr(c.err, ERRF_BOUNDS);
+            t = -1;
+        }
+        ctl.tgt[tid] = t;
+    }
+    if (tid == 0) {
+        ctl.abort_flag = 0;
+        for (int s = 0; s < STAGES; ++s) {
+            mbar_init(smem_u32(&ctl.full[s]), 1 + 128);   // TMA arrive + 128 gather threads
+            mbar_init(smem_u32(&ctl.empty[s]), 1);       // MMA commit
+        }
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(smem_u32(&ctl.acc_full[b]), 1);
+            mbar_init(smem_u32(&ctl.acc_empty[b]), 128);
+        }
+        mbar_init(smem_u32(&ctl.done), 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 5) {   // tensor memory: 2 FP32 entry buffers + the FP64 running sums
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_u32(&ctl.tmem)),
+                     "r"(TMEM_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    // active entries (ballot compaction by warp 0)
+    if (warp == 0) {
+        int base = 0;
+        for (int e0 = 0; e0 < M2L_ENTRIES; e0 += 32) {
+            int e = e0 + lane;
+            bool act = false;
+            if (e < M2L_ENTRIES && (e < N_DISP ? c.disp_compact[e] >= 0 : c.has_l2l != 0)) {
+                for (int j = 0; j < TT && !act; ++j) {
+                    int t = ctl.tgt[j];
+                    if (t >= 0 && c.src_tab[(int64_t)t * M2L_ENTRIES + e] >= 0) act = true;
+                }
+            }
+            unsigned bal = __ballot_sync(0xffffffffu, act);
+            if (act) ctl.act[base + __popc(bal & ((1u << lane) - 1))] = (short)e;
+            base += __popc(bal);
+        }
+        if (lane == 0) ctl.n_act = base;
+    }
+    __syncthreads();
+    const int n_act = ctl.n_act;
+    const int kch = c.ld / BK;
+    const int nq = n_act * kch;
+    const uint32_t tmem = ctl.tmem;
+    const int64_t fs = (int64_t)fam * c.fam_stride;
+
+    if (warp < 4) {
+        // ---------------- B gathers (cp.async, manual SWIZZLE_128B placement)
+        const float* Bh = c.Bhi + fs;
+        const float* Bl = c.Blo + fs;
+        const float* Lh = c.Lhi ? c.Lhi + fs : nullptr;
+        const float* Ll = c.Llo ? c.Llo + fs : nullptr;
+        int pending = -1;
+        for (int q = 0; q < nq; ++q) {
+            const int st = q % STAGES;
+            if (!mbar_wait(smem_u32(&ctl.empty[st]), ((q / STAGES) & 1) ^ 1, abort_flag)) break;
+            const int e = ctl.act[q / kch];
+            const int k0 = (q % kch) * BK;
+            const bool l2l = e >= N_DISP;
+            const float* srch = l2l ? Lh : Bh;
+            const float* srcl = l2l ? Ll : Bl;
+            const uint32_t sbh = smem_u32(sm + st * STAGE_BYTES + 2 * TILE_BYTES);
+            const uint32_t sbl = sbh + TILE_BYTES;
+#pragma unroll 4
+            for (int idx = tid; idx < BN * 8; idx += 128) {
+                const int n = idx >> 3, ch = idx & 7;
+                const int j = n / R, r = n % R;
+                const int t = ctl.tgt[j];
+                int s = -1;
+                if (t >= 0) s = c.src_tab[(int64_t)t * M2L_ENTRIES + e];
+                bool ok = s >= 0 && s < c.nb && srch != nullptr;
+                if (s >= c.nb) atomicOr(c.err, ERRF_BOUNDS);
+                const int64_t off = ok ? ((int64_t)s * R + r) * c.ld + k0 + ch * 4 : 0;
+                const uint32_t so = (uint32_t)((n >> 3) * 1024 + (n & 7) * 128 + ((ch ^ (n & 7)) << 4));
+                cp_async16(sbh + so, ok ? (const void*)(srch + off) : (const void*)Bh, ok);
+                cp_async16(sbl + so, ok ? (const void*)(srcl + off) : (const void*)Bl, ok);
+            }
+            asm volatile("cp.async.commit_group;\n" ::);
+            if (pending >= 0) {
+                asm volatile("cp.async.wait_group 1;\n" ::);
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                mbar_arrive(smem_u32(&ctl.full[pending % STAGES]));
+            }
+            pending = q;
+        }
+        asm volatile("cp.async.wait_all;\n" ::);
+        if (pending >= 0) {
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            mbar_arrive(smem_u32(&ctl.full[pending % STAGES]));
+        }
+    } else if (warp >= 6) {
+        // ---------------- fold entries into the FP64 sums; store at the end
+        const int quad = warp & 3;                 // TMEM lane quadrant of this warp
+        const int m = m0 + quad * 32 + lane;
+        const uint32_t lane_base = tmem + ((uint32_t)(quad * 32) << 16);
+        double* out = c.out + (int64_t)fam * c.out_fam_stride;
+        bool ok = true;
+        const int n_units = (nq + FOLD - 1) / FOLD;
+        for (int i = 0; i < n_units && ok; ++i) {
+            const int b = i & 1;
+            // the TMEM loads below are warp-collective: agree on the wait's outcome
+            const bool got = mbar_wait(smem_u32(&ctl.acc_full[b]), (i >> 1) & 1, abort_flag);
+            if (!__all_sync(0xffffffffu, got)) {
+                ok = false;
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;");
+            for (int cc = 0; cc < BN / 32; ++cc) {
+                uint32_t v[32];
+                tmem_ld32(lane_base + b * BN + cc * 32, v);
+                uint32_t w[64];
+                if (i > 0) {
+                    tmem_ld32(lane_base + 2 * BN + cc * 64, w);
+                    tmem_ld32(lane_base + 2 * BN + cc * 64 + 32, w + 32);
+                }
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+                for (int j = 0; j < 32; ++j) {
+                    double acc = (double)__uint_as_float(v[j]);
+                    if (i > 0) acc += __hiloint2double((int)w[2 * j + 1], (int)w[2 * j]);
+                    w[2 * j] = (uint32_t)__double2loint(acc);
+                    w[2 * j + 1] = (uint32_t)__double2hiint(acc);
+                }
+                tmem_st32(lane_base + 2 * BN + cc * 64, w);
+                tmem_st32(lane_base + 2 * BN + cc * 64 + 32, w + 32);
+            }
+            asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+            asm volatile("tcgen05.fence::before_thread_sync;");
+            mbar_arrive(smem_u32(&ctl.acc_empty[b]));
+        }
+        const bool aborted = !__all_sync(0xffffffffu, ok && !*abort_flag);
+        if (aborted) {
+            if (lane == 0) atomicOr(c.err, ERRF_TIMEOUT);
+        } else if (m0 + quad * 32 < c.ld) {   // ld % 32 == 0: a warp is all in or all out
+            for (int cc = 0; cc < BN / 32; ++cc) {
+                uint32_t w[64];
+                if (nq > 0) {
+                    tmem_ld32(lane_base + 2 * BN + cc * 64, w);
+                    tmem_ld32(lane_base + 2 * BN + cc * 64 + 32, w + 32);
+                    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                }
+#pragma unroll
+                for (int j = 0; j < 32; ++j) {
+                    const int n = cc * 32 + j;
+                    const int t = ctl.tgt[n / R];
+                    const double val = nq > 0 ? __hiloint2double((int)w[2 * j + 1], (int)w[2 * j]) : 0.0;
+                    if (t >= 0) out[((int64_t)t * R + (n % R)) * c.ld + m] = val;
+                }
+            }
+        }
+    } else if (warp == 4) {
+        // ---------------- A tiles by TMA
+        if (lane == 0) {
+            const CUtensorMap* mh = &maps.a_hi[fam];
+            const CUtensorMap* ml = &maps.a_lo[fam];
+            const CUtensorMap* lh = &maps.l_hi[fam];
+            const CUtensorMap* ll = &maps.l_lo[fam];
+            for (int q = 0; q < nq; ++q) {
+                const int st = q % STAGES;
+                if (!mbar_wait(smem_u32(&ctl.empty[st]), ((q / STAGES) & 1) ^ 1, abort_flag)) break;
+                const int e = ctl.act[q / kch];
+                const int k0 = (q % kch) * BK;
+                const uint32_t fb = smem_u32(&ctl.full[st]);
+                const uint32_t sa = smem_u32(sm + st * STAGE_BYTES);
+                mbar_arrive_tx(fb, 2 * TILE_BYTES);
+                if (e < N_DISP) {
+                    const int z = c.disp_compact[e];
+                    tma_load_3d(sa, mh, k0, m0, z, fb);
+                    tma_load_3d(sa + TILE_BYTES, ml, k0, m0, z, fb);
+                } else {
+                    tma_load_3d(sa, lh, k0, m0, e - N_DISP, fb);
+                    tma_load_3d(sa + TILE_BYTES, ll, k0, m0, e - N_DISP, fb);
+                }
+            }
+        }
+    } else {
+        // ---------------- MMA issue (warp 5, one lane)
+        if (lane == 0) {
+            bool ok = true;
+            for (int q = 0; q < nq && ok; ++q) {
+                const int st = q % STAGES;
+                const int unit = q / FOLD, uq = q % FOLD;
+                const int b = unit & 1;
+                if (uq == 0 && unit >= 2) {   // buffer b must have been folded (unit - 2)
+                    if (!mbar_wait(smem_u32(&ctl.acc_empty[b]), ((unit >> 1) & 1) ^ 1, abort_flag)) {
+                        ok = false;
+                        break;
+                    }
+                    asm volatile("tcgen05.fence::after_thread_sync;");
+                }
+                if (!mbar_wait(smem_u32(&ctl.full[st]), (q / STAGES) & 1, abort_flag)) {
+                    ok = false;
+                    break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;");
+                const uint32_t base = smem_u32(sm + st * STAGE_BYTES);
+                const uint64_t ah = sw128_desc(base), al = sw128_desc(base + TILE_BYTES);
+                const uint64_t bh = sw128_desc(base + 2 * TILE_BYTES),
+                               bl = sw128_desc(base + 3 * TILE_BYTES);
+                const uint32_t dt = tmem + b * BN;
+#pragma unroll
+                for (int ks = 0; ks < BK / 8; ++ks) {   // 8 tf32 = 32 bytes per k-step
+                    const uint64_t d = (uint64_t)(ks * 2);
+                    umma_tf32(dt, ah + d, bh + d, IDESC, (uq > 0 || ks > 0) ? 1u : 0u);
+                    umma_tf32(dt, ah + d, bl + d, IDESC, 1u);
+                    umma_tf32(dt, al + d, bh + d, IDESC, 1u);
+                }
+                umma_commit(smem_u32(&ctl.empty[st]));
+                if (uq == FOLD - 1 || q == nq - 1) umma_commit(smem_u32(&ctl.acc_full[b]));
+            }
+            if (ok && nq > 0) umma_commit(smem_u32(&ctl.done));
+        }
+    }
+    // drain: nothing may be in flight into shared or tensor memory when the CTA exits
+    if (warp == 5 && lane == 0 && nq > 0 && *abort_flag) mbar_wait(smem_u32(&ctl.done), 0, abort_flag);
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    if (warp == 5) {
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
+    }
+}
+
+// Round an FP32 value to TF32 (10 explicit mantissa bits, ties away from zero) and
+// clear the 13 low bits, so the container holds exactly the value the tensor core
+// multiplies, however it treats the low bits.
+__device__ __forceinline__ float tf32_exact(float x) {
+    return __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xFFFFE000u);
+}
+
+// x -> (hi, lo) with hi = tf32(x), lo = tf32(x - hi), both exact TF32 in FP32 containers
+__device__ __forceinline__ void split2(double x, float& hi, float& lo) {
+    hi = tf32_exact((float)x);
+    lo = tf32_exact((float)(x - (double)hi));
+}
+
+__global__ void k_split_tf32(const double* __restrict__ src, float* hi, float* lo, int64_t n) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float h, l;
+    split2(src[i], h, l);
+    hi[i] = h;
+    lo[i] = l;
+}
+
+// FP64 A^T tables ([k][m], ld x ld) -> TF32 hi/lo A tables ([m][k]), count matrices
+__global__ void k_split_transpose(const double* __restrict__ at, float* hi, float* lo, int ld) {
+    __shared__ double tile[32][33];
+    const int c = blockIdx.z;
+    const int bk = blockIdx.x * 32, bm = blockIdx.y * 32;
+    const double* S = at + (int64_t)c * ld * ld;
+    for (int yy = threadIdx.y; yy < 32; yy += blockDim.y) {
+        int k = bk + yy, m = bm + threadIdx.x;
+        tile[yy][threadIdx.x] = (k < ld && m < ld) ? S[(int64_t)k * ld + m] : 0.0;
+    }
+    __syncthreads();
+    for (int yy = threadIdx.y; yy < 32; yy += blockDim.y) {
+        int m = bm + yy, k = bk + threadIdx.x;
+        if (m < ld && k < ld) {
+            float h, l;
+            split2(tile[threadIdx.x][yy], h, l);
+            int64_t o = (int64_t)c * ld * ld + (int64_t)m * ld + k;
+            hi[o] = h;
+            lo[o] = l;
+        }
+    }
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+    });
+    if (!fn) throw Error{HFMM_ERR_CUDA, "cuTensorMapEncodeTiled is not available"};
+    return fn;
+}
+
+}  // namespace
+
+void make_table_map(CUtensorMap* map, const float* base, int ld, int count) {
+    if (((uintptr_t)base & 15) || (ld * 4) % 16)
+        throw Error{HFMM_ERR_STATE, "tensor map: table not 16-byte aligned"};
+    cuuint64_t dims[3] = {(cuuint64_t)ld, (cuuint64_t)ld, (cuuint64_t)count};
+    cuuint64_t strides[2] = {(cuuint64_t)ld * 4, (cuuint64_t)ld * ld * 4};
+    cuuint32_t box[3] = {BK, BM, 1};
+    cuuint32_t estr[3] = {1, 1, 1};
+    CUresult r = encode_fn()(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, (void*)base, dims, strides,
+                             box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) throw Error{HFMM_ERR_CUDA, "cuTensorMapEncodeTiled failed: " + std::to_string((int)r)};
+}
+
+void split_tf32(const double* src, float* hi, float* lo, int64_t n, cudaStream_t s) {
+    if (n <= 0) return;
+    HFMM_LAUNCH(k_split_tf32, (unsigned)ceil_div(n, 256), 256, 0, s, src, hi, lo, n);
+}
+
+void split_transpose_tables(const double* at, float* hi, float* lo, int ld, int count) {
+    dim3 grid((unsigned)ceil_div(ld, 32), (unsigned)ceil_div(ld, 32), (unsigned)count);
+    HFMM_LAUNCH(k_split_transpose, grid, dim3(32, 8), 0, 0, at, hi, lo, ld);
+}
+
+size_t m2l_tf32x3_smem() { return (size_t)STAGES * STAGE_BYTES + sizeof(Ctl) + 1024; }
+
+void m2l_tf32x3(const MixedMaps& maps, const MixedCall& c, cudaStream_t s) {
+    if (c.ntiles == 0) return;
+    if (c.ld % BK) throw Error{HFMM_ERR_STATE, "m2l_tf32x3: ld must be a multiple of 32"};
+    const size_t smem = m2l_tf32x3_smem();
+    dim3 grid(c.ntiles, (c.ld + BM - 1) / BM, c.n_fam);
+    if (c.R == 1) {
+        HFMM_CUDA(cudaFuncSetAttribute(k_m2l_tf32x3<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        HFMM_LAUNCH(k_m2l_tf32x3<1>, grid, THREADS, smem, s, maps, c);
+    } else {
+        HFMM_CUDA(cudaFuncSetAttribute(k_m2l_tf32x3<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        HFMM_LAUNCH(k_m2l_tf32x3<2>, grid, THREADS, smem, s, maps, c);
+    }
+}
+
+}  // namespace hfmm

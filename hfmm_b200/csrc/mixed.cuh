@@ -1,0 +1,36 @@
+// Mixed-precision (3xTF32 on tcgen05) M2L: shared declarations.
+#pragma once
+#include "hfmm_internal.cuh"
+
+#include <cuda.h>
+
+namespace hfmm {
+
+// TMA descriptors of one level's TF32 hi/lo tables, per kernel family:
+// M2L (316 non-adjacent displacements) and L2L (8 octants), each [z][m][k] fp32.
+struct MixedMaps {
+    CUtensorMap a_hi[2], a_lo[2], l_hi[2], l_lo[2];
+};
+
+struct MixedCall {
+    const int32_t* tile_tgt;       // ntiles x (128 / R) target boxes, -1 padded
+    int ntiles;
+    const int32_t* src_tab;        // nb x 351 source boxes (-1 = none)
+    const int32_t* disp_compact;   // 343: displacement -> M2L table index (-1 = adjacent)
+    const float* Bhi;              // equivalent densities, split, [fam][box][R][ld]
+    const float* Blo;
+    const float* Lhi;              // parent local densities, split (L2L entries)
+    const float* Llo;
+    double* out;                   // check potentials [fam][box][R][ld], FP64
+    int R, ld, n_fam, has_l2l;
+    int64_t fam_stride, out_fam_stride, nb;
+    int* err;
+};
+
+void make_table_map(CUtensorMap* map, const float* base, int ld, int count);
+void split_tf32(const double* src, float* hi, float* lo, int64_t n, cudaStream_t s);
+void split_transpose_tables(const double* at, float* hi, float* lo, int ld, int count);
+void m2l_tf32x3(const MixedMaps& maps, const MixedCall& c, cudaStream_t s);
+size_t m2l_tf32x3_smem();
+
+}  // namespace hfmm

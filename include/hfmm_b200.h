@@ -35,7 +35,9 @@ extern "C" {
 #define HFMM_ERR_DEVICE -5    /* a kernel raised its device error flag               */
 
 #define HFMM_PREC_FP64 0      /* plain path: every phase in float64                  */
-#define HFMM_PREC_MIXED 1     /* FP32 pair kernels, 3xTF32 M2L, FP64 final sums      */
+#define HFMM_PREC_MIXED 1     /* M2L + L2L as split 3xTF32 on tcgen05 (FP32 accumulate);
+                                 the other phases FP64. Needs p >= 6 (n_s >= 128);
+                                 smaller p runs the FP64 GEMM for that phase.          */
 
 typedef struct hfmm_plan hfmm_plan;
 
@@ -142,9 +144,9 @@ int hfmm_direct_noalloc(const double* pos_dev, const double* q_re_dev, const dou
  * per phase, summed over every evaluate since profiling was enabled or the
  * previous read (up to 8192 phase instances): 0 charge gather, 1 P2M, 2 M2M GEMM, 3 upward decode,
  * 4 M2L+L2L GEMM, 5 X-list P2L, 6 downward decode, 7 P2P, 8 L2P, 9 W-list M2P,
- * 10 combine. (Replaces the reference's wall-clock phase prints; it has no
+ * 10 combine, 11 TF32 splits of the mixed path. (Replaces the reference's wall-clock phase prints; it has no
  * per-phase timers, util.py:692-724.) */
-#define HFMM_N_PHASES 11
+#define HFMM_N_PHASES 12
 int hfmm_plan_set_profiling(hfmm_plan* plan, int32_t enable);
 int hfmm_plan_phase_times(hfmm_plan* plan, double* ms_out);
 

@@ -1,0 +1,59 @@
+"""The mixed-precision path (M2L + L2L as split 3xTF32 on tcgen05, FP32
+accumulation) against the plain FP64 path on the same plan and against the
+FP64 direct sum. Tolerances: mixed vs FP64 relative L2 below 2e-6 (TF32x3
+products carry ~2^-22 relative error); mixed vs direct sum no worse than the
+FP64 error plus 2e-6."""
+import numpy as np
+import pytest
+
+import oracle as O
+from cases import uniform, complex_uniform, sphere_clusters
+
+pytestmark = pytest.mark.gpu
+TOL_VS_FP64 = 2e-6
+
+
+def _both(st, q, field):
+    import hfmm_b200
+    if field:
+        a = hfmm_b200.evaluate_field(st, q, precision=hfmm_b200.PREC_FP64)
+        b = hfmm_b200.evaluate_field(st, q, precision=hfmm_b200.PREC_MIXED)
+    else:
+        a = (hfmm_b200.evaluate(st, q, precision=hfmm_b200.PREC_FP64),)
+        b = (hfmm_b200.evaluate(st, q, precision=hfmm_b200.PREC_MIXED),)
+    return a, b
+
+
+CASES = [
+    ("small_real", uniform, 3000, 3.0, 6, 32, None, False),
+    ("small_cplx_field", complex_uniform, 5000, 5.0, 6, 32, None, True),
+    ("c1_shape", complex_uniform, 20000, 2 * np.pi, 8, 64, None, True),
+    ("adaptive", sphere_clusters, 12000, 10.0, 6, 24, None, True),
+]
+
+
+@pytest.mark.parametrize("name,fn,n,k,p,nmax,md,field", CASES, ids=[c[0] for c in CASES])
+def test_mixed_against_fp64_and_direct(name, fn, n, k, p, nmax, md, field):
+    import hfmm_b200
+    pos, q = fn(n)
+    st = hfmm_b200.setup(pos, k, p=p, N_max=nmax, max_depth=md)
+    a, b = _both(st, q, field)
+    for x, y in zip(a, b):
+        assert np.isfinite(y).all()
+        assert O.relative_error(y, x) < TOL_VS_FP64
+    tg = np.random.default_rng(5).choice(n, min(n, 400), replace=False)
+    ref = O.direct(pos, q, k, tg)
+    e64 = O.relative_error(a[0][tg], ref)
+    emx = O.relative_error(b[0][tg], ref)
+    assert emx < e64 + TOL_VS_FP64, (e64, emx)
+
+
+def test_mixed_is_deterministic():
+    import torch
+    import hfmm_b200
+    pos, q = complex_uniform(8000)
+    st = hfmm_b200.setup(pos, 4.0, p=6, N_max=32)
+    qt = torch.as_tensor(q, device="cuda")
+    r1 = hfmm_b200.evaluate_field(st, qt, precision=hfmm_b200.PREC_MIXED)
+    r2 = hfmm_b200.evaluate_field(st, qt, precision=hfmm_b200.PREC_MIXED)
+    assert torch.equal(r1[0], r2[0]) and torch.equal(r1[1], r2[1])
