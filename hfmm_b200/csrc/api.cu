@@ -244,6 +244,14 @@ void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double*
     }
     EvalView v = view(P);
 
+    // Particle phases. On the mixed path only the near field runs in FP32: P2M and P2L
+    // feed the damped decodes and L2P/M2P read their output; for the sin component
+    // (eps_rel 1e-12) FP32 noise there is amplified along near-null singular
+    // directions, so those phases stay FP64.
+    auto particles = [&](const ParticlePass& p) {
+        if (mixed && p.op == ParticleOp::P2P) particles_mixed(p, s);
+        else particles_f64(p, s);
+    };
     ParticlePass base;
     base.v = v;
     base.nf = NF;
@@ -318,7 +326,7 @@ void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double*
         p.surf = P->check_pts.p;
         p.out = P->check.p;
         PhaseTimer pt(X, s, 1);
-        particles_f64(p, s);
+        particles(p);
     }
     for (int l = P->md; l >= 2; --l) {
         if (l < P->md)
@@ -372,7 +380,7 @@ void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double*
             p.out = P->check.p;
             p.level = l;
             PhaseTimer pt(X, s, 5);
-            particles_f64(p, s);
+            particles(p);
         }
         decode(l, false, P->check.p, P->loc.p);
     }
@@ -386,7 +394,7 @@ void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double*
         p.srcs = P->near_src.p;
         {
             PhaseTimer pt(X, s, 7);
-            particles_f64(p, s);
+            particles(p);
         }
         p = base;
         p.op = ParticleOp::L2P;
@@ -396,7 +404,7 @@ void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double*
         p.dens = P->loc.p;
         {
             PhaseTimer pt(X, s, 8);
-            particles_f64(p, s);
+            particles(p);
         }
         if (P->nW) {
             p = base;
@@ -408,7 +416,7 @@ void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double*
             p.surf = P->equiv_pts.p;
             p.dens = P->equiv.p;
             PhaseTimer pt(X, s, 9);
-            particles_f64(p, s);
+            particles(p);
         }
         p = base;
         p.op = ParticleOp::COMBINE;
@@ -416,7 +424,7 @@ void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double*
         p.phi = phi;
         p.E = E;
         PhaseTimer pt(X, s, 10);
-        particles_f64(p, s);
+        particles(p);
     }
 }
 

@@ -229,32 +229,48 @@ __global__ void __launch_bounds__(THREADS, 1) k_m2l_tf32x3(const __grid_constant
         // ---------------- B gathers (cp.async, manual SWIZZLE_128B placement)
         const float* Bh = c.Bhi + fs;
         const float* Bl = c.Blo + fs;
-        const float* Lh = c.Lhi ? c.Lhi + fs : nullptr;
-        const float* Ll = c.Llo ? c.Llo + fs : nullptr;
-        int pending = -1;
+        // Each thread always serves chunk ch of the same 8 rows (columns) of the B tile:
+        // rows n_i = (tid >> 3) + 16 i. Their swizzled shared-memory offsets are fixed;
+        // their global sources change only when the displacement entry changes.
+        const int ch = tid & 7;
+        uint32_t soff[8];
+        int64_t goff[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const int n = (tid >> 3) + 16 * i;
+            soff[i] = (uint32_t)((n >> 3) * 1024 + (n & 7) * 128 + ((ch ^ (n & 7)) << 4));
+            goff[i] = -1;
+        }
+        int pending = -1, cur_entry = -1;
         for (int q = 0; q < nq; ++q) {
             const int st = q % STAGES;
+            const int ai = q / kch;
+            if (ai != cur_entry) {   // new displacement entry: look up this thread's 8 sources
+                cur_entry = ai;
+                const int e = ctl.act[ai];
+#pragma unroll
+                for (int i = 0; i < 8; ++i) {
+                    const int n = (tid >> 3) + 16 * i;
+                    const int t = ctl.tgt[n / R];
+                    int s_ = -1;
+                    if (t >= 0) s_ = c.src_tab[(int64_t)t * M2L_ENTRIES + e];
+                    if (s_ >= c.nb) {
+                        atomicOr(c.err, ERRF_BOUNDS);
+                        s_ = -1;
+                    }
+                    goff[i] = s_ >= 0 ? ((int64_t)s_ * R + (n % R)) * c.ld + ch * 4 : -1;
+                }
+            }
             if (!mbar_wait(smem_u32(&ctl.empty[st]), ((q / STAGES) & 1) ^ 1, abort_flag)) break;
-            const int e = ctl.act[q / kch];
             const int k0 = (q % kch) * BK;
-            const bool l2l = e >= N_DISP;
-            const float* srch = l2l ? Lh : Bh;
-            const float* srcl = l2l ? Ll : Bl;
             const uint32_t sbh = smem_u32(sm + st * STAGE_BYTES + 2 * TILE_BYTES);
             const uint32_t sbl = sbh + TILE_BYTES;
-#pragma unroll 4
-            for (int idx = tid; idx < BN * 8; idx += 128) {
-                const int n = idx >> 3, ch = idx & 7;
-                const int j = n / R, r = n % R;
-                const int t = ctl.tgt[j];
-                int s = -1;
-                if (t >= 0) s = c.src_tab[(int64_t)t * M2L_ENTRIES + e];
-                bool ok = s >= 0 && s < c.nb && srch != nullptr;
-                if (s >= c.nb) atomicOr(c.err, ERRF_BOUNDS);
-                const int64_t off = ok ? ((int64_t)s * R + r) * c.ld + k0 + ch * 4 : 0;
-                const uint32_t so = (uint32_t)((n >> 3) * 1024 + (n & 7) * 128 + ((ch ^ (n & 7)) << 4));
-                cp_async16(sbh + so, ok ? (const void*)(srch + off) : (const void*)Bh, ok);
-                cp_async16(sbl + so, ok ? (const void*)(srcl + off) : (const void*)Bl, ok);
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                const bool ok = goff[i] >= 0;
+                const int64_t o = ok ? goff[i] + k0 : 0;
+                cp_async16(sbh + soff[i], Bh + o, ok);
+                cp_async16(sbl + soff[i], Bl + o, ok);
             }
             asm volatile("cp.async.commit_group;\n" ::);
             if (pending >= 0) {

@@ -41,6 +41,7 @@ struct ParticlePass {
 };
 
 void particles_f64(const ParticlePass& p, cudaStream_t s);
+void particles_mixed(const ParticlePass& p, cudaStream_t s);
 void gather_charges(int64_t n, const int32_t* sidx, const double* q_re, const double* q_im,
                     double* q_s, cudaStream_t s);
 

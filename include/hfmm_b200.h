@@ -35,9 +35,11 @@ extern "C" {
 #define HFMM_ERR_DEVICE -5    /* a kernel raised its device error flag               */
 
 #define HFMM_PREC_FP64 0      /* plain path: every phase in float64                  */
-#define HFMM_PREC_MIXED 1     /* M2L + L2L as split 3xTF32 on tcgen05 (FP32 accumulate);
-                                 the other phases FP64. Needs p >= 6 (n_s >= 128);
-                                 smaller p runs the FP64 GEMM for that phase.          */
+#define HFMM_PREC_MIXED 1     /* M2L as split 3xTF32 on tcgen05 (FP32 accumulation in
+                                 short chains, folded into FP64), P2P in FP32 with an
+                                 FP64 phase reduction; decodes, M2M, L2L, P2M, L2P FP64.
+                                 M2L needs p >= 6 (n_s >= 128); smaller p runs its FP64
+                                 GEMM.                                                 */
 
 typedef struct hfmm_plan hfmm_plan;
 
