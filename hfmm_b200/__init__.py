@@ -20,9 +20,10 @@ import torch
 
 from . import _lib
 from ._lib import check as _check, HFMMError, launch_count
-from .operators import level_tables, surface_pts, R_EQUIV, R_CHECK, n_surf
+from .operators import level_tables, level_decodes, surface_pts, R_EQUIV, R_CHECK, n_surf
 
-__all__ = ["setup", "evaluate", "evaluate_field", "evaluate_into", "direct", "HFMMState",
+__all__ = ["setup", "evaluate", "evaluate_field", "evaluate_into", "direct", "direct_at",
+           "HFMMState",
            "HFMMError", "launch_count", "PREC_FP64", "PREC_MIXED"]
 
 PREC_FP64 = _lib.HFMM_PREC_FP64
@@ -128,13 +129,18 @@ def _validate_setup(positions, k, p, N_max, max_depth):
     return x, kf
 
 
-def setup(positions, k, p=4, N_max=16, max_depth=None, device=None):
+def setup(positions, k, p=4, N_max=16, max_depth=None, device=None, tables="device"):
     """Build the plan for ``positions`` and wavenumber ``k`` (HFMM.setup, HFMM.py:55-80).
 
     ``p`` is the number of surface points per cube edge, ``N_max`` the leaf
     size and ``max_depth`` an optional depth cap (``None``: the reference's
     automatic depth with refinement, trees/cubic.py:577-600).
+    ``tables``: "device" evaluates the M2M/L2L/M2L kernel matrices on the GPU
+    (the decodes still come from the host SVD); "host" assembles every table in
+    NumPy with the reference's expressions, bit for bit.
     """
+    if tables not in ("device", "host"):
+        raise ValueError('tables must be "device" or "host"')
     x, kf = _validate_setup(positions, k, p, N_max, max_depth)
     dev = _device(device)
     with torch.cuda.device(dev):
@@ -145,7 +151,7 @@ def setup(positions, k, p=4, N_max=16, max_depth=None, device=None):
                                         _lib.ctypes.byref(h)))
         state = HFMMState(h.value, pos, kf, p, N_max, dev)
         try:
-            _load_tables(state)
+            _load_tables(state, tables)
             _check(_lib.lib.hfmm_plan_finalize(state.handle))
         except Exception:
             state.close()
@@ -154,7 +160,7 @@ def setup(positions, k, p=4, N_max=16, max_depth=None, device=None):
     return state
 
 
-def _load_tables(state):
+def _load_tables(state, mode="device"):
     p, md = state.p, state.max_depth
     extent = state.info["domain_extent"]
     eq = np.ascontiguousarray(surface_pts(p, R_EQUIV))
@@ -164,6 +170,14 @@ def _load_tables(state):
     for fam in range(state.n_families):
         eps_rel = 1e-7 if fam == 0 else 1e-12          # HFMM.py:75-77
         for level in range(2, md + 1):
+            if mode == "device":
+                t = level_decodes(p, level, extent, state.k, fam == 1, eps_rel)
+                arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in
+                        (t["F_up"][0], t["F_up"][1], t["F_up"][2], t["F_dn"][0], t["F_dn"][1],
+                         t["F_dn"][2])]
+                _check(_lib.lib.hfmm_plan_set_level_decode(state.handle, fam, level,
+                                                           *[a.ctypes.data for a in arrs]))
+                continue
             t = level_tables(p, level, md, extent, state.k, fam == 1, eps_rel)
             arrs = [t["F_up"][0], t["F_up"][1], t["F_up"][2], t["F_dn"][0], t["F_dn"][1],
                     t["F_dn"][2], t["M2M_K"], t["L2L_K"], t["M2L_K"]]
@@ -237,6 +251,22 @@ def evaluate_field(state, charges, precision=PREC_FP64):
     """Potential and field E = -grad(phi) for real or complex charges (N,).
     Returns (phi (N,), E (N, 3)), both complex128."""
     return _run(state, charges, complex_ok=True, field=True, precision=precision)
+
+
+def direct_at(state, q_re, q_im, targets, field=False, stream=None):
+    """Device form of ``direct``: float64 charge tensors (``q_im`` may be None) and
+    int32 target indices, all on the plan's device; returns device tensors
+    (phi (T,), E (T, 3) or None)."""
+    m = targets.shape[0]
+    dev = state.device
+    phi = torch.empty(m, dtype=torch.complex128, device=dev)
+    E = torch.empty((m, 3), dtype=torch.complex128, device=dev) if field else None
+    s = stream if stream is not None else torch.cuda.current_stream(dev)
+    _check(_lib.lib.hfmm_direct(state.positions.data_ptr(), q_re.data_ptr(),
+                                None if q_im is None else q_im.data_ptr(), state.n,
+                                targets.data_ptr(), m, state.k, phi.data_ptr(),
+                                None if E is None else E.data_ptr(), s.cuda_stream))
+    return phi, E
 
 
 def direct(state, charges, targets, field=False):

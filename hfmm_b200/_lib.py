@@ -48,6 +48,7 @@ SIGNATURES = [
     ("hfmm_plan_info", _c_i32, [_c_vp, ctypes.POINTER(HfmmInfo)]),
     ("hfmm_plan_set_kernel", _c_i32, [_c_vp, _c_dbl, _c_i32, _c_i32, _c_vp, _c_vp]),
     ("hfmm_plan_set_level", _c_i32, [_c_vp, _c_i32, _c_i32] + [_c_vp] * 9),
+    ("hfmm_plan_set_level_decode", _c_i32, [_c_vp, _c_i32, _c_i32] + [_c_vp] * 6),
     ("hfmm_plan_finalize", _c_i32, [_c_vp]),
     ("hfmm_evaluate", _c_i32, [_c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_i32, _c_vp]),
     ("hfmm_plan_check", _c_i32, [_c_vp, _c_vp]),
@@ -61,6 +62,12 @@ SIGNATURES = [
                                      _c_vp, _c_vp]),
     ("hfmm_plan_set_profiling", _c_i32, [_c_vp, _c_i32]),
     ("hfmm_plan_phase_times", _c_i32, [_c_vp, _c_vp]),
+    ("hfmm_mlp_param_count", _c_i32, [_c_i32, _c_i32]),
+    ("hfmm_mlp_forward", _c_i32, [_c_vp, _c_vp, _c_i32, _c_i32, _c_i32, _c_vp, _c_vp]),
+    ("hfmm_mlp_grad", _c_i32, [_c_vp, _c_vp, _c_vp, _c_i32, _c_i32, _c_i32, _c_vp,
+                               ctypes.POINTER(_c_dbl), _c_vp]),
+    ("hfmm_mlp_train", _c_i32, [_c_vp, _c_vp, _c_vp, _c_i64, _c_vp, _c_vp, _c_i32, _c_i32, _c_i32,
+                                _c_i32, ctypes.c_float, ctypes.POINTER(_c_dbl), _c_vp]),
     ("hfmm_last_error", ctypes.c_char_p, []),
     ("hfmm_launch_count", _c_i64, []),
 ]

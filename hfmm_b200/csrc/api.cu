@@ -223,6 +223,11 @@ void upload_level(hfmm_plan* P, int fam, int l, const double* const* h) {
     relayout(h[3], 1, none, n_s, ld, false, T.dn_U);
     upload_vec(h[4], n_s, ld, T.dn_d);
     relayout(h[5], 1, none, n_s, ld, false, T.dn_Vt);
+    if (!h[8]) {   // kernel matrices generated on the device
+        generate_tables(P, fam, l);
+        T.set = true;
+        return;
+    }
     if (h[6] && l < P->md) relayout(h[6], 8, none, n_s, ld, true, T.m2m);
     else T.m2m.release();
     if (h[7] && l >= 3) relayout(h[7], 8, none, n_s, ld, true, T.l2l);
@@ -551,6 +556,23 @@ int hfmm_plan_set_level(hfmm_plan* P, int32_t family, int32_t level, const doubl
     if (level >= 3 && !L2L_K) return fail(HFMM_ERR_ARG, "L2L_K required from level 3");
     API_BEGIN
     const double* h[9] = {F_up_U, F_up_d, F_up_Vt, F_dn_U, F_dn_d, F_dn_Vt, M2M_K, L2L_K, M2L_K};
+    upload_level(P, family, level, h);
+    P->finalized = false;
+    return HFMM_OK;
+    API_END
+}
+
+int hfmm_plan_set_level_decode(hfmm_plan* P, int32_t family, int32_t level, const double* F_up_U,
+                               const double* F_up_d, const double* F_up_Vt, const double* F_dn_U,
+                               const double* F_dn_d, const double* F_dn_Vt) {
+    if (!P) return fail(HFMM_ERR_ARG, "plan is NULL");
+    if (P->n_s == 0) return fail(HFMM_ERR_STATE, "set the kernel first");
+    if (family < 0 || family >= P->n_fam) return fail(HFMM_ERR_ARG, "family out of range");
+    if (level < 2 || level > P->md) return fail(HFMM_ERR_ARG, "level must be in [2, max_depth]");
+    if (!F_up_U || !F_up_d || !F_up_Vt || !F_dn_U || !F_dn_d || !F_dn_Vt)
+        return fail(HFMM_ERR_ARG, "decode factors are required");
+    API_BEGIN
+    const double* h[9] = {F_up_U, F_up_d, F_up_Vt, F_dn_U, F_dn_d, F_dn_Vt, nullptr, nullptr, nullptr};
     upload_level(P, family, level, h);
     P->finalized = false;
     return HFMM_OK;

@@ -179,6 +179,7 @@ void tree_build(hfmm_plan* P, const double* pos_dev);
 void lists_build(hfmm_plan* P);
 void schedules_build(hfmm_plan* P);
 void upload_level(hfmm_plan* P, int fam, int level, const double* const* h);
+void generate_tables(hfmm_plan* P, int fam, int level);
 void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double* phi,
                    double* fld, cudaStream_t s, bool mixed = false);
 void direct_sum(const double* pos, const double* q_re, const double* q_im, int64_t n,

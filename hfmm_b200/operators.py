@@ -69,6 +69,18 @@ def level_scale(domain_extent, level):
     return float(domain_extent) * 0.5 ** (level + 1)
 
 
+def level_decodes(p, level, domain_extent, k, imaginary, eps_rel):
+    """Only the two damped-SVD decodes of one family at one level (the kernel matrices
+    are then generated on the device, hfmm_plan_set_level_decode)."""
+    G = component_matrix(k, imaginary)
+    equiv = surface_pts(p, R_EQUIV)
+    check = surface_pts(p, R_CHECK)
+    s = level_scale(domain_extent, level)
+    F_up = damped_factors(G(check * s, equiv * s), eps_rel)
+    F_dn = damped_factors(G(equiv * s, check * s), eps_rel)
+    return dict(F_up=F_up, F_dn=F_dn)
+
+
 def level_tables(p, level, max_depth, domain_extent, k, imaginary, eps_rel):
     """Tables of one kernel family at one level, in the layout hfmm_plan_set_level takes."""
     G = component_matrix(k, imaginary)

@@ -90,6 +90,14 @@ int hfmm_plan_set_level(hfmm_plan* plan, int32_t family, int32_t level,
                         const double* F_dn_U, const double* F_dn_d, const double* F_dn_Vt,
                         const double* M2M_K, const double* L2L_K, const double* M2L_K);
 
+/* Same as hfmm_plan_set_level, but only the damped-SVD decode factors come from
+ * the host: the M2M, L2L and M2L kernel matrices (operators.py:363-403) are
+ * evaluated on the device from the surfaces, k and the level scale. Entries agree
+ * with the host NumPy tables to rounding (CUDA sincos vs the host libm). */
+int hfmm_plan_set_level_decode(hfmm_plan* plan, int32_t family, int32_t level,
+                               const double* F_up_U, const double* F_up_d, const double* F_up_Vt,
+                               const double* F_dn_U, const double* F_dn_d, const double* F_dn_Vt);
+
 /* Build the V, U, W, X lists and the evaluate schedules on the device
  * (trees/lists.py:818-931, core.py:119-140). */
 int hfmm_plan_finalize(hfmm_plan* plan);
@@ -151,6 +159,27 @@ int hfmm_direct_noalloc(const double* pos_dev, const double* q_re_dev, const dou
 #define HFMM_N_PHASES 12
 int hfmm_plan_set_profiling(hfmm_plan* plan, int32_t enable);
 int hfmm_plan_phase_times(hfmm_plan* plan, double* ms_out);
+
+/* ---- expansion-order network (no counterpart in the reference) ---- */
+/* A 3 x 64 FP32 MLP (tanh hidden layers, linear output) over in_dim features
+ * with out_dim outputs. Parameters are one flat device FP32 array of
+ * hfmm_mlp_param_count(in_dim, out_dim) floats: W1[in][64] b1[64] W2[64][64] b2[64]
+ * W3[64][64] b3[64] W4[64][out] b4[out]. X is (n, in_dim), targets/outputs
+ * (n, out_dim), all row-major on the device. Loss = mean squared error over
+ * samples and outputs. in_dim 1..64, out_dim 1..4. It picks the expansion order
+ * that the reference takes from the caller (HFMM.py:55-80). */
+int hfmm_mlp_param_count(int32_t in_dim, int32_t out_dim);
+int hfmm_mlp_forward(const float* params_dev, const float* X_dev, int32_t n, int32_t in_dim,
+                     int32_t out_dim, float* Y_dev, void* stream);
+/* Full-batch gradient of the loss (written to grad_dev) and the loss itself. Synchronises. */
+int hfmm_mlp_grad(const float* params_dev, const float* X_dev, const float* T_dev, int32_t n,
+                  int32_t in_dim, int32_t out_dim, float* grad_dev, double* loss, void* stream);
+/* `steps` full-batch Adam steps (b1 0.9, b2 0.999, eps 1e-8) continuing from
+ * step number step0 with the moment arrays adam_m/adam_v (param_count floats
+ * each, zero at step0 = 0); *loss is the loss after the last step. Synchronises. */
+int hfmm_mlp_train(float* params_dev, float* adam_m_dev, float* adam_v_dev, int64_t step0,
+                   const float* X_dev, const float* T_dev, int32_t n, int32_t in_dim,
+                   int32_t out_dim, int32_t steps, float lr, double* loss, void* stream);
 
 /* ---- diagnostics ---- */
 const char* hfmm_last_error(void);
