@@ -1,0 +1,312 @@
+"""Learned expansion order and leaf size, certified against a sampled direct sum.
+
+The reference takes ``p`` and ``N_max`` from the caller (HFMM.py:55-80) and
+never checks the result. Here a 3 x 64 FP32 network (the CUDA kernels of
+``csrc/mlp.cu``) reads features of the problem's tree and predicts
+
+* output 0: the smallest expansion order ``p`` (surface points per cube edge)
+  whose evaluate meets the requested tolerance, as a real number;
+* output 1: log2 of the fastest leaf size ``N_max`` (16..128, automatic depth).
+
+Features (``features``) are: log10(tol), k times the domain extent, log2 N,
+the depth, k times the box size at levels 2..7 (0 where the tree is shallower),
+the fraction of boxes on levels 2..7, and an 8-bin histogram of leaf occupancy
+relative to ``N_max`` -- all from the tree that ``hfmm_tree_build`` makes, so
+no operator table is built before ``p`` is known.
+
+``AutoPlan`` is the certified front door (the design precedent is the
+reference's Laplace-only tune.AutoEvaluator, jaxfmm/tune.py:375-516): every
+evaluate checks ``n_check`` random targets against the FP64 direct sum on the
+GPU (the referee of test.py:11-18) and, when the relative L2 error of the
+potential misses the tolerance, reruns with the plain conservative order in
+FP64, stepping ``p`` up by 2 while the check still fails.
+"""
+import math
+import os
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import check as _check
+
+N_FEATURES = 24
+N_OUTPUTS = 2
+P_MIN, P_MAX = 4, 16
+LEAVES = (16, 32, 64, 128)
+FEATURE_LEAF = 64          # the tree the features are read from
+TOL_MIXED = 1e-6           # the mixed-precision path is used at tolerances >= this
+DEFAULT_WEIGHTS = os.path.join(os.path.dirname(__file__), "data", "order_net.npz")
+
+
+def conservative_p(tol):
+    """The plain order: two surface points per edge for each decade of tolerance,
+    clamped to [4, 16] (1e-6 -> 12, the order of the plain path's 1M-point config)."""
+    return int(min(P_MAX, max(P_MIN, math.ceil(-2.0 * math.log10(tol)))))
+
+
+def precision_for(tol, p):
+    from . import PREC_FP64, PREC_MIXED
+    return PREC_MIXED if (tol >= TOL_MIXED and p >= 5) else PREC_FP64
+
+
+def tree_features(tree, info, k, tol, n_max=FEATURE_LEAF):
+    """Feature vector (float32, N_FEATURES) from exported tree arrays and plan info."""
+    lv = np.asarray(tree["lvls"])
+    cnt = np.asarray(tree["counts"])
+    leaf = np.asarray(tree["is_leaf"]).astype(bool)
+    md = int(info["max_depth"])
+    D = float(info["domain_extent"])
+    n = int(cnt[lv == 0].sum()) if np.any(lv == 0) else int(cnt[leaf].sum())
+    f = np.zeros(N_FEATURES, np.float64)
+    f[0] = math.log10(tol)
+    f[1] = k * D
+    f[2] = math.log2(max(n, 1))
+    f[3] = md
+    for j, l in enumerate(range(2, 8)):
+        if l <= md:
+            f[4 + j] = k * D * 0.5 ** (l + 1)
+        f[10 + j] = np.count_nonzero(lv == l) / max(len(lv), 1)
+    occ = cnt[leaf & (cnt > 0)] / float(n_max)
+    if occ.size:
+        h = np.histogram(np.minimum(occ, 0.999999), bins=8, range=(0.0, 1.0))[0]
+        f[16:24] = h / occ.size
+    return f.astype(np.float32)
+
+
+def features_for(positions, k, tol, device=None):
+    """Build the feature tree for ``positions`` on the GPU and return its features."""
+    from . import _validate_setup, _device, HFMMState
+    x, kf = _validate_setup(positions, k, 4, FEATURE_LEAF, None)
+    dev = _device(device)
+    with torch.cuda.device(dev):
+        pos = torch.as_tensor(x, dtype=torch.float64).to(dev).contiguous()
+        h = _lib.ctypes.c_void_p()
+        _check(_lib.lib.hfmm_tree_build(pos.data_ptr(), pos.shape[0], FEATURE_LEAF, 0,
+                                        _lib.ctypes.byref(h)))
+        st = HFMMState(h.value, pos, kf, 4, FEATURE_LEAF, dev)
+        try:
+            return tree_features(st.tree(), st.info, kf, tol)
+        finally:
+            st.close()
+
+
+def label_p(ps, errs, tol):
+    """Smallest (fractional) p from which every swept order meets ``tol``.
+
+    ``errs[i]`` is the error at ``ps[i]`` (ascending). Between the last miss and
+    the first hit the crossing is interpolated linearly in log10(error); when no
+    order meets ``tol`` the label is ``ps[-1] + 1``.
+    """
+    ps = np.asarray(ps, np.float64)
+    e = np.asarray(errs, np.float64)
+    ok = np.isfinite(e) & (e <= tol)
+    if not ok[-1]:
+        return float(ps[-1] + 1)
+    i = len(ok) - 1
+    while i > 0 and ok[i - 1]:
+        i -= 1
+    if i == 0:
+        return float(ps[0])
+    if not np.isfinite(e[i - 1]):         # the order below was not run (no crossing to read)
+        return float(ps[i])
+    la, lb, lt = math.log10(max(e[i - 1], 1e-300)), math.log10(max(e[i], 1e-300)), math.log10(tol)
+    t = (la - lt) / (la - lb) if la != lb else 1.0
+    return float(ps[i - 1] + min(max(t, 0.0), 1.0) * (ps[i] - ps[i - 1]))
+
+
+class OrderNet:
+    """The 3 x 64 network with its feature normalisation, on one GPU.
+
+    ``params`` is the flat FP32 parameter vector (layout of hfmm_mlp_param_count);
+    ``mu``/``sd`` normalise the features, ``t_mu``/``t_sd`` the targets.
+    """
+
+    def __init__(self, params, mu, sd, t_mu, t_sd, device=None):
+        from . import _device
+        self.device = _device(device)
+        n = _lib.lib.hfmm_mlp_param_count(N_FEATURES, N_OUTPUTS)
+        _check(min(n, 0))
+        if len(params) != n:
+            raise ValueError(f"expected {n} parameters, got {len(params)}")
+        self.params = torch.as_tensor(np.asarray(params, np.float32)).to(self.device)
+        self.mu = np.asarray(mu, np.float32)
+        self.sd = np.asarray(sd, np.float32)
+        self.t_mu = np.asarray(t_mu, np.float32)
+        self.t_sd = np.asarray(t_sd, np.float32)
+        self.m = torch.zeros_like(self.params)
+        self.v = torch.zeros_like(self.params)
+        self.step = 0
+
+    @classmethod
+    def init(cls, X, T, seed=0, device=None):
+        """Fresh network (Glorot-uniform weights, zero biases) normalised to the data."""
+        rng = np.random.default_rng(seed)
+        parts = []
+        for fan_in, fan_out in ((N_FEATURES, 64), (64, 64), (64, 64), (64, N_OUTPUTS)):
+            lim = math.sqrt(6.0 / (fan_in + fan_out))
+            parts += [rng.uniform(-lim, lim, fan_in * fan_out), np.zeros(fan_out)]
+        X = np.asarray(X, np.float64)
+        T = np.asarray(T, np.float64).reshape(len(X), N_OUTPUTS)
+        sd = X.std(0)
+        sd[sd < 1e-6] = 1.0
+        tsd = T.std(0)
+        tsd[tsd < 1e-6] = 1.0
+        return cls(np.concatenate(parts), X.mean(0), sd, T.mean(0), tsd, device)
+
+    @classmethod
+    def load(cls, path=DEFAULT_WEIGHTS, device=None):
+        z = np.load(path)
+        return cls(z["params"], z["mu"], z["sd"], z["t_mu"], z["t_sd"], device)
+
+    def save(self, path, **extra):
+        np.savez(path, params=self.params.cpu().numpy(), mu=self.mu, sd=self.sd, t_mu=self.t_mu,
+                 t_sd=self.t_sd, **extra)
+
+    def _x(self, X):
+        X = (np.asarray(X, np.float32).reshape(-1, N_FEATURES) - self.mu) / self.sd
+        return torch.as_tensor(np.ascontiguousarray(X, np.float32)).to(self.device)
+
+    def _t(self, T):
+        T = (np.asarray(T, np.float32).reshape(-1, N_OUTPUTS) - self.t_mu) / self.t_sd
+        return torch.as_tensor(np.ascontiguousarray(T, np.float32)).to(self.device)
+
+    def predict(self, X):
+        """(n, 2) outputs in target units: fractional p and log2 of the leaf size."""
+        x = self._x(X)
+        y = torch.empty((x.shape[0], N_OUTPUTS), dtype=torch.float32, device=self.device)
+        s = torch.cuda.current_stream(self.device)
+        with torch.cuda.device(self.device):
+            _check(_lib.lib.hfmm_mlp_forward(self.params.data_ptr(), x.data_ptr(), x.shape[0],
+                                             N_FEATURES, N_OUTPUTS, y.data_ptr(), s.cuda_stream))
+        return y.cpu().numpy() * self.t_sd + self.t_mu
+
+    def train(self, X, T, steps, lr=1e-3):
+        """Full-batch Adam on the GPU; returns the normalised loss after the last step."""
+        x, t = self._x(X), self._t(T)
+        loss = _lib.ctypes.c_double()
+        s = torch.cuda.current_stream(self.device)
+        with torch.cuda.device(self.device):
+            _check(_lib.lib.hfmm_mlp_train(self.params.data_ptr(), self.m.data_ptr(),
+                                           self.v.data_ptr(), self.step, x.data_ptr(),
+                                           t.data_ptr(), x.shape[0], N_FEATURES, N_OUTPUTS,
+                                           int(steps), float(lr), _lib.ctypes.byref(loss),
+                                           s.cuda_stream))
+        self.step += int(steps)
+        return loss.value
+
+    def choose(self, feats, margin=0.5):
+        """(p, N_max) for one feature vector: p rounded up after adding ``margin``."""
+        y = self.predict(feats)[0]
+        p = int(min(P_MAX, max(P_MIN, math.ceil(float(y[0]) + margin))))
+        leaf = int(2 ** min(7, max(4, round(float(y[1])))))
+        return p, leaf
+
+
+def _rel_l2(a, b):
+    a = np.asarray(a).reshape(len(b), -1)
+    b = np.asarray(b).reshape(len(b), -1)
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+class AutoPlan:
+    """Certified evaluate at a requested tolerance (one-knob front door).
+
+    ``net``: an OrderNet, None for the bundled weights, or False for the
+    conservative order in place of the network's (the ablation: the same
+    precision rule, leaf size and certification, only the network removed). ``n_check`` random
+    targets (seeded) are compared against the FP64 direct sum on every evaluate.
+    After a call, ``report`` holds the order, leaf, precision, measured error and
+    whether the plain rerun was taken.
+    """
+
+    def __init__(self, positions, k, tol=1e-6, net=None, n_check=256, seed=0, device=None,
+                 margin=0.5):
+        from . import setup, _device
+        if not (0 < tol < 1):
+            raise ValueError("tol must be in (0, 1)")
+        self.tol = float(tol)
+        self.k = float(k)
+        self.device = _device(device)
+        self.positions = positions
+        self.p_plain = conservative_p(self.tol)
+        if net is False:
+            self.p, self.leaf, self.feats = self.p_plain, FEATURE_LEAF, None
+        else:
+            net = OrderNet.load(device=self.device) if net is None else net
+            self.feats = features_for(positions, k, tol, self.device)
+            self.p, self.leaf = net.choose(self.feats, margin)
+        self.precision = precision_for(self.tol, self.p)
+        self.state = setup(positions, k, p=self.p, N_max=self.leaf, device=self.device)
+        rng = np.random.default_rng(seed)
+        n = self.state.n
+        self.check_idx = np.sort(rng.choice(n, size=min(n_check, n), replace=False)).astype(np.int32)
+        self._check_dev = torch.as_tensor(self.check_idx).to(self.device)
+        self._plain = {}
+        self.report = {}
+
+    def _direct(self, q_re, q_im, field):
+        """FP64 direct sum at the check targets (device tensors in, NumPy out)."""
+        from . import direct_at
+        phi, E = direct_at(self.state, q_re, q_im, self._check_dev, field)
+        return phi.cpu().numpy(), (E.cpu().numpy() if field else None)
+
+    def _error(self, phi, E, ref):
+        i = self._check_dev
+        err = _rel_l2(phi[i].cpu().numpy(), ref[0])
+        if E is not None:
+            err = max(err, _rel_l2(E[i].cpu().numpy(), ref[1]))
+        return err
+
+    def _plain_state(self, p):
+        from . import setup
+        if p not in self._plain:
+            self._plain[p] = setup(self.positions, self.k, p=p, N_max=FEATURE_LEAF,
+                                   device=self.device)
+        return self._plain[p]
+
+    def evaluate_field(self, charges, field=True):
+        """Certified (phi, E) (E is None with field=False); complex or real charges (N,).
+
+        The error checked is the relative L2 error over the check targets of the
+        potential, and of the field when it is computed (the larger of the two)."""
+        from . import evaluate_into, check_errors, PREC_FP64
+        numpy_in = not isinstance(charges, torch.Tensor)
+        dev = self.device
+        with torch.cuda.device(dev):
+            q = torch.as_tensor(np.asarray(charges)).to(dev) if numpy_in else charges.to(dev)
+            if q.is_complex():
+                q_re, q_im = q.real.double().contiguous(), q.imag.double().contiguous()
+            else:
+                q_re, q_im = q.double().contiguous(), None
+            n = self.state.n
+            phi = torch.empty(n, dtype=torch.complex128, device=dev)
+            E = torch.empty((n, 3), dtype=torch.complex128, device=dev) if field else None
+            evaluate_into(self.state, q_re, q_im, phi, E, self.precision)
+            check_errors(self.state)
+            ref = self._direct(q_re, q_im, field)
+            err = self._error(phi, E, ref)
+            rep = dict(p=self.p, leaf=self.leaf, precision=int(self.precision), error=err,
+                       fallback=False, p_final=self.p)
+            p = self.p_plain
+            while err > self.tol and p <= P_MAX:
+                st = self._plain_state(p)
+                evaluate_into(st, q_re, q_im, phi, E, PREC_FP64)
+                check_errors(st)
+                err = self._error(phi, E, ref)
+                rep.update(fallback=True, p_final=p, error=err, precision=int(PREC_FP64))
+                p += 2
+            rep["certified"] = bool(err <= self.tol)
+            self.report = rep
+        if numpy_in:
+            return phi.cpu().numpy(), (E.cpu().numpy() if E is not None else None)
+        return phi, E
+
+    def evaluate(self, charges):
+        return self.evaluate_field(charges, field=False)[0]
+
+    def close(self):
+        self.state.close()
+        for st in self._plain.values():
+            st.close()
+        self._plain.clear()

@@ -1,0 +1,120 @@
+"""The expansion-order network's CUDA kernels against the NumPy oracle, and the
+certified auto-plan (check on sampled targets, plain rerun on a miss)."""
+import numpy as np
+import pytest
+import torch
+
+from oracle import mlp as om
+
+pytestmark = pytest.mark.gpu
+
+N_IN, N_OUT = 24, 2
+
+
+def _dev(a):
+    return torch.as_tensor(np.ascontiguousarray(a, np.float32)).cuda()
+
+
+def _data(n=300, seed=0):
+    rng = np.random.default_rng(seed)
+    X = rng.normal(size=(n, N_IN)).astype(np.float32)
+    T = np.stack([X[:, 0] - 0.5 * X[:, 3] * X[:, 5], np.tanh(X[:, 1] + X[:, 2])], 1)
+    P = rng.normal(0, 0.2, om.param_count(N_IN, N_OUT)).astype(np.float32)
+    return P, X, T.astype(np.float32)
+
+
+def _rel(a, b):
+    return float(np.linalg.norm(np.asarray(a, np.float64) - b) / np.linalg.norm(b))
+
+
+def test_forward_matches_oracle():
+    from hfmm_b200 import _lib
+    P, X, _ = _data()
+    Y = torch.empty((len(X), N_OUT), dtype=torch.float32, device="cuda")
+    assert _lib.lib.hfmm_mlp_forward(_dev(P).data_ptr(), _dev(X).data_ptr(), len(X), N_IN, N_OUT,
+                                     Y.data_ptr(), None) == 0
+    ref, _ = om.forward(P.astype(np.float64), X, N_OUT)
+    assert _rel(Y.cpu().numpy(), ref) < 1e-5
+
+
+@pytest.mark.parametrize("n", [1, 300, 4097])
+def test_gradient_matches_oracle(n):
+    from hfmm_b200 import _lib
+    P, X, T = _data(n, seed=n)
+    G = torch.empty(len(P), dtype=torch.float32, device="cuda")
+    loss = _lib.ctypes.c_double()
+    assert _lib.lib.hfmm_mlp_grad(_dev(P).data_ptr(), _dev(X).data_ptr(), _dev(T).data_ptr(), n,
+                                  N_IN, N_OUT, G.data_ptr(), _lib.ctypes.byref(loss), None) == 0
+    l_ref, g_ref = om.loss_grad(P.astype(np.float64), X, T, N_OUT)
+    assert loss.value == pytest.approx(l_ref, rel=1e-5)
+    assert _rel(G.cpu().numpy(), g_ref) < 1e-4
+
+
+def test_adam_steps_match_oracle():
+    from hfmm_b200 import _lib
+    P, X, T = _data(256, seed=3)
+    p, m, v = _dev(P), torch.zeros(len(P), device="cuda"), torch.zeros(len(P), device="cuda")
+    loss = _lib.ctypes.c_double()
+    for t0 in (0, 3):           # two calls continue one optimiser run
+        assert _lib.lib.hfmm_mlp_train(p.data_ptr(), m.data_ptr(), v.data_ptr(), t0,
+                                       _dev(X).data_ptr(), _dev(T).data_ptr(), len(X), N_IN, N_OUT,
+                                       3, 1e-3, _lib.ctypes.byref(loss), None) == 0
+    P_ref, m_ref, _, l_ref = om.adam(P.astype(np.float64), X, T, N_OUT, steps=6, lr=1e-3)
+    got = p.cpu().numpy()
+    assert _rel(got, P_ref) < 1e-5
+    # the update itself: a few parameters with near-zero gradients may take the other sign
+    assert _rel(got - P, P_ref - P) < 2e-2
+    assert _rel(m.cpu().numpy(), m_ref) < 1e-3
+    assert loss.value == pytest.approx(l_ref, rel=1e-3)
+
+
+def test_training_on_gpu_fits():
+    from hfmm_b200.learned import OrderNet
+    _, X, T = _data(512, seed=4)
+    net = OrderNet.init(X, T, seed=0, device="cuda")
+    y0 = net.predict(X)
+    l0 = float(np.mean(((y0 - T) / net.t_sd) ** 2))
+    l1 = net.train(X, T, steps=1500, lr=3e-3)
+    assert l1 < 0.1 * l0
+    y1 = net.predict(X)
+    assert float(np.mean(((y1 - T) / net.t_sd) ** 2)) == pytest.approx(l1, rel=1e-3)
+
+
+def _problem(n=6000, seed=0):
+    rng = np.random.default_rng(seed)
+    x = rng.random((n, 3))
+    q = rng.standard_normal(n) + 1j * rng.standard_normal(n)
+    return x, q
+
+
+def test_auto_plan_conservative_certifies():
+    from hfmm_b200.learned import AutoPlan
+    x, q = _problem()
+    ap = AutoPlan(x, 6.0, tol=1e-5, net=False)
+    phi, E = ap.evaluate_field(q)
+    assert ap.report["certified"] and not ap.report["fallback"]
+    assert ap.report["p"] == 10 and ap.report["error"] <= 1e-5
+    assert phi.shape == (len(x),) and E.shape == (len(x), 3)
+    ap.close()
+
+
+def test_auto_plan_reruns_plainly_on_a_miss():
+    """A network that asks for the lowest order misses 1e-7; the plain rerun certifies."""
+    from hfmm_b200.learned import AutoPlan, OrderNet, N_FEATURES, N_OUTPUTS
+    import hfmm_b200 as hf
+    net = OrderNet(np.zeros(om.param_count(N_FEATURES, N_OUTPUTS), np.float32),
+                   np.zeros(N_FEATURES), np.ones(N_FEATURES), np.array([2.0, 6.0]),
+                   np.ones(2), device="cuda")
+    x, q = _problem(seed=1)
+    ap = AutoPlan(x, 4.0, tol=1e-7, net=net)
+    assert ap.p == 4 and ap.leaf == 64
+    phi = ap.evaluate(q)
+    rep = ap.report
+    assert rep["fallback"] and rep["certified"] and rep["p_final"] >= 14
+    assert rep["precision"] == hf.PREC_FP64
+    # the returned potential is the plain evaluate's, checked on other targets too
+    st = hf.setup(x, 4.0, p=rep["p_final"], N_max=64)
+    ref = hf.evaluate_field(st, q)[0]
+    assert np.linalg.norm(phi - ref) <= 1e-13 * np.linalg.norm(ref)
+    st.close()
+    ap.close()
