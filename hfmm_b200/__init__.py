@@ -129,7 +129,8 @@ def _validate_setup(positions, k, p, N_max, max_depth):
     return x, kf
 
 
-def setup(positions, k, p=4, N_max=16, max_depth=None, device=None, tables="device"):
+def setup(positions, k, p=4, N_max=16, max_depth=None, device=None, tables="device",
+          stream_tables=False):
     """Build the plan for ``positions`` and wavenumber ``k`` (HFMM.setup, HFMM.py:55-80).
 
     ``p`` is the number of surface points per cube edge, ``N_max`` the leaf
@@ -138,9 +139,14 @@ def setup(positions, k, p=4, N_max=16, max_depth=None, device=None, tables="devi
     ``tables``: "device" evaluates the M2M/L2L/M2L kernel matrices on the GPU
     (the decodes still come from the host SVD); "host" assembles every table in
     NumPy with the reference's expressions, bit for bit.
+    ``stream_tables``: keep no M2L table resident; each evaluate regenerates a
+    level's 316 M2L matrices on the device right before its M2L (bit-identical
+    to the resident "device" tables; memory per plan drops to one level's worth).
     """
     if tables not in ("device", "host"):
         raise ValueError('tables must be "device" or "host"')
+    if stream_tables and tables != "device":
+        raise ValueError('stream_tables needs tables="device"')
     x, kf = _validate_setup(positions, k, p, N_max, max_depth)
     dev = _device(device)
     with torch.cuda.device(dev):
@@ -151,7 +157,7 @@ def setup(positions, k, p=4, N_max=16, max_depth=None, device=None, tables="devi
                                         _lib.ctypes.byref(h)))
         state = HFMMState(h.value, pos, kf, p, N_max, dev)
         try:
-            _load_tables(state, tables)
+            _load_tables(state, tables, stream_tables)
             _check(_lib.lib.hfmm_plan_finalize(state.handle))
         except Exception:
             state.close()
@@ -160,13 +166,15 @@ def setup(positions, k, p=4, N_max=16, max_depth=None, device=None, tables="devi
     return state
 
 
-def _load_tables(state, mode="device"):
+def _load_tables(state, mode="device", streamed=False):
     p, md = state.p, state.max_depth
     extent = state.info["domain_extent"]
     eq = np.ascontiguousarray(surface_pts(p, R_EQUIV))
     ch = np.ascontiguousarray(surface_pts(p, R_CHECK))
     _check(_lib.lib.hfmm_plan_set_kernel(state.handle, state.k, p, state.n_families,
                                          eq.ctypes.data, ch.ctypes.data))
+    _check(_lib.lib.hfmm_plan_set_streaming(state.handle, int(bool(streamed))))
+    state.streamed = bool(streamed)
     for fam in range(state.n_families):
         eps_rel = 1e-7 if fam == 0 else 1e-12          # HFMM.py:75-77
         for level in range(2, md + 1):

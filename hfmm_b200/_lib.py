@@ -13,9 +13,9 @@ LIB_PATH = os.path.join(_HERE, "_lib", "libhfmm_b200.so")
 HFMM_OK = 0
 HFMM_PREC_FP64 = 0
 HFMM_PREC_MIXED = 1
-N_PHASES = 12
+N_PHASES = 13
 PHASES = ("gather", "p2m", "m2m_gemm", "up_decode", "m2l_l2l_gemm", "p2l", "down_decode",
-          "p2p", "l2p", "m2p", "combine", "tf32_split")
+          "p2p", "l2p", "m2p", "combine", "tf32_split", "m2l_tables")
 
 _c_i32, _c_i64, _c_dbl, _c_vp = ctypes.c_int32, ctypes.c_int64, ctypes.c_double, ctypes.c_void_p
 
@@ -49,6 +49,9 @@ SIGNATURES = [
     ("hfmm_plan_set_kernel", _c_i32, [_c_vp, _c_dbl, _c_i32, _c_i32, _c_vp, _c_vp]),
     ("hfmm_plan_set_level", _c_i32, [_c_vp, _c_i32, _c_i32] + [_c_vp] * 9),
     ("hfmm_plan_set_level_decode", _c_i32, [_c_vp, _c_i32, _c_i32] + [_c_vp] * 6),
+    ("hfmm_plan_set_streaming", _c_i32, [_c_vp, _c_i32]),
+    ("hfmm_plan_workspace_bytes", _c_i32, [_c_vp, ctypes.POINTER(_c_i64)]),
+    ("hfmm_plan_bind_workspace", _c_i32, [_c_vp, _c_vp, _c_i64]),
     ("hfmm_plan_finalize", _c_i32, [_c_vp]),
     ("hfmm_evaluate", _c_i32, [_c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_i32, _c_vp]),
     ("hfmm_plan_check", _c_i32, [_c_vp, _c_vp]),
@@ -62,6 +65,12 @@ SIGNATURES = [
                                      _c_vp, _c_vp]),
     ("hfmm_plan_set_profiling", _c_i32, [_c_vp, _c_i32]),
     ("hfmm_plan_phase_times", _c_i32, [_c_vp, _c_vp]),
+    ("hfmm_batch_create", _c_i32, [ctypes.POINTER(_c_vp), _c_i32, _c_i32, ctypes.POINTER(_c_vp)]),
+    ("hfmm_batch_stream_of", _c_i32, [_c_vp, _c_i32]),
+    ("hfmm_batch_set_problem", _c_i32, [_c_vp, _c_i32, _c_vp, _c_vp, _c_vp, _c_vp, _c_i32]),
+    ("hfmm_batch_capture", _c_i32, [_c_vp]),
+    ("hfmm_batch_launch", _c_i32, [_c_vp, _c_vp]),
+    ("hfmm_batch_destroy", None, [_c_vp]),
     ("hfmm_mlp_param_count", _c_i32, [_c_i32, _c_i32]),
     ("hfmm_mlp_forward", _c_i32, [_c_vp, _c_vp, _c_i32, _c_i32, _c_i32, _c_vp, _c_vp]),
     ("hfmm_mlp_grad", _c_i32, [_c_vp, _c_vp, _c_vp, _c_i32, _c_i32, _c_i32, _c_vp,

@@ -1,0 +1,244 @@
+"""Batched evaluate of many independent problems in one CUDA-graph launch.
+
+No counterpart in the reference (one problem per ``HFMM.evaluate`` call,
+HFMM.py:83-91). ``Batch`` binds finalized plans to the native batch runtime
+(``hfmm_batch_*`` in include/hfmm_b200.h): the plans are spread over CUDA
+streams by their work estimate, streaming plans share one M2L-table workspace
+per stream, and the whole batch is captured into one graph.
+
+``autotune`` measures the graph time for each candidate stream count and keeps
+the fastest in a JSON "wisdom" file keyed by the batch's shape (the design
+precedent is the reference's Laplace autotuner, jaxfmm/tune.py:123-172).
+
+``AutoBatch`` is the certified front door for a list of (positions, k): the
+expansion-order network picks each problem's p and leaf size from one batched
+forward pass, the problems run as one graph, and each result is checked on
+256 sampled targets against the FP64 direct sum, with a plain rerun of the
+problems that miss.
+"""
+import hashlib
+import json
+import os
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import check as _check
+
+
+class Batch:
+    """Finalized plans evaluated together; ``bind`` sets the inputs and captures."""
+
+    def __init__(self, states, n_streams=4):
+        if not states:
+            raise ValueError("a batch needs at least one plan")
+        self.states = list(states)
+        self.n_streams = int(n_streams)
+        arr = (_lib.ctypes.c_void_p * len(states))(*[s.handle for s in states])
+        h = _lib.ctypes.c_void_p()
+        with torch.cuda.device(states[0].device):
+            _check(_lib.lib.hfmm_batch_create(arr, len(states), self.n_streams,
+                                              _lib.ctypes.byref(h)))
+        self._h = h.value
+        self.outputs = None
+
+    def stream_of(self, i):
+        r = _lib.lib.hfmm_batch_stream_of(self._h, i)
+        _check(min(r, 0))
+        return r
+
+    def bind(self, charges, field=True, precision=None):
+        """Device charge tensors (complex128 or float64, one per plan); allocates the
+        outputs, sets every problem and captures the graph. ``precision``: one value
+        or one per problem (default mixed)."""
+        from . import PREC_MIXED
+        if len(charges) != len(self.states):
+            raise ValueError("one charge vector per plan")
+        precs = precision if isinstance(precision, (list, tuple)) else \
+            [PREC_MIXED if precision is None else precision] * len(self.states)
+        self._keep, self.outputs = [], []
+        for i, (st, q) in enumerate(zip(self.states, charges)):
+            if tuple(q.shape) != (st.n,):
+                raise ValueError(f"charges of problem {i} must have shape ({st.n},)")
+            if q.is_complex():
+                q_re, q_im = q.real.double().contiguous(), q.imag.double().contiguous()
+            else:
+                q_re, q_im = q.double().contiguous(), None
+            phi = torch.empty(st.n, dtype=torch.complex128, device=st.device)
+            E = torch.empty((st.n, 3), dtype=torch.complex128, device=st.device) if field else None
+            _check(_lib.lib.hfmm_batch_set_problem(
+                self._h, i, q_re.data_ptr(), None if q_im is None else q_im.data_ptr(),
+                phi.data_ptr(), None if E is None else E.data_ptr(), int(precs[i])))
+            self._keep.append((q_re, q_im))
+            self.outputs.append((phi, E))
+        with torch.cuda.device(self.states[0].device):
+            _check(_lib.lib.hfmm_batch_capture(self._h))
+        return self.outputs
+
+    def launch(self, stream=None):
+        s = stream if stream is not None else torch.cuda.current_stream(self.states[0].device)
+        _check(_lib.lib.hfmm_batch_launch(self._h, s.cuda_stream))
+
+    def check_errors(self):
+        from . import check_errors
+        for st in self.states:
+            check_errors(st)
+
+    def time_ms(self, reps=3, warmup=1):
+        """Mean CUDA-event time of one graph launch."""
+        s = torch.cuda.current_stream(self.states[0].device)
+        for _ in range(warmup):
+            self.launch(s)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(s)
+        for _ in range(reps):
+            self.launch(s)
+        b.record(s)
+        b.synchronize()
+        return a.elapsed_time(b) / reps
+
+    def close(self):
+        if getattr(self, "_h", None) is not None:
+            _lib.lib.hfmm_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def signature(states):
+    """Key of a batch's shape for the wisdom file: sizes, orders and depths."""
+    desc = sorted((s.n, s.p, s.max_depth, s.N_max, round(s.k, 6)) for s in states)
+    dev = torch.cuda.get_device_name(states[0].device)
+    return dev + ":" + hashlib.sha1(repr(desc).encode()).hexdigest()[:16]
+
+
+def autotune(states, charges, candidates=(1, 2, 4, 8), wisdom=None, reps=3, field=True,
+             precision=None):
+    """Pick the stream count with the lowest graph time; returns (Batch, timings).
+
+    With ``wisdom`` (a JSON path) a previous result for the same signature is
+    reused without measuring, and new measurements are stored there."""
+    key = signature(states)
+    store = {}
+    if wisdom and os.path.exists(wisdom):
+        with open(wisdom) as f:
+            store = json.load(f)
+    if key in store:
+        b = Batch(states, store[key]["n_streams"])
+        b.bind(charges, field, precision)
+        return b, store[key]["ms"]
+    times = {}
+    for S in candidates:                 # a plan belongs to one batch at a time
+        if S > len(states) and S != candidates[0]:
+            continue
+        b = Batch(states, S)
+        b.bind(charges, field, precision)
+        times[S] = b.time_ms(reps)
+        b.close()
+    best = min(times, key=times.get)
+    if wisdom:
+        store[key] = {"n_streams": best, "ms": {str(k): v for k, v in times.items()}}
+        tmp = wisdom + ".tmp"
+        with open(tmp, "w") as f:
+            json.dump(store, f, indent=1, sort_keys=True)
+        os.replace(tmp, wisdom)
+    b = Batch(states, best)
+    b.bind(charges, field, precision)
+    return b, times
+
+
+class AutoBatch:
+    """Certified batched evaluate of problems [(positions, k), ...] at one tolerance.
+
+    ``net``: an OrderNet, None for the bundled weights, or False for the
+    conservative order (the ablation). Every problem's plan streams its M2L
+    tables, so the batch's table memory is one workspace per stream.
+    """
+
+    def __init__(self, problems, tol=1e-6, net=None, n_streams=None, n_check=256, seed=0,
+                 device=None, margin=0.5, wisdom=None):
+        from . import setup, _device
+        from .learned import (OrderNet, features_for, conservative_p, precision_for,
+                              FEATURE_LEAF)
+        self.tol = float(tol)
+        self.device = _device(device)
+        self.problems = problems
+        if net is False:
+            choice = [(conservative_p(self.tol), FEATURE_LEAF)] * len(problems)
+        else:
+            net = OrderNet.load(device=self.device) if net is None else net
+            feats = np.stack([features_for(x, k, self.tol, self.device) for x, k in problems])
+            Y = net.predict(feats)
+            choice = [net.choose_from(y, margin) for y in Y]
+        self.choice = choice
+        self.precisions = [precision_for(self.tol, p) for p, _ in choice]
+        self.states = [setup(x, k, p=p, N_max=leaf, device=self.device, stream_tables=True)
+                       for (x, k), (p, leaf) in zip(problems, choice)]
+        rng = np.random.default_rng(seed)
+        self.checks = [torch.as_tensor(np.sort(rng.choice(st.n, min(n_check, st.n), replace=False))
+                                       .astype(np.int32)).to(self.device) for st in self.states]
+        self.n_streams = n_streams
+        self.wisdom = wisdom
+        self.batch = None
+        self.report = []
+
+    def bind(self, charges, field=True):
+        qs = [torch.as_tensor(np.asarray(q)).to(self.device) if not isinstance(q, torch.Tensor)
+              else q.to(self.device) for q in charges]
+        self._q = qs
+        self._field = field
+        if self.n_streams is None:
+            self.batch, self.tune_ms = autotune(self.states, qs, wisdom=self.wisdom, field=field,
+                                                precision=self.precisions)
+        else:
+            self.batch = Batch(self.states, self.n_streams)
+            self.batch.bind(qs, field, self.precisions)
+        return self.batch.outputs
+
+    def certify(self):
+        """Check every problem on its sampled targets; rerun misses plainly (FP64,
+        conservative order, stepping p by 2). Returns the per-problem reports."""
+        from . import direct_at, evaluate_into, check_errors, setup, PREC_FP64
+        from .learned import conservative_p, P_MAX, FEATURE_LEAF, _rel_l2
+        self.batch.check_errors()
+        rep = []
+        for i, (st, tg) in enumerate(zip(self.states, self.checks)):
+            q = self._q[i]
+            q_re = q.real.double().contiguous() if q.is_complex() else q.double().contiguous()
+            q_im = q.imag.double().contiguous() if q.is_complex() else None
+            phi, E = self.batch.outputs[i]
+            r_phi, r_E = direct_at(st, q_re, q_im, tg, field=E is not None)
+            ref = (r_phi.cpu().numpy(), None if r_E is None else r_E.cpu().numpy())
+
+            def err_of():
+                e = _rel_l2(phi[tg].cpu().numpy(), ref[0])
+                if E is not None:
+                    e = max(e, _rel_l2(E[tg].cpu().numpy(), ref[1]))
+                return e
+            err = err_of()
+            r = dict(p=self.choice[i][0], leaf=self.choice[i][1], error=err, fallback=False)
+            p = conservative_p(self.tol)
+            while err > self.tol and p <= P_MAX:
+                x, k = self.problems[i]
+                plain = setup(x, k, p=p, N_max=FEATURE_LEAF, device=self.device)
+                evaluate_into(plain, q_re, q_im, phi, E, PREC_FP64)
+                check_errors(plain)
+                plain.close()
+                err = err_of()
+                r.update(fallback=True, p_final=p, error=err)
+                p += 2
+            r["certified"] = bool(err <= self.tol)
+            rep.append(r)
+        self.report = rep
+        return rep
+
+    def close(self):
+        if self.batch is not None:
+            self.batch.close()
+        for st in self.states:
+            st.close()

@@ -128,11 +128,14 @@ void build_a_ptrs(hfmm_plan* P, PtrIndex& ix) {
                     case K_M2M:
                         for (int o = 0; o < 8; ++o) h.push_back(T.m2m.p ? T.m2m.p + o * mat : nullptr);
                         break;
-                    case K_DN:
+                    case K_DN: {
+                        const double* m2l = P->streamed
+                            ? static_cast<const double*>(P->ws) + (size_t)f * 316 * mat : T.m2l.p;
                         for (int d = 0; d < N_DISP; ++d)
-                            h.push_back(compact[d] >= 0 ? T.m2l.p + compact[d] * mat : nullptr);
+                            h.push_back(compact[d] >= 0 && m2l ? m2l + compact[d] * mat : nullptr);
                         for (int o = 0; o < 8; ++o) h.push_back(T.l2l.p ? T.l2l.p + o * mat : nullptr);
                         break;
+                    }
                     case K_L2L:
                         for (int o = 0; o < 8; ++o) h.push_back(T.l2l.p ? T.l2l.p + o * mat : nullptr);
                         break;
@@ -223,6 +226,8 @@ void upload_level(hfmm_plan* P, int fam, int l, const double* const* h) {
     relayout(h[3], 1, none, n_s, ld, false, T.dn_U);
     upload_vec(h[4], n_s, ld, T.dn_d);
     relayout(h[5], 1, none, n_s, ld, false, T.dn_Vt);
+    if (P->streamed && h[8])
+        throw Error{HFMM_ERR_STATE, "streamed M2L tables are generated on the device: pass no M2L table"};
     if (!h[8]) {   // kernel matrices generated on the device
         generate_tables(P, fam, l);
         T.set = true;
@@ -234,6 +239,22 @@ void upload_level(hfmm_plan* P, int fam, int l, const double* const* h) {
     else T.l2l.release();
     relayout(h[8], N_DISP, nonadjacent_map(), n_s, ld, true, T.m2l);
     T.set = true;
+}
+
+// Tensor maps of the streamed TF32 tables: every level reads the same workspace
+// (hi halves of both families, then the lo halves; [fam][316][m][k] each).
+void stream_maps(hfmm_plan* P) {
+    if (!P->mx_maps) P->mx_maps = new MixedMaps[MAX_LEVELS];
+    MixedMaps* maps = static_cast<MixedMaps*>(P->mx_maps);
+    std::memset(maps, 0, sizeof(MixedMaps) * MAX_LEVELS);
+    const size_t fam = (size_t)316 * P->ld * P->ld;
+    const float* hi = static_cast<const float*>(P->ws);
+    const float* lo = hi + (size_t)P->n_fam * fam;
+    for (int l = 2; l <= P->md; ++l)
+        for (int f = 0; f < P->n_fam; ++f) {
+            make_table_map(&maps[l].a_hi[f], hi + f * fam, P->ld, 316);
+            make_table_map(&maps[l].a_lo[f], lo + f * fam, P->ld, 316);
+        }
 }
 
 void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double* phi, double* E,
@@ -346,6 +367,10 @@ void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double*
     }
     // ---- downward pass (M2L + L2L in one GEMM, then X-list P2L, then decode)
     for (int l = 2; l <= P->md; ++l) {
+        if (P->streamed) {
+            PhaseTimer pt(X, s, 12);
+            generate_m2l_stream(P, l, use_mx, P->ws, s);
+        }
         if (use_mx) {
             PhaseTimer pt(X, s, 4);
             MixedCall mc{};
@@ -542,6 +567,47 @@ int hfmm_plan_set_kernel(hfmm_plan* P, double k, int32_t p, int32_t n_families,
     API_END
 }
 
+int hfmm_plan_set_streaming(hfmm_plan* P, int32_t enable) {
+    if (!P) return fail(HFMM_ERR_ARG, "plan is NULL");
+    if (P->n_s == 0) return fail(HFMM_ERR_STATE, "set the kernel first");
+    for (int f = 0; f < 2; ++f)
+        for (int l = 0; l < MAX_LEVELS; ++l)
+            if (P->tables[f][l].set)
+                return fail(HFMM_ERR_STATE, "choose the table mode before the level tables");
+    P->streamed = enable != 0;
+    if (!P->streamed) {
+        P->ws_own.release();
+        P->ws = nullptr;
+        P->ws_bytes = 0;
+    }
+    return HFMM_OK;
+}
+
+int hfmm_plan_workspace_bytes(const hfmm_plan* P, int64_t* bytes) {
+    if (!P || !bytes) return fail(HFMM_ERR_ARG, "plan or output is NULL");
+    if (P->n_s == 0) return fail(HFMM_ERR_STATE, "set the kernel first");
+    *bytes = (int64_t)stream_ws_bytes(P);
+    return HFMM_OK;
+}
+
+int hfmm_plan_bind_workspace(hfmm_plan* P, void* ws_dev, int64_t bytes) {
+    if (!P || !ws_dev) return fail(HFMM_ERR_ARG, "plan or workspace is NULL");
+    if (!P->streamed) return fail(HFMM_ERR_STATE, "the plan does not stream its M2L tables");
+    if (bytes < (int64_t)stream_ws_bytes(P)) return fail(HFMM_ERR_CAPACITY, "workspace too small");
+    if ((uintptr_t)ws_dev % 256) return fail(HFMM_ERR_ARG, "workspace must be 256-byte aligned");
+    API_BEGIN
+    require_device_ptr(ws_dev, "workspace");
+    P->ws_own.release();
+    P->ws = ws_dev;
+    P->ws_bytes = (size_t)bytes;
+    if (P->finalized) {
+        build_a_ptrs(P, extra(P, true)->ix);
+        if (P->mixed_ready) stream_maps(P);
+    }
+    return HFMM_OK;
+    API_END
+}
+
 int hfmm_plan_set_level(hfmm_plan* P, int32_t family, int32_t level, const double* F_up_U,
                         const double* F_up_d, const double* F_up_Vt, const double* F_dn_U,
                         const double* F_dn_d, const double* F_dn_Vt, const double* M2M_K,
@@ -593,7 +659,7 @@ int hfmm_plan_finalize(hfmm_plan* P) {
         schedules_build(P);
     }
     PlanExtra* X = extra(P, true);
-    build_a_ptrs(P, X->ix);
+    build_a_ptrs(P, X->ix);   // streamed plans without a workspace yet: see evaluate
     const size_t exp = (size_t)P->n_fam * P->nb * 2 * P->ld;
     P->check.alloc(exp);
     P->equiv.alloc(exp);
@@ -615,16 +681,20 @@ int hfmm_plan_finalize(hfmm_plan* P) {
         if (!P->mx_maps) P->mx_maps = new MixedMaps[MAX_LEVELS];
         MixedMaps* maps = static_cast<MixedMaps*>(P->mx_maps);
         std::memset(maps, 0, sizeof(MixedMaps) * MAX_LEVELS);
-        for (int f = 0; f < P->n_fam; ++f)
-            for (int l = 2; l <= P->md; ++l) {
-                LevelTables& T = P->tables[f][l];
-                const int nm = (int)madj.size();
-                T.m2l_hi.alloc(nm * mat);
-                T.m2l_lo.alloc(nm * mat);
-                split_transpose_tables(T.m2l.p, T.m2l_hi.p, T.m2l_lo.p, P->ld, nm);
-                make_table_map(&maps[l].a_hi[f], T.m2l_hi.p, P->ld, nm);
-                make_table_map(&maps[l].a_lo[f], T.m2l_lo.p, P->ld, nm);
-            }
+        if (P->streamed) {
+            if (P->ws) stream_maps(P);
+        } else {
+            for (int f = 0; f < P->n_fam; ++f)
+                for (int l = 2; l <= P->md; ++l) {
+                    LevelTables& T = P->tables[f][l];
+                    const int nm = (int)madj.size();
+                    T.m2l_hi.alloc(nm * mat);
+                    T.m2l_lo.alloc(nm * mat);
+                    split_transpose_tables(T.m2l.p, T.m2l_hi.p, T.m2l_lo.p, P->ld, nm);
+                    make_table_map(&maps[l].a_hi[f], T.m2l_hi.p, P->ld, nm);
+                    make_table_map(&maps[l].a_lo[f], T.m2l_lo.p, P->ld, nm);
+                }
+        }
         P->e_hi.alloc(exp);
         P->e_lo.alloc(exp);
         P->e_hi.zero();
@@ -652,6 +722,13 @@ int hfmm_evaluate(hfmm_plan* P, const double* q_re, const double* q_im, double* 
     if (q_im) require_device_ptr(q_im, "q_im");
     require_device_ptr(phi, "phi_out");
     if (E) require_device_ptr(E, "field_out");
+    if (P->streamed && !P->ws) {   // first evaluate without a bound workspace: the plan's own
+        P->ws_bytes = stream_ws_bytes(P);
+        P->ws_own.alloc(P->ws_bytes / sizeof(double));
+        P->ws = P->ws_own.p;
+        build_a_ptrs(P, extra(P, true)->ix);
+        if (P->mixed_ready) stream_maps(P);
+    }
     evaluate_fp64(P, q_re, q_im, phi, E, (cudaStream_t)stream, precision == HFMM_PREC_MIXED);
     return HFMM_OK;
     API_END
@@ -673,6 +750,17 @@ int hfmm_plan_check(hfmm_plan* P, void* stream) {
     return HFMM_OK;
     API_END
 }
+
+}  // extern "C"
+
+namespace hfmm {
+bool plan_profiling(hfmm_plan* P) {
+    PlanExtra* X = extra(P, false);
+    return X && X->profiling;
+}
+}  // namespace hfmm
+
+extern "C" {
 
 int hfmm_plan_set_profiling(hfmm_plan* P, int32_t enable) {
     if (!P) return fail(HFMM_ERR_ARG, "plan is NULL");
@@ -709,6 +797,7 @@ int hfmm_plan_phase_times(hfmm_plan* P, double* ms) {
 
 void hfmm_plan_destroy(hfmm_plan* P) {
     if (!P) return;
+    if (P->batch_owner) batch_forget_plan(P->batch_owner, P);
     drop_extra(P);
     delete[] static_cast<MixedMaps*>(P->mx_maps);
     P->mx_maps = nullptr;

@@ -1,0 +1,249 @@
+// Batched evaluate: many independent problems (plans of uneven size and
+// wavenumber) in one CUDA-graph launch. No counterpart in the reference, which
+// evaluates one problem per call (HFMM.py:83-91).
+//
+// The plans are spread over S streams by longest-processing-time-first on an
+// estimate of each plan's work (M2L GEMM FLOPs + near-field pairs); each stream
+// evaluates its plans in turn, so small problems overlap the tails of large ones.
+// Plans that stream their M2L tables share one workspace per stream (sized for
+// the largest of them), which bounds the table memory of the whole batch by S
+// workspaces. The whole batch -- fork, every evaluate, join -- is captured once
+// into a graph; a launch replays it with the charge and output pointers given
+// before capture.
+#include "hfmm_internal.cuh"
+
+#include <algorithm>
+#include <numeric>
+#include <vector>
+
+struct hfmm_batch {
+    int device = 0;
+    std::vector<hfmm_plan*> plans;
+    std::vector<int> stream_of;                 // plan -> stream
+    std::vector<std::vector<int>> order;        // stream -> plans in launch order
+    std::vector<double> cost;
+    struct Io {
+        const double *q_re = nullptr, *q_im = nullptr;
+        double *phi = nullptr, *E = nullptr;
+        int precision = 0;
+        bool set = false;
+    };
+    std::vector<Io> io;
+    std::vector<cudaStream_t> streams;
+    std::vector<cudaEvent_t> events;            // [0] fork, [1 + s] join of stream s
+    std::vector<hfmm::DevBuf<double>> ws;       // per stream (streamed plans only)
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    void drop_graph() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        exec = nullptr;
+        graph = nullptr;
+    }
+    ~hfmm_batch() {
+        if (!streams.empty()) cudaStreamSynchronize(streams[0]);
+        drop_graph();
+        // release the plans: a streaming plan falls back to its own workspace,
+        // allocated at its next evaluate
+        for (auto* P : plans) {
+            if (!P) continue;
+            if (P->streamed) {
+                P->ws = nullptr;
+                P->ws_bytes = 0;
+            }
+            P->batch_owner = nullptr;
+        }
+        for (auto e : events) cudaEventDestroy(e);
+        for (auto s : streams) cudaStreamDestroy(s);
+    }
+};
+
+namespace hfmm {
+
+namespace {
+
+// Work estimate of one evaluate (complex charges): far field M2L+L2L FLOPs and
+// near-field pairs weighted by ~40 flops each; only the relative size matters.
+double plan_cost(const hfmm_plan* P) {
+    const double ns = P->n_s;
+    const double far = 2.0 * ns * ns * 2.0 * P->n_fam * ((double)P->nV + 8.0 * P->nb);
+    const double occ = P->n_leaves ? (double)P->n / P->n_leaves : 0.0;
+    const double near = 40.0 * (double)P->nNear * occ * occ;
+    return far + near + 1e6;   // + a launch-overhead floor
+}
+
+}  // namespace
+
+}  // namespace hfmm
+
+using namespace hfmm;
+
+extern "C" {
+
+int hfmm_batch_create(hfmm_plan* const* plans, int32_t n_plans, int32_t n_streams,
+                      hfmm_batch** out) {
+    if (!out) return fail(HFMM_ERR_ARG, "out is NULL");
+    *out = nullptr;
+    if (!plans || n_plans <= 0) return fail(HFMM_ERR_ARG, "no plans");
+    if (n_streams < 1 || n_streams > 64) return fail(HFMM_ERR_ARG, "n_streams must be in [1, 64]");
+    int dev = -1;
+    for (int i = 0; i < n_plans; ++i) {
+        if (!plans[i]) return fail(HFMM_ERR_ARG, "plan is NULL");
+        if (!plans[i]->finalized) return fail(HFMM_ERR_STATE, "every plan must be finalized");
+        if (dev >= 0 && plans[i]->device != dev)
+            return fail(HFMM_ERR_ARG, "plans of one batch must live on one device");
+        dev = plans[i]->device;
+        for (int j = 0; j < i; ++j)
+            if (plans[j] == plans[i]) return fail(HFMM_ERR_ARG, "a plan appears twice");
+        if (plans[i]->batch_owner) return fail(HFMM_ERR_STATE, "a plan already belongs to a batch");
+    }
+    hfmm_batch* B = new hfmm_batch();
+    try {
+        B->device = dev;
+        HFMM_CUDA(cudaSetDevice(dev));
+        B->plans.assign(plans, plans + n_plans);
+        for (auto* P : B->plans) P->batch_owner = B;
+        const int S = std::min<int>(n_streams, n_plans);
+        B->cost.resize(n_plans);
+        for (int i = 0; i < n_plans; ++i) B->cost[i] = plan_cost(plans[i]);
+        std::vector<int> idx(n_plans);
+        std::iota(idx.begin(), idx.end(), 0);
+        std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return B->cost[a] > B->cost[b]; });
+        std::vector<double> load(S, 0.0);
+        B->order.assign(S, {});
+        B->stream_of.assign(n_plans, 0);
+        for (int i : idx) {   // LPT: the next largest plan goes to the least loaded stream
+            const int s = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+            load[s] += B->cost[i];
+            B->order[s].push_back(i);
+            B->stream_of[i] = s;
+        }
+        B->io.assign(n_plans, {});
+        B->streams.resize(S);
+        for (auto& s : B->streams) HFMM_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+        B->events.resize(S + 1);
+        for (auto& e : B->events) HFMM_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        // one M2L-table workspace per stream, shared by the streamed plans on it
+        B->ws = std::vector<DevBuf<double>>(S);
+        for (int s = 0; s < S; ++s) {
+            size_t need = 0;
+            for (int i : B->order[s])
+                if (plans[i]->streamed) need = std::max(need, stream_ws_bytes(plans[i]));
+            if (!need) continue;
+            B->ws[s].alloc(need / sizeof(double));
+            for (int i : B->order[s]) {
+                if (!plans[i]->streamed) continue;
+                int rc = hfmm_plan_bind_workspace(plans[i], B->ws[s].p, (int64_t)need);
+                if (rc != HFMM_OK) throw Error{rc, hfmm_last_error()};
+            }
+        }
+        *out = B;
+        return HFMM_OK;
+    } catch (const Error& e) {
+        delete B;
+        return fail(e.code, e.msg);
+    }
+}
+
+int hfmm_batch_stream_of(const hfmm_batch* B, int32_t i) {
+    if (!B || i < 0 || i >= (int)B->plans.size()) return fail(HFMM_ERR_ARG, "bad batch or index");
+    return B->stream_of[i];
+}
+
+int hfmm_batch_set_problem(hfmm_batch* B, int32_t i, const double* q_re_dev, const double* q_im_dev,
+                           double* phi_out_dev, double* field_out_dev, int32_t precision) {
+    if (!B || i < 0 || i >= (int)B->plans.size()) return fail(HFMM_ERR_ARG, "bad batch or index");
+    if (!B->plans[i]) return fail(HFMM_ERR_STATE, "the plan was destroyed");
+    if (!q_re_dev || !phi_out_dev) return fail(HFMM_ERR_ARG, "charges and output are required");
+    if (precision != HFMM_PREC_FP64 && precision != HFMM_PREC_MIXED)
+        return fail(HFMM_ERR_ARG, "precision must be HFMM_PREC_FP64 or HFMM_PREC_MIXED");
+    try {
+        require_device_ptr(q_re_dev, "q_re");
+        if (q_im_dev) require_device_ptr(q_im_dev, "q_im");
+        require_device_ptr(phi_out_dev, "phi_out");
+        if (field_out_dev) require_device_ptr(field_out_dev, "field_out");
+    } catch (const Error& e) {
+        return fail(e.code, e.msg);
+    }
+    auto& io = B->io[i];
+    io.q_re = q_re_dev;
+    io.q_im = q_im_dev;
+    io.phi = phi_out_dev;
+    io.E = field_out_dev;
+    io.precision = precision;
+    io.set = true;
+    B->drop_graph();   // pointers changed: the graph must be captured again
+    return HFMM_OK;
+}
+
+int hfmm_batch_capture(hfmm_batch* B) {
+    if (!B) return fail(HFMM_ERR_ARG, "batch is NULL");
+    for (auto& io : B->io)
+        if (!io.set) return fail(HFMM_ERR_STATE, "every problem needs its charges and outputs");
+    for (auto* P : B->plans) {
+        if (!P) return fail(HFMM_ERR_STATE, "a plan of the batch was destroyed");
+        if (plan_profiling(P)) return fail(HFMM_ERR_STATE, "turn profiling off before capture");
+        if (P->streamed && !P->ws) return fail(HFMM_ERR_STATE, "a streaming plan has no workspace");
+    }
+    try {
+        HFMM_CUDA(cudaSetDevice(B->device));
+        B->drop_graph();
+        const int S = (int)B->streams.size();
+        cudaStream_t s0 = B->streams[0];
+        HFMM_CUDA(cudaStreamBeginCapture(s0, cudaStreamCaptureModeRelaxed));
+        try {
+            HFMM_CUDA(cudaEventRecord(B->events[0], s0));
+            for (int s = 1; s < S; ++s) HFMM_CUDA(cudaStreamWaitEvent(B->streams[s], B->events[0], 0));
+            for (int s = 0; s < S; ++s)
+                for (int i : B->order[s]) {
+                    const auto& io = B->io[i];
+                    evaluate_fp64(B->plans[i], io.q_re, io.q_im, io.phi, io.E, B->streams[s],
+                                  io.precision == HFMM_PREC_MIXED);
+                }
+            for (int s = 1; s < S; ++s) {
+                HFMM_CUDA(cudaEventRecord(B->events[1 + s], B->streams[s]));
+                HFMM_CUDA(cudaStreamWaitEvent(s0, B->events[1 + s], 0));
+            }
+        } catch (...) {
+            cudaGraph_t g = nullptr;
+            cudaStreamEndCapture(s0, &g);
+            if (g) cudaGraphDestroy(g);
+            throw;
+        }
+        HFMM_CUDA(cudaStreamEndCapture(s0, &B->graph));
+        HFMM_CUDA(cudaGraphInstantiate(&B->exec, B->graph, 0));
+        return HFMM_OK;
+    } catch (const Error& e) {
+        return fail(e.code, e.msg);
+    }
+}
+
+int hfmm_batch_launch(hfmm_batch* B, void* stream) {
+    if (!B) return fail(HFMM_ERR_ARG, "batch is NULL");
+    for (auto* P : B->plans)
+        if (!P) return fail(HFMM_ERR_STATE, "a plan of the batch was destroyed");
+    if (!B->exec) return fail(HFMM_ERR_STATE, "capture the batch first");
+    try {
+        HFMM_CUDA(cudaGraphLaunch(B->exec, (cudaStream_t)stream));
+        return HFMM_OK;
+    } catch (const Error& e) {
+        return fail(e.code, e.msg);
+    }
+}
+
+void hfmm_batch_destroy(hfmm_batch* B) { delete B; }
+
+}  // extern "C"
+
+namespace hfmm {
+// A plan destroyed while its batch lives: the batch drops the plan and its graph.
+void batch_forget_plan(hfmm_batch* B, hfmm_plan* P) {
+    B->drop_graph();
+    for (auto& q : B->plans)
+        if (q == P) q = nullptr;
+}
+}  // namespace hfmm
+
+extern "C" {
+
+}  // extern "C"

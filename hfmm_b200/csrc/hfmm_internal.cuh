@@ -159,6 +159,13 @@ struct hfmm_plan {
     hfmm::DevBuf<float> e_hi, e_lo, l_hi, l_lo;   // split densities [fam][box][R][ld]
     void* mx_maps = nullptr;                // MixedMaps per level (host array)
     bool mixed_ready = false;
+    // streamed M2L tables: regenerated per level and evaluate into a workspace
+    // (the plan's own, or one bound by the caller and shared by plans that run in turn)
+    bool streamed = false;
+    void* ws = nullptr;
+    size_t ws_bytes = 0;
+    hfmm::DevBuf<double> ws_own;
+    struct hfmm_batch* batch_owner = nullptr;   // the batch whose workspace and graph use this plan
     hfmm::DevBuf<const double*> a_ptrs;     // device arrays of A pointers per GEMM call
     std::vector<const double*> h_a_ptrs;
     size_t a_ptr_cursor = 0;
@@ -180,6 +187,10 @@ void lists_build(hfmm_plan* P);
 void schedules_build(hfmm_plan* P);
 void upload_level(hfmm_plan* P, int fam, int level, const double* const* h);
 void generate_tables(hfmm_plan* P, int fam, int level);
+size_t stream_ws_bytes(const hfmm_plan* P);
+bool plan_profiling(hfmm_plan* P);
+void batch_forget_plan(struct hfmm_batch* B, hfmm_plan* P);
+void generate_m2l_stream(hfmm_plan* P, int level, bool mixed, void* ws, cudaStream_t s);
 void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double* phi,
                    double* fld, cudaStream_t s, bool mixed = false);
 void direct_sum(const double* pos, const double* q_re, const double* q_im, int64_t n,

@@ -197,7 +197,11 @@ class OrderNet:
 
     def choose(self, feats, margin=0.5):
         """(p, N_max) for one feature vector: p rounded up after adding ``margin``."""
-        y = self.predict(feats)[0]
+        return self.choose_from(self.predict(feats)[0], margin)
+
+    @staticmethod
+    def choose_from(y, margin=0.5):
+        """(p, N_max) from one output row (fractional p, log2 leaf size)."""
         p = int(min(P_MAX, max(P_MIN, math.ceil(float(y[0]) + margin))))
         leaf = int(2 ** min(7, max(4, round(float(y[1])))))
         return p, leaf

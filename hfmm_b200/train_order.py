@@ -68,8 +68,9 @@ class _DecodeCache:
         return self.memo[key]
 
 
-def _time_eval(hf, st, q_re, q_im, phi, E, prec, reps=3):
-    hf.evaluate_into(st, q_re, q_im, phi, E, prec)
+def _time_eval(hf, st, q_re, q_im, phi, E, prec, reps=1, warmup=0):
+    for _ in range(warmup):
+        hf.evaluate_into(st, q_re, q_im, phi, E, prec)
     s = torch.cuda.current_stream()
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     a.record(s)
@@ -127,7 +128,7 @@ def generate(n_problems, seed=0, n_check=256, verbose=True):
                 st = hf.setup(x, k, p=lp, N_max=leaf, device=dev)
                 phi = torch.empty(st.n, dtype=torch.complex128, device=dev)
                 E = torch.empty((st.n, 3), dtype=torch.complex128, device=dev)
-                lt.append(_time_eval(hf, st, q_re, q_im, phi, E, hf.PREC_MIXED))
+                lt.append(_time_eval(hf, st, q_re, q_im, phi, E, hf.PREC_MIXED, reps=2, warmup=1))
                 st.close()
                 del phi, E
             for key, val in (("feats", f), ("err64", e64), ("errmx", emx), ("t64", t64),

@@ -38,8 +38,8 @@ extern "C" {
 #define HFMM_PREC_MIXED 1     /* M2L as split 3xTF32 on tcgen05 (FP32 accumulation in
                                  short chains, folded into FP64), P2P in FP32 with an
                                  FP64 phase reduction; decodes, M2M, L2L, P2M, L2P FP64.
-                                 M2L needs p >= 6 (n_s >= 128); smaller p runs its FP64
-                                 GEMM.                                                 */
+                                 M2L needs p >= 5 (ld = n_s rounded up to 32 >= 128);
+                                 smaller p runs its FP64 GEMM.                         */
 
 typedef struct hfmm_plan hfmm_plan;
 
@@ -98,6 +98,21 @@ int hfmm_plan_set_level_decode(hfmm_plan* plan, int32_t family, int32_t level,
                                const double* F_up_U, const double* F_up_d, const double* F_up_Vt,
                                const double* F_dn_U, const double* F_dn_d, const double* F_dn_Vt);
 
+/* Streaming M2L tables (no counterpart in the reference, whose M2L tables are
+ * resident, kifmm/operators.py:612-613): instead of keeping the 316 M2L matrices
+ * of every level (11 GB per family at p = 12, depth 5), the plan regenerates a
+ * level's matrices on the device right before that level's M2L, into a
+ * workspace of hfmm_plan_workspace_bytes bytes, bit-identical to the resident
+ * tables. Choose the mode after hfmm_plan_set_kernel and before the level tables
+ * (which must then come without M2L_K: hfmm_plan_set_level_decode). Without a
+ * bound workspace, the first hfmm_evaluate allocates the plan's own (so make
+ * that call outside stream capture). hfmm_plan_bind_workspace
+ * points the plan at a caller-owned device buffer (256-byte aligned); plans that
+ * share one must not run concurrently (a batch gives each stream its own). */
+int hfmm_plan_set_streaming(hfmm_plan* plan, int32_t enable);
+int hfmm_plan_workspace_bytes(const hfmm_plan* plan, int64_t* bytes);
+int hfmm_plan_bind_workspace(hfmm_plan* plan, void* ws_dev, int64_t bytes);
+
 /* Build the V, U, W, X lists and the evaluate schedules on the device
  * (trees/lists.py:818-931, core.py:119-140). */
 int hfmm_plan_finalize(hfmm_plan* plan);
@@ -154,11 +169,36 @@ int hfmm_direct_noalloc(const double* pos_dev, const double* q_re_dev, const dou
  * per phase, summed over every evaluate since profiling was enabled or the
  * previous read (up to 8192 phase instances): 0 charge gather, 1 P2M, 2 M2M GEMM, 3 upward decode,
  * 4 M2L+L2L GEMM, 5 X-list P2L, 6 downward decode, 7 P2P, 8 L2P, 9 W-list M2P,
- * 10 combine, 11 TF32 splits of the mixed path. (Replaces the reference's wall-clock phase prints; it has no
+ * 10 combine, 11 TF32 splits of the mixed path, 12 M2L table generation of a
+ * streaming plan. (Replaces the reference's wall-clock phase prints; it has no
  * per-phase timers, util.py:692-724.) */
-#define HFMM_N_PHASES 12
+#define HFMM_N_PHASES 13
 int hfmm_plan_set_profiling(hfmm_plan* plan, int32_t enable);
 int hfmm_plan_phase_times(hfmm_plan* plan, double* ms_out);
+
+/* ---- batches (no counterpart in the reference: one problem per call there) ---- */
+/* Many finalized plans (problems of uneven size and wavenumber) evaluated by one
+ * CUDA-graph launch. hfmm_batch_create spreads the plans over n_streams streams
+ * (longest work estimate first, onto the least loaded stream) and gives each
+ * stream one M2L-table workspace shared by its streaming plans
+ * (hfmm_plan_set_streaming). Set every problem's device charges and outputs
+ * (same meaning as hfmm_evaluate), capture once, then launch as often as
+ * wanted; changing a problem's pointers drops the graph until the next capture.
+ * Read each plan's device error flag with hfmm_plan_check after a launch.
+ * A plan belongs to at most one batch at a time; destroying the batch hands
+ * streaming plans back to their own workspace (allocated at their next
+ * hfmm_evaluate); destroying a plan first disables the batch's launches. */
+typedef struct hfmm_batch hfmm_batch;
+int hfmm_batch_create(hfmm_plan* const* plans, int32_t n_plans, int32_t n_streams,
+                      hfmm_batch** out);
+/* Stream index [0, n_streams) plan i runs on (>= 0), or a negative status. */
+int hfmm_batch_stream_of(const hfmm_batch* batch, int32_t i);
+int hfmm_batch_set_problem(hfmm_batch* batch, int32_t i, const double* q_re_dev,
+                           const double* q_im_dev, double* phi_out_dev, double* field_out_dev,
+                           int32_t precision);
+int hfmm_batch_capture(hfmm_batch* batch);
+int hfmm_batch_launch(hfmm_batch* batch, void* stream);
+void hfmm_batch_destroy(hfmm_batch* batch);
 
 /* ---- expansion-order network (no counterpart in the reference) ---- */
 /* A 3 x 64 FP32 MLP (tanh hidden layers, linear output) over in_dim features

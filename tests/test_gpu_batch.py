@@ -1,0 +1,164 @@
+"""Streamed M2L tables and batched graph launches on the GPU.
+
+Streaming regenerates each level's M2L matrices per evaluate with the same
+arithmetic as the resident device tables, so results must be bit-identical.
+A batch replays the same kernels with the same inputs, so each problem's result
+must equal its individual evaluate bit for bit as well."""
+import json
+
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+
+def _problem(n, k, seed, clustered=False):
+    rng = np.random.default_rng(seed)
+    if clustered:
+        c = rng.uniform(0.2, 0.8, (3, 3))
+        x = np.clip(c[rng.integers(0, 3, n)] + 0.05 * rng.standard_normal((n, 3)), 0, 1)
+    else:
+        x = rng.random((n, 3))
+    q = rng.standard_normal(n) + 1j * rng.standard_normal(n)
+    return x, float(k), q
+
+
+@pytest.mark.parametrize("p,mixed", [(4, False), (6, False), (6, True), (7, True)])
+def test_streamed_tables_bit_identical(p, mixed):
+    import hfmm_b200 as hf
+    x, k, q = _problem(5000, 5.0, 1, clustered=True)
+    prec = hf.PREC_MIXED if mixed else hf.PREC_FP64
+    a = hf.setup(x, k, p=p, N_max=32)
+    b = hf.setup(x, k, p=p, N_max=32, stream_tables=True)
+    pa, ea = hf.evaluate_field(a, q, prec)
+    pb, eb = hf.evaluate_field(b, q, prec)
+    assert np.array_equal(pa, pb) and np.array_equal(ea, eb)
+    # the other precision through the same streamed plan, then back
+    other = hf.PREC_FP64 if mixed else hf.PREC_MIXED
+    assert np.array_equal(hf.evaluate_field(a, q, other)[0], hf.evaluate_field(b, q, other)[0])
+    assert np.array_equal(hf.evaluate_field(b, q, prec)[0], pa)
+    a.close()
+    b.close()
+
+
+def test_shared_workspace_and_errors():
+    import hfmm_b200 as hf
+    from hfmm_b200 import _lib
+    x1, k1, q1 = _problem(3000, 3.0, 2)
+    x2, k2, q2 = _problem(4000, 9.0, 3)
+    s1 = hf.setup(x1, k1, p=6, N_max=32, stream_tables=True)
+    s2 = hf.setup(x2, k2, p=6, N_max=32, stream_tables=True)
+    need = _lib.ctypes.c_int64()
+    _lib.check(_lib.lib.hfmm_plan_workspace_bytes(s1.handle, _lib.ctypes.byref(need)))
+    ws = torch.empty(need.value // 8, dtype=torch.float64, device="cuda")
+    with pytest.raises(hf.HFMMError):      # too small
+        _lib.check(_lib.lib.hfmm_plan_bind_workspace(s1.handle, ws.data_ptr(), need.value - 8))
+    for s in (s1, s2):
+        _lib.check(_lib.lib.hfmm_plan_bind_workspace(s.handle, ws.data_ptr(), need.value))
+    r1 = hf.setup(x1, k1, p=6, N_max=32)
+    r2 = hf.setup(x2, k2, p=6, N_max=32)
+    for prec in (hf.PREC_FP64, hf.PREC_MIXED):
+        assert np.array_equal(hf.evaluate_field(s1, q1, prec)[0], hf.evaluate_field(r1, q1, prec)[0])
+        assert np.array_equal(hf.evaluate_field(s2, q2, prec)[0], hf.evaluate_field(r2, q2, prec)[0])
+    # a resident plan cannot take a workspace; streaming is chosen before the tables
+    with pytest.raises(hf.HFMMError):
+        _lib.check(_lib.lib.hfmm_plan_bind_workspace(r1.handle, ws.data_ptr(), need.value))
+    with pytest.raises(hf.HFMMError):
+        _lib.check(_lib.lib.hfmm_plan_set_streaming(r1.handle, 1))
+    for s in (s1, s2, r1, r2):
+        s.close()
+
+
+def _batch_problems():
+    specs = [(20000, 2.0, 10, False, 8), (3000, 7.0, 11, True, 6), (9000, 12.0, 12, False, 7),
+             (1500, 1.0, 13, True, 5), (12000, 4.0, 14, True, 4)]
+    out = []
+    for n, k, seed, cl, p in specs:
+        x, k, q = _problem(n, k, seed, cl)
+        out.append((x, k, q, p))
+    return out
+
+
+@pytest.mark.parametrize("n_streams,streamed", [(1, False), (3, True), (8, True)])
+def test_batch_matches_individual_evaluates(n_streams, streamed):
+    import hfmm_b200 as hf
+    from hfmm_b200.batch import Batch
+    probs = _batch_problems()
+    states = [hf.setup(x, k, p=p, N_max=32, stream_tables=streamed) for x, k, q, p in probs]
+    precs = [hf.PREC_MIXED, hf.PREC_FP64, hf.PREC_MIXED, hf.PREC_FP64, hf.PREC_FP64]
+    qs = [torch.as_tensor(q).cuda() for _, _, q, _ in probs]
+    b = Batch(states, n_streams)
+    assert {b.stream_of(i) for i in range(len(states))} <= set(range(min(n_streams, 5)))
+    outs = b.bind(qs, field=True, precision=precs)
+    for _ in range(2):                      # relaunch: same results
+        b.launch()
+        torch.cuda.synchronize()
+        b.check_errors()
+        for st, q, prec, (phi, E) in zip(states, qs, precs, outs):
+            ref = hf.setup(st.positions, st.k, p=st.p, N_max=32)
+            rp, re = hf.evaluate_field(ref, q, prec)
+            assert torch.equal(phi, rp) and torch.equal(E, re)
+            ref.close()
+    b.close()
+    for st in states:
+        st.close()
+
+
+def test_batch_repoint_requires_capture():
+    import hfmm_b200 as hf
+    from hfmm_b200 import _lib
+    from hfmm_b200.batch import Batch
+    probs = _batch_problems()[:2]
+    states = [hf.setup(x, k, p=p, N_max=32, stream_tables=True) for x, k, q, p in probs]
+    qs = [torch.as_tensor(q).cuda() for _, _, q, _ in probs]
+    b = Batch(states, 2)
+    outs = b.bind(qs, field=False)
+    b.launch()
+    q2 = qs[0] * 2.0
+    qr, qi = q2.real.contiguous(), q2.imag.contiguous()
+    _lib.check(_lib.lib.hfmm_batch_set_problem(b._h, 0, qr.data_ptr(), qi.data_ptr(),
+                                               outs[0][0].data_ptr(), None, hf.PREC_MIXED))
+    with pytest.raises(hf.HFMMError):
+        _lib.check(_lib.lib.hfmm_batch_launch(b._h, None))
+    _lib.check(_lib.lib.hfmm_batch_capture(b._h))
+    b.launch()
+    torch.cuda.synchronize()
+    ref = hf.evaluate_field(states[0], q2, hf.PREC_MIXED)[0]
+    assert torch.equal(outs[0][0], ref)
+    b.close()
+    for st in states:
+        st.close()
+
+
+def test_autotune_writes_and_reuses_wisdom(tmp_path):
+    import hfmm_b200 as hf
+    from hfmm_b200.batch import autotune
+    probs = _batch_problems()
+    states = [hf.setup(x, k, p=p, N_max=32, stream_tables=True) for x, k, q, p in probs]
+    qs = [torch.as_tensor(q).cuda() for _, _, q, _ in probs]
+    w = tmp_path / "wisdom.json"
+    b, times = autotune(states, qs, candidates=(1, 2, 4), wisdom=str(w), reps=2)
+    store = json.loads(w.read_text())
+    assert len(store) == 1
+    entry = next(iter(store.values()))
+    assert entry["n_streams"] == b.n_streams and set(entry["ms"]) == {"1", "2", "4"}
+    assert b.n_streams == min(times, key=times.get)
+    b.close()
+    b2, t2 = autotune(states, qs, candidates=(1, 2, 4), wisdom=str(w))
+    assert b2.n_streams == entry["n_streams"] and t2 == entry["ms"]
+    b2.close()
+    for st in states:
+        st.close()
+
+
+def test_auto_batch_certifies_every_problem():
+    from hfmm_b200.batch import AutoBatch
+    probs = _batch_problems()[:3]
+    ab = AutoBatch([(x, k) for x, k, _, _ in probs], tol=1e-5, net=False, n_streams=2)
+    ab.bind([q for _, _, q, _ in probs], field=True)
+    ab.batch.launch()
+    rep = ab.certify()
+    assert all(r["certified"] for r in rep)
+    assert all(r["p"] == 10 for r in rep)
+    ab.close()
