@@ -3,12 +3,23 @@
 
 Default workload (the 1-GPU configuration the headline metric is quoted on):
 N = 1,000,000 points uniform in [0,1]^3, complex charges with re/im i.i.d.
-N(0,1), wavenumber k = 10, p = 12 surface points per cube edge (728 per box),
-leaf size 64, potential and field. Error against an FP64 direct sum on 1,024
-sampled targets is reported with every run.
+N(0,1), wavenumber k = 10 (k x domain = 10), potential and field, tolerance
+1e-6. The headline (``--mode auto``) is the certified evaluate: the
+expansion-order network picks p and the leaf size, the evaluate runs in mixed
+precision, and every step checks 256 sampled targets against the FP64 direct
+sum (rerunning plainly on a miss) inside the timed region. The plain FP64 path
+at the configuration's conservative p = 12 (728 surface points per box), leaf 64,
+is measured in the same run and reported beside it. Error against an FP64
+direct sum on 1,024 sampled targets is reported with every run.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--precision fp64|mixed] [--config c2|c1] [--n ..] [--p ..] ...
+                    [--mode auto|plain] [--precision fp64|mixed] [--config c2|c1|c4]
+                    [--n ..] [--p ..] [--tol ..] ...
+
+``--config c4`` is the batched workload: 64 problems with N log-uniform in
+[1e4, 5e5], uniform cube, k ~ U[1, 30], tolerance 1e-6, learned order, mixed
+precision, all evaluated by one CUDA-graph launch (value = total points / time
+of one launch).
 
 One process per GPU (torchrun for N > 1). The evaluate does not shard: every rank
 runs an independent replica of the workload ("replicas only"), the timing is the
@@ -41,6 +52,10 @@ CONFIGS = {
     "c1": dict(n=20_000, k=2 * np.pi, p=8, leaf=64, max_depth=None,
                workload="uniform cube, N=2e4, complex N(0,1) charges, k=2pi, p=8, leaf 64, "
                         "potential+field"),
+    "c4": dict(n=64, k=None, p=12, leaf=64, max_depth=None,
+               workload="64 problems, N log-uniform in [1e4, 5e5], uniform cube, k ~ U[1, 30], "
+                        "complex N(0,1) charges, tol 1e-6, learned p, mixed, one graph launch, "
+                        "potential+field"),
 }
 
 
@@ -50,6 +65,12 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--mode", choices=["auto", "plain"], default="auto",
+                    help="auto: learned order + mixed precision, certified (headline); "
+                         "plain: one fixed p and precision")
+    ap.add_argument("--tol", type=float, default=1e-6)
+    ap.add_argument("--no-plain", action="store_true",
+                    help="auto mode: skip the plain FP64 comparison run")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
     ap.add_argument("--config", choices=sorted(CONFIGS), default="c2")
     ap.add_argument("--n", type=int)
@@ -277,6 +298,39 @@ def measured_fp64_peak(torch):
     return best
 
 
+def measured_tf32_peak(torch):
+    """cuBLAS FP32 GEMM with TF32 tensor cores on this GPU (TFLOP/s): the roofline
+    of the 3xTF32 M2L, whose work is counted as three TF32 products."""
+    prev = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = True
+    try:
+        n = 8192
+        a = torch.randn(n, n, dtype=torch.float32, device="cuda")
+        b = torch.randn(n, n, dtype=torch.float32, device="cuda")
+        for _ in range(3):
+            a @ b
+        torch.cuda.synchronize()
+        best = 0.0
+        for _ in range(5):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            a @ b
+            e1.record()
+            e1.synchronize()
+            best = max(best, 2 * n ** 3 / (e0.elapsed_time(e1) * 1e-3) / 1e12)
+        del a, b
+        return best
+    finally:
+        torch.backends.cuda.matmul.allow_tf32 = prev
+
+
+def m2l_flops(state, R, NF):
+    """Algorithmic FLOPs of M2L alone per evaluate: one n_s x n_s product per V pair,
+    per charge column and kernel family."""
+    n_s = state.info["n_s"]
+    return 2.0 * n_s * n_s * R * NF * state.info["n_v"]
+
+
 def dominant_flops(state, R, NF):
     """Algorithmic FLOPs of the M2L+L2L GEMM phase per evaluate: each V pair and each
     L2L child is one n_s x n_s matrix times R charge columns, per kernel family."""
@@ -441,10 +495,273 @@ def run_ours(a, cfg, rank, world, local_rank):
     return out
 
 
+def _init_dist(world):
+    if world <= 1:
+        return None
+    import datetime
+    import torch.distributed as dist
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return dist
+
+
+def _max_over_ranks(dist, torch, dev, ms):
+    if not dist:
+        return ms
+    t = torch.tensor([ms], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def _timed(torch, stream, fn, steps):
+    """Mean CUDA-event milliseconds of ``fn`` over ``steps`` calls on ``stream``."""
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def run_auto(a, cfg, rank, world, local_rank):
+    """Headline: learned order + mixed precision, certified on 256 targets per step,
+    with the plain FP64 path at the configuration's p measured beside it."""
+    import torch
+    import hfmm_b200
+    from hfmm_b200 import _lib, learned
+    torch.cuda.set_device(local_rank)
+    dist = _init_dist(world)
+    dev = torch.device("cuda", local_rank)
+    stream = torch.cuda.current_stream(dev)
+    pos, q = make_problem(cfg, rank)
+    n = cfg["n"]
+    t0 = time.time()
+    ap = learned.AutoPlan(pos, cfg["k"], tol=a.tol, device=dev)
+    torch.cuda.synchronize()
+    setup_s = time.time() - t0
+    q_dev = torch.as_tensor(q).to(dev)
+    out_dev = {}
+
+    def step():
+        out_dev["r"] = ap.evaluate_field(q_dev)
+
+    for _ in range(a.warmup):
+        step()
+    st = ap.state
+    _lib.check(_lib.lib.hfmm_plan_set_profiling(st.handle, 1))
+    sampler = ClockSampler(local_rank) if rank == 0 else None
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    if sampler:
+        sampler.start()
+    launches0 = hfmm_b200.launch_count()
+    reports = []
+
+    def timed_step():
+        step()
+        reports.append(dict(ap.report))
+
+    ms = _timed(torch, stream, timed_step, a.steps)
+    launches = hfmm_b200.launch_count() - launches0
+    clocks = sampler.stop() if sampler else None
+    phase = np.zeros(_lib.N_PHASES)
+    _lib.check(_lib.lib.hfmm_plan_phase_times(st.handle, phase.ctypes.data))
+    phase /= a.steps
+    _lib.check(_lib.lib.hfmm_plan_set_profiling(st.handle, 0))
+    ms = _max_over_ranks(dist, torch, dev, ms)
+    phi, E = out_dev["r"]
+    tg = np.random.default_rng(42 + n + 1).choice(n, min(a.targets, n), replace=False)
+    d_phi, d_E = hfmm_b200.direct(st, q, tg, field=True)
+    rel = lambda x, y: float(np.linalg.norm(x - y) / np.linalg.norm(y))
+    phi_h, E_h = phi.cpu().numpy(), E.cpu().numpy()
+    acc = {"targets": int(len(tg)), "rel_l2_phi": rel(phi_h[tg], d_phi),
+           "rel_l2_field": rel(E_h[tg], d_E)}
+
+    e2e = None
+    if not a.no_e2e:          # the user's call: NumPy charges in, NumPy results out
+        ap.evaluate_field(q)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        ms_e2e = _timed(torch, stream, lambda: ap.evaluate_field(q), a.steps)
+        ms_e2e = _max_over_ranks(dist, torch, dev, ms_e2e)
+        e2e = {"value": world * n / (ms_e2e * 1e-3), "unit": "points/s",
+               "h2d_bytes_per_step": int(16 * n), "d2h_bytes_per_step": int(16 * n + 48 * n),
+               "ms_per_step": ms_e2e, "call": "AutoPlan.evaluate_field(numpy complex128 charges)"}
+
+    plain = None
+    if not a.no_plain:        # the plain FP64 path at the configuration's p, same points
+        sp = hfmm_b200.setup(pos, cfg["k"], p=cfg["p"], N_max=cfg["leaf"],
+                             max_depth=cfg["max_depth"], device=dev)
+        q_re = torch.as_tensor(q.real.copy()).to(dev)
+        q_im = torch.as_tensor(q.imag.copy()).to(dev)
+        pphi = torch.empty(n, dtype=torch.complex128, device=dev)
+        pE = torch.empty((n, 3), dtype=torch.complex128, device=dev)
+        pstep = lambda: hfmm_b200.evaluate_into(sp, q_re, q_im, pphi, pE, hfmm_b200.PREC_FP64,
+                                                 stream)
+        for _ in range(max(1, a.warmup)):
+            pstep()
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        pms = _max_over_ranks(dist, torch, dev, _timed(torch, stream, pstep, a.steps))
+        hfmm_b200.check_errors(sp)
+        plain = {"value": world * n / (pms * 1e-3), "unit": "points/s", "ms_per_step": pms,
+                 "p": cfg["p"], "leaf": cfg["leaf"], "precision": "fp64",
+                 "accuracy": {"rel_l2_phi": rel(pphi.cpu().numpy()[tg], d_phi),
+                              "rel_l2_field": rel(pE.cpu().numpy()[tg], d_E)}}
+        sp.close()
+        del pphi, pE
+
+    out = None
+    if rank == 0:
+        NF, R = st.n_families, 2
+        flops = 3.0 * m2l_flops(st, R, NF)
+        dom_ms = float(phase[_lib.PHASES.index("m2l_l2l_gemm")])
+        peak = measured_tf32_peak(torch)
+        achieved = flops / (dom_ms * 1e-3) / 1e12 if dom_ms > 0 else None
+        roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                "frac": (achieved / peak) if achieved else None, "traffic": _traffic(a, "auto"),
+                "kernel": "k_m2l_tf32x3 (M2L, 3xTF32 on tcgen05, all levels)",
+                "algorithmic_flops_per_evaluate": flops, "kernel_ms_per_evaluate": dom_ms,
+                "flop_count": "3 TF32 products x 2 n_s^2 per V pair, charge column and family",
+                "peak_source": "cuBLAS FP32 GEMM with TF32 tensor cores, 8192^3, measured in "
+                               "this run (of measured; MEASURED_PEAKS.json has no TF32 figure)"}
+        cpu = None
+        if not a.no_cpu and world == 1:
+            cores, blas = cpu_threads()
+            t_cpu, sample, _ = oracle_estimate(cfg, a.cpu_budget,
+                                               log=lambda *x: print(*x, file=sys.stderr))
+            cpu = {"value": n / t_cpu, "unit": "points/s", "cores": int(blas), "kind": "port",
+                   "sample": sample + f"; the reference's path at the configuration's p={cfg['p']}",
+                   "seconds_per_evaluate": t_cpu, "host_cores": cores}
+        last = reports[-1] if reports else ap.report
+        out = {
+            "metric": METRIC, "value": world * n / (ms * 1e-3), "unit": "points/s",
+            "n_gpus": world, "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32+tf32x3+f64",
+            "data": "synthetic (seeded uniform points and N(0,1) complex charges)",
+            "config": {"workload": f"uniform cube, N={n:.0e}, complex N(0,1) charges, "
+                                   f"k={cfg['k']:g}, tol {a.tol:g}, learned p and leaf, "
+                                   "mixed precision, certified on 256 targets, potential+field",
+                       "n_points": n, "k": cfg["k"], "tol": a.tol, "p": last["p"],
+                       "leaf": last["leaf"], "n_s": st.info["n_s"], "max_depth": st.max_depth,
+                       "precision": "mixed" if last["precision"] == 1 else "fp64",
+                       "parallelism": f"replicas x{world}",
+                       "l2": "inputs larger than L2 (operator tables and expansions of "
+                             f"{st.info['n_boxes']} boxes)"},
+            "certification": {"targets": int(len(ap.check_idx)), "tol": a.tol,
+                              "steps_certified": int(sum(r["certified"] for r in reports)),
+                              "steps_fallback": int(sum(r["fallback"] for r in reports)),
+                              "error_256": last["error"]},
+            "accuracy": acc, "setup_s": setup_s,
+            "phase_ms": {k: float(v) for k, v in zip(_lib.PHASES, phase)},
+            "plain_fp64": plain,
+            "speedup_vs_plain_fp64": (plain["ms_per_step"] / ms) if plain else None,
+            "gpu_launches": int(launches), "clocks": clocks, "e2e": e2e,
+            "roofline": roof, "cpu_baseline": cpu,
+        }
+    ap.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return out
+
+
+def c4_problems(seed=4):
+    """64 problems: N log-uniform in [1e4, 5e5], uniform cube, k ~ U[1, 30]."""
+    rng = np.random.default_rng(seed)
+    probs = []
+    for _ in range(64):
+        n = int(np.exp(rng.uniform(np.log(1e4), np.log(5e5))))
+        x = rng.uniform(0.0, 1.0, (n, 3))
+        k = float(rng.uniform(1.0, 30.0))
+        q = rng.normal(size=n) + 1j * rng.normal(size=n)
+        probs.append((x, k, q))
+    return probs
+
+
+def run_batch(a, cfg, rank, world, local_rank):
+    """C4: 64 problems as one graph launch; certification timed separately."""
+    import torch
+    import hfmm_b200
+    from hfmm_b200.batch import AutoBatch
+    torch.cuda.set_device(local_rank)
+    dist = _init_dist(world)
+    dev = torch.device("cuda", local_rank)
+    stream = torch.cuda.current_stream(dev)
+    probs = c4_problems(4 + rank)
+    n_tot = sum(len(x) for x, _, _ in probs)
+    t0 = time.time()
+    ab = AutoBatch([(x, k) for x, k, _ in probs], tol=a.tol, device=dev,
+                   wisdom=os.path.join(ROOT, "hfmm_b200", "data", "wisdom.json"))
+    ab.bind([q for _, _, q in probs], field=True)
+    torch.cuda.synchronize()
+    setup_s = time.time() - t0
+    for _ in range(a.warmup):
+        ab.batch.launch(stream)
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local_rank) if rank == 0 else None
+    if dist:
+        dist.barrier()
+    if sampler:
+        sampler.start()
+    launches0 = hfmm_b200.launch_count()
+    ms = _timed(torch, stream, lambda: ab.batch.launch(stream), a.steps)
+    launches = hfmm_b200.launch_count() - launches0
+    clocks = sampler.stop() if sampler else None
+    ms = _max_over_ranks(dist, torch, dev, ms)
+    t1 = time.time()
+    rep = ab.certify()
+    cert_s = time.time() - t1
+    out = None
+    if rank == 0:
+        ps = [c[0] for c in ab.choice]
+        out = {
+            "metric": METRIC + " (batched C4)", "value": world * n_tot / (ms * 1e-3),
+            "unit": "points/s", "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32+tf32x3+f64",
+            "data": "synthetic (seeded uniform points and N(0,1) complex charges)",
+            "config": {"workload": cfg["workload"], "problems": len(probs), "points_total": n_tot,
+                       "n_streams": ab.batch.n_streams, "p_chosen": ps, "tol": a.tol,
+                       "parallelism": f"replicas x{world}",
+                       "l2": "inputs larger than L2 (64 problems' expansions and workspaces)"},
+            "certification": {"certified": int(sum(r["certified"] for r in rep)),
+                              "fallback": int(sum(r["fallback"] for r in rep)),
+                              "max_error": float(max(r["error"] for r in rep)),
+                              "seconds_incl_plain_reruns": cert_s},
+            "setup_s": setup_s, "gpu_launches": int(launches), "clocks": clocks,
+            "e2e": None, "roofline": None, "cpu_baseline": None,
+            "note": "a step is one graph launch of all 64 evaluates; the per-problem "
+                    "256-target certification runs after the timed region"}
+    ab.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return out
+
+
+def _traffic(a, mode):
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if not os.path.exists(tpath):
+        return None
+    try:
+        return json.load(open(tpath)).get(f"{a.config}:{mode}")
+    except Exception:
+        return None
+
+
 def run_reference(a, cfg, rank, world):
     """The reference arm: the oracle timed on this host's cores (rank 0 only)."""
     if rank != 0:
         return None
+    if a.config == "c4":
+        return {"impl": "reference",
+                "unavailable": "the reference has no batched evaluate (one problem per "
+                               "HFMM.evaluate call); time --config c2 for the reference arm"}
     cores, blas = cpu_threads()
     times, sample = [], None
     budget = max(2.0, min(a.cpu_budget, 240.0 / max(1, a.steps + a.warmup)))
@@ -475,6 +792,10 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if a.impl == "reference":
         out = run_reference(a, cfg, rank, world)
+    elif a.config == "c4":
+        out = run_batch(a, cfg, rank, world, local_rank)
+    elif a.mode == "auto":
+        out = run_auto(a, cfg, rank, world, local_rank)
     else:
         out = run_ours(a, cfg, rank, world, local_rank)
     if rank == 0 and out is not None:

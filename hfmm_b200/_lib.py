@@ -13,9 +13,9 @@ LIB_PATH = os.path.join(_HERE, "_lib", "libhfmm_b200.so")
 HFMM_OK = 0
 HFMM_PREC_FP64 = 0
 HFMM_PREC_MIXED = 1
-N_PHASES = 13
+N_PHASES = 14
 PHASES = ("gather", "p2m", "m2m_gemm", "up_decode", "m2l_l2l_gemm", "p2l", "down_decode",
-          "p2p", "l2p", "m2p", "combine", "tf32_split", "m2l_tables")
+          "p2p", "l2p", "m2p", "combine", "tf32_split", "m2l_tables", "l2l_gemm")
 
 _c_i32, _c_i64, _c_dbl, _c_vp = ctypes.c_int32, ctypes.c_int64, ctypes.c_double, ctypes.c_void_p
 

@@ -290,7 +290,7 @@ void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double*
     auto gemm = [&](int kind, int l, const hfmm_plan::Tiles& tiles, const int32_t* src_tab,
                     int src_ld, const double* B0, const double* B1, double* out,
                     const double* scale_set) {
-        PhaseTimer pt(X, s, kind == K_M2M ? 2 : (kind == K_DN || kind == K_L2L) ? 4 : (kind <= K_UPV ? 3 : 6));
+        PhaseTimer pt(X, s, kind == K_M2M ? 2 : kind == K_DN ? 4 : kind == K_L2L ? 13 : (kind <= K_UPV ? 3 : 6));
         GemmCall c{};
         c.tile_tgt = tiles.tgt.p;
         c.ntiles = tiles.ntiles;
@@ -372,7 +372,6 @@ void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double*
             generate_m2l_stream(P, l, use_mx, P->ws, s);
         }
         if (use_mx) {
-            PhaseTimer pt(X, s, 4);
             MixedCall mc{};
             mc.tile_tgt = P->mx_tiles[l][R - 1].tgt.p;
             mc.ntiles = P->mx_tiles[l][R - 1].ntiles;
@@ -391,7 +390,10 @@ void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double*
             mc.out_fam_stride = fs;
             mc.nb = P->nb;
             mc.err = P->d_err.p;
-            m2l_tf32x3(static_cast<MixedMaps*>(P->mx_maps)[l], mc, s);
+            {
+                PhaseTimer pt(X, s, 4);
+                m2l_tf32x3(static_cast<MixedMaps*>(P->mx_maps)[l], mc, s);
+            }
             if (l >= 3)   // L2L (phases.py:273-278) in FP64, added to the check potential
                 gemm(K_L2L, l, P->dn_tiles[l][R - 1], P->m2l_src.p + N_DISP, M2L_ENTRIES, P->loc.p,
                      nullptr, P->check.p, nullptr);

@@ -46,7 +46,10 @@ constexpr int TILE_BYTES = BM * BK * 4;   // 16 KiB, one operand half
 constexpr int STAGE_BYTES = 4 * TILE_BYTES;
 constexpr int THREADS = 320;       // warps 0-3 gather, 4 TMA, 5 MMA, 6-9 accumulate
 constexpr int TMEM_COLS = 512;
-constexpr int FOLD = 2;            // k-chunks per FP32 accumulation unit
+#ifndef HFMM_MX_FOLD
+#define HFMM_MX_FOLD 2
+#endif
+constexpr int FOLD = HFMM_MX_FOLD;   // k-chunks per FP32 accumulation unit
 constexpr uint64_t WAIT_NS = 2000000000ull;   // bounded waits: 2 s
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {

@@ -168,11 +168,12 @@ int hfmm_direct_noalloc(const double* pos_dev, const double* q_re_dev, const dou
  * stream. hfmm_plan_phase_times synchronises and writes the milliseconds spent
  * per phase, summed over every evaluate since profiling was enabled or the
  * previous read (up to 8192 phase instances): 0 charge gather, 1 P2M, 2 M2M GEMM, 3 upward decode,
- * 4 M2L+L2L GEMM, 5 X-list P2L, 6 downward decode, 7 P2P, 8 L2P, 9 W-list M2P,
- * 10 combine, 11 TF32 splits of the mixed path, 12 M2L table generation of a
- * streaming plan. (Replaces the reference's wall-clock phase prints; it has no
- * per-phase timers, util.py:692-724.) */
-#define HFMM_N_PHASES 13
+ * 4 M2L (with L2L fused on the FP64 path), 5 X-list P2L, 6 downward decode,
+ * 7 P2P, 8 L2P, 9 W-list M2P, 10 combine, 11 TF32 splits of the mixed path,
+ * 12 M2L table generation of a streaming plan, 13 the FP64 L2L GEMM of the mixed
+ * path. (Replaces the reference's wall-clock phase prints; it has no per-phase
+ * timers, util.py:692-724.) */
+#define HFMM_N_PHASES 14
 int hfmm_plan_set_profiling(hfmm_plan* plan, int32_t enable);
 int hfmm_plan_phase_times(hfmm_plan* plan, double* ms_out);
 

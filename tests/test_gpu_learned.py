@@ -30,8 +30,9 @@ def _rel(a, b):
 def test_forward_matches_oracle():
     from hfmm_b200 import _lib
     P, X, _ = _data()
+    Pd, Xd = _dev(P), _dev(X)       # held: the call reads them
     Y = torch.empty((len(X), N_OUT), dtype=torch.float32, device="cuda")
-    assert _lib.lib.hfmm_mlp_forward(_dev(P).data_ptr(), _dev(X).data_ptr(), len(X), N_IN, N_OUT,
+    assert _lib.lib.hfmm_mlp_forward(Pd.data_ptr(), Xd.data_ptr(), len(X), N_IN, N_OUT,
                                      Y.data_ptr(), None) == 0
     ref, _ = om.forward(P.astype(np.float64), X, N_OUT)
     assert _rel(Y.cpu().numpy(), ref) < 1e-5
@@ -41,9 +42,10 @@ def test_forward_matches_oracle():
 def test_gradient_matches_oracle(n):
     from hfmm_b200 import _lib
     P, X, T = _data(n, seed=n)
+    Pd, Xd, Td = _dev(P), _dev(X), _dev(T)
     G = torch.empty(len(P), dtype=torch.float32, device="cuda")
     loss = _lib.ctypes.c_double()
-    assert _lib.lib.hfmm_mlp_grad(_dev(P).data_ptr(), _dev(X).data_ptr(), _dev(T).data_ptr(), n,
+    assert _lib.lib.hfmm_mlp_grad(Pd.data_ptr(), Xd.data_ptr(), Td.data_ptr(), n,
                                   N_IN, N_OUT, G.data_ptr(), _lib.ctypes.byref(loss), None) == 0
     l_ref, g_ref = om.loss_grad(P.astype(np.float64), X, T, N_OUT)
     assert loss.value == pytest.approx(l_ref, rel=1e-5)
@@ -54,10 +56,11 @@ def test_adam_steps_match_oracle():
     from hfmm_b200 import _lib
     P, X, T = _data(256, seed=3)
     p, m, v = _dev(P), torch.zeros(len(P), device="cuda"), torch.zeros(len(P), device="cuda")
+    Xd, Td = _dev(X), _dev(T)
     loss = _lib.ctypes.c_double()
     for t0 in (0, 3):           # two calls continue one optimiser run
         assert _lib.lib.hfmm_mlp_train(p.data_ptr(), m.data_ptr(), v.data_ptr(), t0,
-                                       _dev(X).data_ptr(), _dev(T).data_ptr(), len(X), N_IN, N_OUT,
+                                       Xd.data_ptr(), Td.data_ptr(), len(X), N_IN, N_OUT,
                                        3, 1e-3, _lib.ctypes.byref(loss), None) == 0
     P_ref, m_ref, _, l_ref = om.adam(P.astype(np.float64), X, T, N_OUT, steps=6, lr=1e-3)
     got = p.cpu().numpy()
