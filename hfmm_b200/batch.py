@@ -164,11 +164,11 @@ class AutoBatch:
                  device=None, margin=0.5, wisdom=None):
         from . import setup, _device
         from .learned import (OrderNet, features_for, conservative_p, precision_for,
-                              FEATURE_LEAF)
+                              FEATURE_LEAF, TOL_LEARNED)
         self.tol = float(tol)
         self.device = _device(device)
         self.problems = problems
-        if net is False:
+        if net is False or self.tol < TOL_LEARNED:
             choice = [(conservative_p(self.tol), FEATURE_LEAF)] * len(problems)
         else:
             net = OrderNet.load(device=self.device) if net is None else net

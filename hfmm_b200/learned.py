@@ -36,6 +36,7 @@ P_MIN, P_MAX = 4, 16
 LEAVES = (16, 32, 64, 128)
 FEATURE_LEAF = 64          # the tree the features are read from
 TOL_MIXED = 1e-6           # the mixed-precision path is used at tolerances >= this
+TOL_LEARNED = 3e-7         # below this the network is not consulted (outside its training range)
 DEFAULT_WEIGHTS = os.path.join(os.path.dirname(__file__), "data", "order_net.npz")
 
 
@@ -234,7 +235,7 @@ class AutoPlan:
         self.device = _device(device)
         self.positions = positions
         self.p_plain = conservative_p(self.tol)
-        if net is False:
+        if net is False or self.tol < TOL_LEARNED:
             self.p, self.leaf, self.feats = self.p_plain, FEATURE_LEAF, None
         else:
             net = OrderNet.load(device=self.device) if net is None else net

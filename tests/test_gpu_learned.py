@@ -121,3 +121,65 @@ def test_auto_plan_reruns_plainly_on_a_miss():
     assert np.linalg.norm(phi - ref) <= 1e-13 * np.linalg.norm(ref)
     st.close()
     ap.close()
+
+
+def test_gpu_training_generalises_across_problems():
+    """Cross-validation on the committed sweep with the CUDA kernels: the held-out
+    p error stays well under one order (the CPU oracle run of the same recipe gives 0.29)."""
+    import os
+    from hfmm_b200 import train_order as to
+    data = dict(np.load(os.path.join(os.path.dirname(to.__file__), "data", "order_sweep.npz")))
+    cvs = to.cross_validate(data, steps_list=(400,), device="cuda")
+    r = cvs[400]
+    assert r["p_mae"] < 0.5, r
+    assert r["under@0.5"] < 0.08, r
+    assert r["leaf_acc"] > 0.6, r
+
+
+def test_bundled_network_predicts_the_regime():
+    from hfmm_b200.learned import OrderNet, features_for
+    net = OrderNet.load(device="cuda")
+    rng = np.random.default_rng(7)
+    x = rng.random((200000, 3))
+    f6 = features_for(x, 10.0, 1e-6)
+    f3 = features_for(x, 10.0, 1e-3)
+    p6 = net.predict(f6)[0, 0]
+    p3 = net.predict(f3)[0, 0]
+    assert 6.0 <= p6 <= 9.5, p6          # the sweep's labels at 1e-6 span 6.6 .. 8.4
+    assert p3 < p6                         # a looser tolerance needs a lower order
+
+
+def _time_eval(ap, q, reps=3):
+    ap.evaluate_field(q)
+    s = torch.cuda.current_stream()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(s)
+    for _ in range(reps):
+        ap.evaluate_field(q)
+    b.record(s)
+    b.synchronize()
+    return a.elapsed_time(b) / reps
+
+
+def test_ablation_network_beats_conservative_order():
+    """What the trained network gains over the method without it: the same
+    certified evaluate (mixed precision, 256-target check) with the conservative
+    order in place of the network's."""
+    from hfmm_b200.learned import AutoPlan
+    rng = np.random.default_rng(11)
+    n = 200000
+    x = rng.random((n, 3))
+    q = torch.as_tensor(rng.standard_normal(n) + 1j * rng.standard_normal(n)).cuda()
+    learned = AutoPlan(x, 10.0, tol=1e-6)
+    plain = AutoPlan(x, 10.0, tol=1e-6, net=False)
+    t_l = _time_eval(learned, q)
+    t_c = _time_eval(plain, q)
+    rl, rc = learned.report, plain.report
+    assert rl["certified"] and rc["certified"], (rl, rc)
+    assert not rl["fallback"], rl
+    assert rl["p"] < rc["p"] == 12, (rl, rc)
+    assert t_l < 0.67 * t_c, (t_l, t_c, rl, rc)
+    print(f"ablation: learned p={rl['p']} leaf={rl['leaf']} {t_l:.1f} ms, err {rl['error']:.2e}; "
+          f"conservative p={rc['p']} {t_c:.1f} ms, err {rc['error']:.2e}")
+    learned.close()
+    plain.close()
