@@ -155,6 +155,7 @@ EvalView view(hfmm_plan* P) {
     v.ld = P->ld;
     v.k = P->k;
     v.pos_s = P->pos_s.p;
+    v.pos_f = P->pos_f.p;
     v.q_s = P->q_s.p;
     v.leaf_start = P->leaf_start.p;
     v.counts = P->counts.p;

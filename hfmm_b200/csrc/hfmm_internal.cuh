@@ -114,6 +114,7 @@ struct hfmm_plan {
 
     // particles (Morton-sorted order == leaf-major order)
     hfmm::DevBuf<double> pos_s;       // 3 x n SoA (x | y | z)
+    hfmm::DevBuf<float> pos_f;        // 6 x n: hi(x|y|z) then lo(x|y|z), pos = hi + lo
     hfmm::DevBuf<int32_t> sort_idx;   // sorted slot -> original index
     hfmm::DevBuf<int32_t> rank;       // original index -> sorted slot
 

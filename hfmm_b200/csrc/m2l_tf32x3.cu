@@ -20,10 +20,14 @@
 // Accumulation precision: the error of an FP32 accumulator grows with the
 // length of its chain of MMAs (measured: about linearly), and the damped decode
 // amplifies it. So every FOLD k-chunks (24 MMAs) accumulate into a fresh FP32
-// buffer in TMEM (two buffers alternate), and warps 6-9 fold each finished
-// buffer into an FP64 running sum kept in TMEM (two 32-bit columns per double)
-// while the tensor core fills the other buffer. TMEM: 2 x 128 FP32 columns + 256 for the FP64
-// sums = 512 columns. The FP64 sums are stored as the check potentials.
+// buffer in TMEM (two buffers alternate), and the fold warps (8: two per TMEM lane
+// quadrant, each taking half the columns; measured 13 % faster than 4 on the
+// 1M-point p = 8 M2L, with the same bits) fold each finished buffer into an FP64
+// running sum kept in TMEM (two 32-bit columns per double) while the tensor core
+// fills the other buffer. TMEM: 2 x 128 FP32 columns + 256 for the FP64 sums =
+// 512 columns. The FP64 sums are stored as the check potentials. (Folding every
+// 4 k-chunks instead was 22 % faster but doubled the M2L error: 8.3e-7 against
+// 4.6e-7 for the potential at p = 8.)
 // Every mbarrier wait is bounded (2 s of %globaltimer); a timeout sets the
 // device error flag and every role drains and exits, TMEM is freed.
 #include "hfmm_internal.cuh"
@@ -44,7 +48,14 @@ constexpr int BK = 32;           // fp32 elements per k-chunk (128-byte rows)
 constexpr int STAGES = 3;
 constexpr int TILE_BYTES = BM * BK * 4;   // 16 KiB, one operand half
 constexpr int STAGE_BYTES = 4 * TILE_BYTES;
-constexpr int THREADS = 320;       // warps 0-3 gather, 4 TMA, 5 MMA, 6-9 accumulate
+#ifndef HFMM_MX_FOLD_WARPS
+#define HFMM_MX_FOLD_WARPS 8
+#endif
+constexpr int N_FOLD_WARPS = HFMM_MX_FOLD_WARPS;   // 4, 8 or 16: NFW/4 per TMEM lane quadrant
+constexpr int THREADS = (6 + N_FOLD_WARPS) * 32;  // warps 0-3 gather, 4 TMA, 5 MMA, 6.. fold
+constexpr int COLS_PER_FOLD_WARP = BN * 4 / N_FOLD_WARPS;
+constexpr int SUB = N_FOLD_WARPS >= 16 ? 16 : 32;  // columns per TMEM access of a fold warp
+static_assert(N_FOLD_WARPS == 4 || N_FOLD_WARPS == 8 || N_FOLD_WARPS == 16, "fold warps");
 constexpr int TMEM_COLS = 512;
 #ifndef HFMM_MX_FOLD
 #define HFMM_MX_FOLD 2
@@ -145,6 +156,36 @@ __device__ __forceinline__ void tmem_st32(uint32_t taddr, const uint32_t* v) {
         : "memory");
 }
 
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t* v) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,"
+        "%14,%15}, [%16];"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+          "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
+          "=r"(v[14]), "=r"(v[15])
+        : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t* v) {
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,"
+        "%13,%14,%15,%16};" ::"r"(taddr),
+        "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7]),
+        "r"(v[8]), "r"(v[9]), "r"(v[10]), "r"(v[11]), "r"(v[12]), "r"(v[13]), "r"(v[14]),
+        "r"(v[15])
+        : "memory");
+}
+// n consecutive 32-bit TMEM columns of this warp's 32 lanes (n = 16 or 32)
+template <int n>
+__device__ __forceinline__ void tmem_ld(uint32_t taddr, uint32_t* v) {
+    if constexpr (n == 32) tmem_ld32(taddr, v);
+    else tmem_ld16(taddr, v);
+}
+template <int n>
+__device__ __forceinline__ void tmem_st(uint32_t taddr, const uint32_t* v) {
+    if constexpr (n == 32) tmem_st32(taddr, v);
+    else tmem_st16(taddr, v);
+}
+
 // Instruction descriptor: D = F32, A = B = TF32, both K-major, M = 128, N = BN.
 constexpr uint32_t IDESC = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(BN >> 3) << 17) |
                            ((uint32_t)(BM >> 4) << 24);
@@ -189,7 +230,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_m2l_tf32x3(const __grid_constant
         }
         for (int b = 0; b < 2; ++b) {
             mbar_init(smem_u32(&ctl.acc_full[b]), 1);
-            mbar_init(smem_u32(&ctl.acc_empty[b]), 128);
+            mbar_init(smem_u32(&ctl.acc_empty[b]), 32 * N_FOLD_WARPS);
         }
         mbar_init(smem_u32(&ctl.done), 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -290,7 +331,10 @@ __global__ void __launch_bounds__(THREADS, 1) k_m2l_tf32x3(const __grid_constant
         }
     } else if (warp >= 6) {
         // ---------------- fold entries into the FP64 sums; store at the end
+        // Warp w may touch TMEM lanes 32 (w % 4) .. + 31 only: the NFW fold warps
+        // cover each lane quadrant NFW / 4 times, each folding its share of columns.
         const int quad = warp & 3;                 // TMEM lane quadrant of this warp
+        const int c_lo = ((warp - 6) >> 2) * COLS_PER_FOLD_WARP;
         const int m = m0 + quad * 32 + lane;
         const uint32_t lane_base = tmem + ((uint32_t)(quad * 32) << 16);
         double* out = c.out + (int64_t)fam * c.out_fam_stride;
@@ -305,24 +349,24 @@ __global__ void __launch_bounds__(THREADS, 1) k_m2l_tf32x3(const __grid_constant
                 break;
             }
             asm volatile("tcgen05.fence::after_thread_sync;");
-            for (int cc = 0; cc < BN / 32; ++cc) {
-                uint32_t v[32];
-                tmem_ld32(lane_base + b * BN + cc * 32, v);
-                uint32_t w[64];
+            for (int cb = c_lo; cb < c_lo + COLS_PER_FOLD_WARP; cb += SUB) {
+                uint32_t v[SUB];
+                tmem_ld<SUB>(lane_base + b * BN + cb, v);
+                uint32_t w[2 * SUB];
                 if (i > 0) {
-                    tmem_ld32(lane_base + 2 * BN + cc * 64, w);
-                    tmem_ld32(lane_base + 2 * BN + cc * 64 + 32, w + 32);
+                    tmem_ld<SUB>(lane_base + 2 * BN + 2 * cb, w);
+                    tmem_ld<SUB>(lane_base + 2 * BN + 2 * cb + SUB, w + SUB);
                 }
                 asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-                for (int j = 0; j < 32; ++j) {
+                for (int j = 0; j < SUB; ++j) {
                     double acc = (double)__uint_as_float(v[j]);
                     if (i > 0) acc += __hiloint2double((int)w[2 * j + 1], (int)w[2 * j]);
                     w[2 * j] = (uint32_t)__double2loint(acc);
                     w[2 * j + 1] = (uint32_t)__double2hiint(acc);
                 }
-                tmem_st32(lane_base + 2 * BN + cc * 64, w);
-                tmem_st32(lane_base + 2 * BN + cc * 64 + 32, w + 32);
+                tmem_st<SUB>(lane_base + 2 * BN + 2 * cb, w);
+                tmem_st<SUB>(lane_base + 2 * BN + 2 * cb + SUB, w + SUB);
             }
             asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
             asm volatile("tcgen05.fence::before_thread_sync;");
@@ -332,16 +376,16 @@ __global__ void __launch_bounds__(THREADS, 1) k_m2l_tf32x3(const __grid_constant
         if (aborted) {
             if (lane == 0) atomicOr(c.err, ERRF_TIMEOUT);
         } else if (m0 + quad * 32 < c.ld) {   // ld % 32 == 0: a warp is all in or all out
-            for (int cc = 0; cc < BN / 32; ++cc) {
-                uint32_t w[64];
+            for (int cb = c_lo; cb < c_lo + COLS_PER_FOLD_WARP; cb += SUB) {
+                uint32_t w[2 * SUB];
                 if (nq > 0) {
-                    tmem_ld32(lane_base + 2 * BN + cc * 64, w);
-                    tmem_ld32(lane_base + 2 * BN + cc * 64 + 32, w + 32);
+                    tmem_ld<SUB>(lane_base + 2 * BN + 2 * cb, w);
+                    tmem_ld<SUB>(lane_base + 2 * BN + 2 * cb + SUB, w + SUB);
                     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
                 }
 #pragma unroll
-                for (int j = 0; j < 32; ++j) {
-                    const int n = cc * 32 + j;
+                for (int j = 0; j < SUB; ++j) {
+                    const int n = cb + j;
                     const int t = ctl.tgt[n / R];
                     const double val = nq > 0 ? __hiloint2double((int)w[2 * j + 1], (int)w[2 * j]) : 0.0;
                     if (t >= 0) out[((int64_t)t * R + (n % R)) * c.ld + m] = val;

@@ -9,6 +9,7 @@ struct EvalView {
     int n_s, ld;
     double k;
     const double* pos_s;       // 3 x n, leaf-major sorted
+    const float* pos_f;        // 6 x n: FP32 hi parts x|y|z, then lo parts (pos = hi + lo)
     const double* q_s;         // R x n, leaf-major sorted
     const int32_t* leaf_start;
     const int32_t* counts;

@@ -436,6 +436,18 @@ BuildResult build_depth(int64_t n, int md, int n_max, const DevBuf<uint64_t>& sk
 
 }  // namespace
 
+// Positions as FP32 pairs: hi = fl32(x), lo = fl32(x - hi); hi + lo carries x to
+// about 48 bits, and a separation formed as (hi - hi') + (lo - lo') in FP32 has the
+// relative accuracy of an FP32 number however close the two points are.
+__global__ void k_split_pos(const double* __restrict__ pos, int64_t m, float* out) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= m) return;
+    const double x = pos[i];
+    const float hi = (float)x;
+    out[i] = hi;
+    out[m + i] = (float)(x - (double)hi);
+}
+
 void tree_build(hfmm_plan* P, const double* pos_dev) {
     const int64_t n = P->n;
     int* d_err = P->d_err.p;
@@ -587,6 +599,8 @@ void tree_build(hfmm_plan* P, const double* pos_dev) {
         }
         if (at != n) throw Error{HFMM_ERR_STATE, "tree: leaves do not cover every particle"};
     }
+    P->pos_f.alloc(6 * (size_t)n);
+    HFMM_LAUNCH(k_split_pos, nblocks(3 * n), TPB, 0, 0, P->pos_s.p, 3 * n, P->pos_f.p);
     P->rmax.alloc(nb);
     HFMM_LAUNCH(k_rmax, nblocks(nb), TPB, 0, 0, pos_dev, P->pos_s.p, P->leaf_start.p, P->counts.p,
                 n, nb, P->maxleaf, P->rmax.p);

@@ -248,6 +248,7 @@ class AutoPlan:
         self.check_idx = np.sort(rng.choice(n, size=min(n_check, n), replace=False)).astype(np.int32)
         self._check_dev = torch.as_tensor(self.check_idx).to(self.device)
         self._plain = {}
+        self._pin = {}
         self.report = {}
 
     def _direct(self, q_re, q_im, field):
@@ -279,7 +280,16 @@ class AutoPlan:
         numpy_in = not isinstance(charges, torch.Tensor)
         dev = self.device
         with torch.cuda.device(dev):
-            q = torch.as_tensor(np.asarray(charges)).to(dev) if numpy_in else charges.to(dev)
+            if numpy_in:      # through pinned staging: pageable copies run far slower
+                qn = np.asarray(charges)
+                if qn.shape != (self.state.n,):
+                    raise ValueError(f"charges must have shape ({self.state.n},)")
+                qp = self._pinned("q", qn.shape, torch.complex128 if np.iscomplexobj(qn)
+                                  else torch.float64)
+                qp.numpy()[...] = qn
+                q = qp.to(dev, non_blocking=True)
+            else:
+                q = charges.to(dev)
             if q.is_complex():
                 q_re, q_im = q.real.double().contiguous(), q.imag.double().contiguous()
             else:
@@ -304,8 +314,22 @@ class AutoPlan:
             rep["certified"] = bool(err <= self.tol)
             self.report = rep
         if numpy_in:
-            return phi.cpu().numpy(), (E.cpu().numpy() if E is not None else None)
+            php = self._pinned("phi", phi.shape, phi.dtype)
+            php.copy_(phi, non_blocking=True)
+            if E is not None:
+                Ep = self._pinned("E", E.shape, E.dtype)
+                Ep.copy_(E, non_blocking=True)
+            torch.cuda.current_stream(dev).synchronize()
+            return php.numpy().copy(), (Ep.numpy().copy() if E is not None else None)
         return phi, E
+
+    def _pinned(self, name, shape, dtype):
+        """A reused page-locked host buffer (one per role, shape and dtype)."""
+        t = self._pin.get(name)
+        if t is None or tuple(t.shape) != tuple(shape) or t.dtype != dtype:
+            t = torch.empty(tuple(shape), dtype=dtype, pin_memory=True)
+            self._pin[name] = t
+        return t
 
     def evaluate(self, charges):
         return self.evaluate_field(charges, field=False)[0]

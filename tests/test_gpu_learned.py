@@ -90,6 +90,16 @@ def _problem(n=6000, seed=0):
     return x, q
 
 
+def test_auto_plan_below_the_learned_range_uses_the_conservative_order():
+    from hfmm_b200.learned import AutoPlan, TOL_LEARNED
+    x, q = _problem(3000, seed=3)
+    ap = AutoPlan(x, 3.0, tol=TOL_LEARNED / 2)       # the network is not consulted
+    assert ap.feats is None and ap.p == 14
+    ap.evaluate(q)
+    assert ap.report["p"] == 14
+    ap.close()
+
+
 def test_auto_plan_conservative_certifies():
     from hfmm_b200.learned import AutoPlan
     x, q = _problem()
@@ -102,18 +112,18 @@ def test_auto_plan_conservative_certifies():
 
 
 def test_auto_plan_reruns_plainly_on_a_miss():
-    """A network that asks for the lowest order misses 1e-7; the plain rerun certifies."""
+    """A network that asks for the lowest order misses 1e-6; the plain rerun certifies."""
     from hfmm_b200.learned import AutoPlan, OrderNet, N_FEATURES, N_OUTPUTS
     import hfmm_b200 as hf
     net = OrderNet(np.zeros(om.param_count(N_FEATURES, N_OUTPUTS), np.float32),
                    np.zeros(N_FEATURES), np.ones(N_FEATURES), np.array([2.0, 6.0]),
                    np.ones(2), device="cuda")
     x, q = _problem(seed=1)
-    ap = AutoPlan(x, 4.0, tol=1e-7, net=net)
+    ap = AutoPlan(x, 4.0, tol=1e-6, net=net)
     assert ap.p == 4 and ap.leaf == 64
     phi = ap.evaluate(q)
     rep = ap.report
-    assert rep["fallback"] and rep["certified"] and rep["p_final"] >= 14
+    assert rep["fallback"] and rep["certified"] and rep["p_final"] == 12
     assert rep["precision"] == hf.PREC_FP64
     # the returned potential is the plain evaluate's, checked on other targets too
     st = hf.setup(x, 4.0, p=rep["p_final"], N_max=64)
