@@ -117,7 +117,9 @@ class ClockSampler:
         self.rows = []
         self.proc = None
 
-    def start(self):
+    def start(self, settle_s=3.0):
+        """Start sampling and wait for the first sample (nvidia-smi's start-up would
+        otherwise overlap the first timed steps)."""
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}",
@@ -127,6 +129,10 @@ class ClockSampler:
             self.t.start()
         except Exception:
             self.proc = None
+            return
+        t0 = time.time()
+        while not self.rows and time.time() - t0 < settle_s:
+            time.sleep(0.05)
 
     def _read(self):
         for line in self.proc.stdout:
@@ -372,13 +378,15 @@ def run_ours(a, cfg, rank, world, local_rank):
     for _ in range(a.warmup):
         step()
     hfmm_b200.check_errors(st)
-    _lib.check(_lib.lib.hfmm_plan_set_profiling(st.handle, 1))
     sampler = ClockSampler(local_rank) if rank == 0 else None
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
     if sampler:
         sampler.start()
+        step()
+        torch.cuda.synchronize()
+    _lib.check(_lib.lib.hfmm_plan_set_profiling(st.handle, 1))
     launches0 = hfmm_b200.launch_count()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
@@ -548,13 +556,15 @@ def run_auto(a, cfg, rank, world, local_rank):
     for _ in range(a.warmup):
         step()
     st = ap.state
-    _lib.check(_lib.lib.hfmm_plan_set_profiling(st.handle, 1))
     sampler = ClockSampler(local_rank) if rank == 0 else None
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
     if sampler:
         sampler.start()
+        step()
+        torch.cuda.synchronize()
+    _lib.check(_lib.lib.hfmm_plan_set_profiling(st.handle, 1))
     launches0 = hfmm_b200.launch_count()
     reports = []
 
@@ -708,9 +718,10 @@ def run_batch(a, cfg, rank, world, local_rank):
         dist.barrier()
     if sampler:
         sampler.start()
-    launches0 = hfmm_b200.launch_count()
+        ab.batch.launch(stream)
+        torch.cuda.synchronize()
     ms = _timed(torch, stream, lambda: ab.batch.launch(stream), a.steps)
-    launches = hfmm_b200.launch_count() - launches0
+    launches = ab.batch.kernels_per_launch * a.steps   # kernels replayed by the graph
     clocks = sampler.stop() if sampler else None
     ms = _max_over_ranks(dist, torch, dev, ms)
     t1 = time.time()

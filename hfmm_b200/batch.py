@@ -73,7 +73,9 @@ class Batch:
             self._keep.append((q_re, q_im))
             self.outputs.append((phi, E))
         with torch.cuda.device(self.states[0].device):
+            before = _lib.launch_count()
             _check(_lib.lib.hfmm_batch_capture(self._h))
+            self.kernels_per_launch = _lib.launch_count() - before   # kernels in the graph
         return self.outputs
 
     def launch(self, stream=None):

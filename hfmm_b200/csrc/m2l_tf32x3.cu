@@ -20,9 +20,10 @@
 // Accumulation precision: the error of an FP32 accumulator grows with the
 // length of its chain of MMAs (measured: about linearly), and the damped decode
 // amplifies it. So every FOLD k-chunks (24 MMAs) accumulate into a fresh FP32
-// buffer in TMEM (two buffers alternate), and the fold warps (8: two per TMEM lane
-// quadrant, each taking half the columns; measured 13 % faster than 4 on the
-// 1M-point p = 8 M2L, with the same bits) fold each finished buffer into an FP64
+// buffer in TMEM (two buffers alternate), and the fold warps (16: four per TMEM lane
+// quadrant, each taking a quarter of the columns; on the 1M-point p = 8 M2L, 8 fold
+// warps were 14 % faster than 4 and 16 another 3 %, all with the same bits) fold each
+// finished buffer into an FP64
 // running sum kept in TMEM (two 32-bit columns per double) while the tensor core
 // fills the other buffer. TMEM: 2 x 128 FP32 columns + 256 for the FP64 sums =
 // 512 columns. The FP64 sums are stored as the check potentials. (Folding every
@@ -49,7 +50,7 @@ constexpr int STAGES = 3;
 constexpr int TILE_BYTES = BM * BK * 4;   // 16 KiB, one operand half
 constexpr int STAGE_BYTES = 4 * TILE_BYTES;
 #ifndef HFMM_MX_FOLD_WARPS
-#define HFMM_MX_FOLD_WARPS 8
+#define HFMM_MX_FOLD_WARPS 16
 #endif
 constexpr int N_FOLD_WARPS = HFMM_MX_FOLD_WARPS;   // 4, 8 or 16: NFW/4 per TMEM lane quadrant
 constexpr int THREADS = (6 + N_FOLD_WARPS) * 32;  // warps 0-3 gather, 4 TMA, 5 MMA, 6.. fold
@@ -201,6 +202,7 @@ struct __align__(8) Ctl {
     int n_act;
     int tgt[BN];
     short act[M2L_ENTRIES + 1];
+    short zidx[M2L_ENTRIES + 1];   // A-table index of each active entry (M2L or L2L table)
 };
 
 template <int R>
@@ -257,7 +259,11 @@ __global__ void __launch_bounds__(THREADS, 1) k_m2l_tf32x3(const __grid_constant
                 }
             }
             unsigned bal = __ballot_sync(0xffffffffu, act);
-            if (act) ctl.act[base + __popc(bal & ((1u << lane) - 1))] = (short)e;
+            if (act) {
+                const int slot = base + __popc(bal & ((1u << lane) - 1));
+                ctl.act[slot] = (short)e;
+                ctl.zidx[slot] = (short)(e < N_DISP ? c.disp_compact[e] : e - N_DISP);
+            }
             base += __popc(bal);
         }
         if (lane == 0) ctl.n_act = base;
@@ -285,25 +291,35 @@ __global__ void __launch_bounds__(THREADS, 1) k_m2l_tf32x3(const __grid_constant
             soff[i] = (uint32_t)((n >> 3) * 1024 + (n & 7) * 128 + ((ch ^ (n & 7)) << 4));
             goff[i] = -1;
         }
+        // The source boxes of the next entry are loaded while the current one streams,
+        // so the table lookups' latency stays off the copy pipeline.
+        int nsrc[8];
+        auto load_sources = [&](int ai) {
+            const int e = ctl.act[ai];
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                const int t = ctl.tgt[((tid >> 3) + 16 * i) / R];
+                nsrc[i] = t >= 0 ? c.src_tab[(int64_t)t * M2L_ENTRIES + e] : -1;
+            }
+        };
+        if (nq > 0) load_sources(0);
         int pending = -1, cur_entry = -1;
         for (int q = 0; q < nq; ++q) {
             const int st = q % STAGES;
             const int ai = q / kch;
-            if (ai != cur_entry) {   // new displacement entry: look up this thread's 8 sources
+            if (ai != cur_entry) {   // new displacement entry: this thread's 8 sources
                 cur_entry = ai;
-                const int e = ctl.act[ai];
 #pragma unroll
                 for (int i = 0; i < 8; ++i) {
                     const int n = (tid >> 3) + 16 * i;
-                    const int t = ctl.tgt[n / R];
-                    int s_ = -1;
-                    if (t >= 0) s_ = c.src_tab[(int64_t)t * M2L_ENTRIES + e];
+                    int s_ = nsrc[i];
                     if (s_ >= c.nb) {
                         atomicOr(c.err, ERRF_BOUNDS);
                         s_ = -1;
                     }
                     goff[i] = s_ >= 0 ? ((int64_t)s_ * R + (n % R)) * c.ld + ch * 4 : -1;
                 }
+                if (ai + 1 < n_act) load_sources(ai + 1);
             }
             if (!mbar_wait(smem_u32(&ctl.empty[st]), ((q / STAGES) & 1) ^ 1, abort_flag)) break;
             const int k0 = (q % kch) * BK;
@@ -403,17 +419,17 @@ __global__ void __launch_bounds__(THREADS, 1) k_m2l_tf32x3(const __grid_constant
                 const int st = q % STAGES;
                 if (!mbar_wait(smem_u32(&ctl.empty[st]), ((q / STAGES) & 1) ^ 1, abort_flag)) break;
                 const int e = ctl.act[q / kch];
+                const int z = ctl.zidx[q / kch];
                 const int k0 = (q % kch) * BK;
                 const uint32_t fb = smem_u32(&ctl.full[st]);
                 const uint32_t sa = smem_u32(sm + st * STAGE_BYTES);
                 mbar_arrive_tx(fb, 2 * TILE_BYTES);
                 if (e < N_DISP) {
-                    const int z = c.disp_compact[e];
                     tma_load_3d(sa, mh, k0, m0, z, fb);
                     tma_load_3d(sa + TILE_BYTES, ml, k0, m0, z, fb);
                 } else {
-                    tma_load_3d(sa, lh, k0, m0, e - N_DISP, fb);
-                    tma_load_3d(sa + TILE_BYTES, ll, k0, m0, e - N_DISP, fb);
+                    tma_load_3d(sa, lh, k0, m0, z, fb);
+                    tma_load_3d(sa + TILE_BYTES, ll, k0, m0, z, fb);
                 }
             }
         }
