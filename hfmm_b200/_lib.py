@@ -68,6 +68,7 @@ SIGNATURES = [
     ("hfmm_batch_create", _c_i32, [ctypes.POINTER(_c_vp), _c_i32, _c_i32, ctypes.POINTER(_c_vp)]),
     ("hfmm_batch_stream_of", _c_i32, [_c_vp, _c_i32]),
     ("hfmm_batch_set_problem", _c_i32, [_c_vp, _c_i32, _c_vp, _c_vp, _c_vp, _c_vp, _c_i32]),
+    ("hfmm_batch_set_check", _c_i32, [_c_vp, _c_i32, _c_vp, _c_vp, _c_i32, _c_vp]),
     ("hfmm_batch_capture", _c_i32, [_c_vp]),
     ("hfmm_batch_launch", _c_i32, [_c_vp, _c_vp]),
     ("hfmm_batch_destroy", None, [_c_vp]),

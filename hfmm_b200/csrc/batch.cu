@@ -13,6 +13,7 @@
 #include "hfmm_internal.cuh"
 
 #include <algorithm>
+#include <memory>
 #include <numeric>
 #include <vector>
 
@@ -27,8 +28,15 @@ struct hfmm_batch {
         double *phi = nullptr, *E = nullptr;
         int precision = 0;
         bool set = false;
+        // optional in-graph check against the FP64 direct sum at sampled targets
+        const double* pos = nullptr;          // n x 3, input order
+        const int32_t* tg = nullptr;
+        int n_t = 0, n_split = 1;
+        double* sums = nullptr;               // 4 doubles, written by every launch
+        hfmm::DevBuf<double> ref, scratch;    // direct-sum values and partial sums
     };
-    std::vector<Io> io;
+    std::vector<std::unique_ptr<Io>> io_;   // one per plan (Io owns device buffers)
+    Io& io(int i) { return *io_[i]; }
     std::vector<cudaStream_t> streams;
     std::vector<cudaEvent_t> events;            // [0] fork, [1 + s] join of stream s
     std::vector<hfmm::DevBuf<double>> ws;       // per stream (streamed plans only)
@@ -61,6 +69,45 @@ struct hfmm_batch {
 namespace hfmm {
 
 namespace {
+
+// Squared-norm sums of the check: sums = (sum |phi - phi_ref|^2, sum |phi_ref|^2,
+// sum |E - E_ref|^2, sum |E_ref|^2) over the sampled targets (E terms 0 without a
+// field). One CTA, fixed-order tree reduction: the sums are deterministic.
+__global__ void __launch_bounds__(256) k_check_sums(const double* __restrict__ phi,
+                                                    const double* __restrict__ E,
+                                                    const int32_t* __restrict__ tg, int n_t,
+                                                    int64_t n, const double* __restrict__ rphi,
+                                                    const double* __restrict__ rE, double* sums,
+                                                    int* err) {
+    __shared__ double red[4][256];
+    double a[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int t = threadIdx.x; t < n_t; t += blockDim.x) {
+        const int64_t i = tg[t];
+        if (i < 0 || i >= n) {
+            atomicOr(err, ERRF_BOUNDS);
+            continue;
+        }
+        for (int c = 0; c < 2; ++c) {
+            const double r = rphi[2 * t + c], d = phi[2 * i + c] - r;
+            a[0] += d * d;
+            a[1] += r * r;
+        }
+        if (E)
+            for (int c = 0; c < 6; ++c) {
+                const double r = rE[6 * t + c], d = E[6 * i + c] - r;
+                a[2] += d * d;
+                a[3] += r * r;
+            }
+    }
+    for (int v = 0; v < 4; ++v) red[v][threadIdx.x] = a[v];
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+        if (threadIdx.x < w)
+            for (int v = 0; v < 4; ++v) red[v][threadIdx.x] += red[v][threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x < 4) sums[threadIdx.x] = red[threadIdx.x][0];
+}
 
 // Work estimate of one evaluate (complex charges): far field M2L+L2L FLOPs and
 // near-field pairs weighted by ~40 flops each; only the relative size matters.
@@ -118,7 +165,7 @@ int hfmm_batch_create(hfmm_plan* const* plans, int32_t n_plans, int32_t n_stream
             B->order[s].push_back(i);
             B->stream_of[i] = s;
         }
-        B->io.assign(n_plans, {});
+        for (int i = 0; i < n_plans; ++i) B->io_.push_back(std::make_unique<hfmm_batch::Io>());
         B->streams.resize(S);
         for (auto& s : B->streams) HFMM_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
         B->events.resize(S + 1);
@@ -165,7 +212,7 @@ int hfmm_batch_set_problem(hfmm_batch* B, int32_t i, const double* q_re_dev, con
     } catch (const Error& e) {
         return fail(e.code, e.msg);
     }
-    auto& io = B->io[i];
+    auto& io = B->io(i);
     io.q_re = q_re_dev;
     io.q_im = q_im_dev;
     io.phi = phi_out_dev;
@@ -176,10 +223,37 @@ int hfmm_batch_set_problem(hfmm_batch* B, int32_t i, const double* q_re_dev, con
     return HFMM_OK;
 }
 
+int hfmm_batch_set_check(hfmm_batch* B, int32_t i, const double* pos_dev,
+                         const int32_t* targets_dev, int32_t n_t, double* sums_dev) {
+    if (!B || i < 0 || i >= (int)B->plans.size()) return fail(HFMM_ERR_ARG, "bad batch or index");
+    if (!B->plans[i]) return fail(HFMM_ERR_STATE, "the plan was destroyed");
+    if (!pos_dev || !targets_dev || !sums_dev || n_t <= 0)
+        return fail(HFMM_ERR_ARG, "positions, targets and sums are required");
+    try {
+        require_device_ptr(pos_dev, "positions");
+        require_device_ptr(targets_dev, "targets");
+        require_device_ptr(sums_dev, "sums");
+        HFMM_CUDA(cudaSetDevice(B->device));
+        auto& io = B->io(i);
+        io.pos = pos_dev;
+        io.tg = targets_dev;
+        io.n_t = n_t;
+        io.sums = sums_dev;
+        io.n_split = direct_splits(B->plans[i]->n, n_t);
+        io.ref.alloc((size_t)8 * n_t);
+        io.ref.zero();
+        io.scratch.alloc((size_t)io.n_split * n_t * 8);
+        B->drop_graph();
+        return HFMM_OK;
+    } catch (const Error& e) {
+        return fail(e.code, e.msg);
+    }
+}
+
 int hfmm_batch_capture(hfmm_batch* B) {
     if (!B) return fail(HFMM_ERR_ARG, "batch is NULL");
-    for (auto& io : B->io)
-        if (!io.set) return fail(HFMM_ERR_STATE, "every problem needs its charges and outputs");
+    for (auto& io : B->io_)
+        if (!io->set) return fail(HFMM_ERR_STATE, "every problem needs its charges and outputs");
     for (auto* P : B->plans) {
         if (!P) return fail(HFMM_ERR_STATE, "a plan of the batch was destroyed");
         if (plan_profiling(P)) return fail(HFMM_ERR_STATE, "turn profiling off before capture");
@@ -196,9 +270,19 @@ int hfmm_batch_capture(hfmm_batch* B) {
             for (int s = 1; s < S; ++s) HFMM_CUDA(cudaStreamWaitEvent(B->streams[s], B->events[0], 0));
             for (int s = 0; s < S; ++s)
                 for (int i : B->order[s]) {
-                    const auto& io = B->io[i];
-                    evaluate_fp64(B->plans[i], io.q_re, io.q_im, io.phi, io.E, B->streams[s],
+                    auto& io = B->io(i);
+                    hfmm_plan* P = B->plans[i];
+                    evaluate_fp64(P, io.q_re, io.q_im, io.phi, io.E, B->streams[s],
                                   io.precision == HFMM_PREC_MIXED);
+                    if (io.sums) {   // check the result against the direct sum, in the graph
+                        double* rphi = io.ref.p;
+                        double* rE = io.ref.p + 2 * io.n_t;
+                        direct_sum(io.pos, io.q_re, io.q_im, P->n, io.tg, io.n_t, P->k, rphi,
+                                   io.E ? rE : nullptr, io.scratch.p, io.n_split, B->streams[s],
+                                   P->d_err.p);
+                        HFMM_LAUNCH(k_check_sums, 1, 256, 0, B->streams[s], io.phi, io.E, io.tg,
+                                    io.n_t, P->n, rphi, rE, io.sums, P->d_err.p);
+                    }
                 }
             for (int s = 1; s < S; ++s) {
                 HFMM_CUDA(cudaEventRecord(B->events[1 + s], B->streams[s]));

@@ -197,6 +197,13 @@ int hfmm_batch_stream_of(const hfmm_batch* batch, int32_t i);
 int hfmm_batch_set_problem(hfmm_batch* batch, int32_t i, const double* q_re_dev,
                            const double* q_im_dev, double* phi_out_dev, double* field_out_dev,
                            int32_t precision);
+/* Optional: check problem i in the graph against the FP64 direct sum (the referee
+ * of test.py:11-18) at n_t target indices. pos_dev: the n x 3 positions (input
+ * order) the plan was built from. After each launch sums_dev[0..3] hold
+ * sum |phi - phi_ref|^2, sum |phi_ref|^2, sum |E - E_ref|^2, sum |E_ref|^2 over the
+ * targets (the E terms are 0 without a field output). */
+int hfmm_batch_set_check(hfmm_batch* batch, int32_t i, const double* pos_dev,
+                         const int32_t* targets_dev, int32_t n_t, double* sums_dev);
 int hfmm_batch_capture(hfmm_batch* batch);
 int hfmm_batch_launch(hfmm_batch* batch, void* stream);
 void hfmm_batch_destroy(hfmm_batch* batch);

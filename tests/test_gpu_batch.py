@@ -162,3 +162,31 @@ def test_auto_batch_certifies_every_problem():
     assert all(r["certified"] for r in rep)
     assert all(r["p"] == 10 for r in rep)
     ab.close()
+
+
+def test_in_graph_check_matches_host_referee():
+    """The direct sum and error sums captured in the graph give the errors the
+    host-side referee gives for the same targets."""
+    import hfmm_b200 as hf
+    from hfmm_b200.batch import Batch
+    probs = _batch_problems()[:3]
+    states = [hf.setup(x, k, p=p, N_max=32, stream_tables=True) for x, k, q, p in probs]
+    qs = [torch.as_tensor(q).cuda() for _, _, q, _ in probs]
+    rng = np.random.default_rng(5)
+    tgs = [torch.as_tensor(np.sort(rng.choice(st.n, 200, replace=False)).astype(np.int32)).cuda()
+           for st in states]
+    b = Batch(states, 2)
+    outs = b.bind(qs, field=True, precision=hf.PREC_MIXED, checks=tgs)
+    b.launch()
+    torch.cuda.synchronize()
+    b.check_errors()
+    got = b.check_rel_errors()
+    for st, q, tg, (phi, E), (e_phi, e_E) in zip(states, qs, tgs, outs, got):
+        r_phi, r_E = hf.direct_at(st, q.real.contiguous(), q.imag.contiguous(), tg, field=True)
+        want_phi = float(torch.linalg.norm(phi[tg.long()] - r_phi) / torch.linalg.norm(r_phi))
+        want_E = float(torch.linalg.norm(E[tg.long()] - r_E) / torch.linalg.norm(r_E))
+        assert e_phi == pytest.approx(want_phi, rel=1e-9) and e_E == pytest.approx(want_E, rel=1e-9)
+        assert 0 < e_phi < 1e-3
+    b.close()
+    for st in states:
+        st.close()
