@@ -72,6 +72,8 @@ def parse():
     ap.add_argument("--no-plain", action="store_true",
                     help="auto mode: skip the plain FP64 comparison run")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
+    ap.add_argument("--m2l-compress", type=float, default=None,
+                    help="plain mode: low-rank M2L tolerance for the mixed evaluate")
     ap.add_argument("--config", choices=sorted(CONFIGS), default="c2")
     ap.add_argument("--n", type=int)
     ap.add_argument("--k", type=float)
@@ -362,7 +364,7 @@ def run_ours(a, cfg, rank, world, local_rank):
     pos, q = make_problem(cfg, rank)
     t0 = time.time()
     st = hfmm_b200.setup(pos, cfg["k"], p=cfg["p"], N_max=cfg["leaf"], max_depth=cfg["max_depth"],
-                         device=dev)
+                         device=dev, m2l_compress=a.m2l_compress)
     torch.cuda.synchronize()
     setup_s = time.time() - t0
     n = cfg["n"]
@@ -454,26 +456,25 @@ def run_ours(a, cfg, rank, world, local_rank):
     out = None
     if rank == 0:
         NF, R = st.n_families, 2
-        flops = dominant_flops(st, R, NF)
-        dom_ms = phase[_lib.PHASES.index("m2l_l2l_gemm")]
-        peak = measured_fp64_peak(torch)
+        dom_ms = float(phase[_lib.PHASES.index("m2l_l2l_gemm")])
+        if a.precision == "fp64":
+            flops = dominant_flops(st, R, NF)
+            peak = measured_fp64_peak(torch)
+            kernel = "k_gemm_f64 (M2L + L2L, all levels)"
+            src = ("cuBLAS DGEMM 4096^3 measured in this run, FP64 (of measured; "
+                   "MEASURED_PEAKS.json has no FP64 figure)")
+        else:
+            flops = 3.0 * m2l_flops(st, R, NF)
+            peak = measured_tf32_peak(torch)
+            kernel = "k_m2l_tf32x3 (M2L, 3xTF32 on tcgen05, all levels)"
+            src = ("cuBLAS FP32 GEMM with TF32 tensor cores, 8192^3, measured in this run "
+                   "(of measured; MEASURED_PEAKS.json has no TF32 figure)")
         achieved = flops / (dom_ms * 1e-3) / 1e12 if dom_ms > 0 else None
-        traffic = None
-        tpath = os.path.join(ROOT, "profiles", "traffic.json")
-        if os.path.exists(tpath):
-            try:
-                tj = json.load(open(tpath))
-                key = f"{a.config}:{a.precision}"
-                if key in tj:
-                    traffic = tj[key]
-            except Exception:
-                traffic = None
         roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                "frac": (achieved / peak) if achieved else None, "traffic": traffic,
-                "kernel": "k_gemm_f64 (M2L + L2L, all levels)",
-                "algorithmic_flops_per_evaluate": flops, "kernel_ms_per_evaluate": float(dom_ms),
-                "peak_source": "cuBLAS DGEMM 4096^3 measured in this run, FP64 (of measured; "
-                               "MEASURED_PEAKS.json has no FP64 figure)"}
+                "frac": (achieved / peak) if achieved else None,
+                "traffic": _traffic(a, a.precision), "kernel": kernel,
+                "algorithmic_flops_per_evaluate": flops, "kernel_ms_per_evaluate": dom_ms,
+                "peak_source": src}
         cpu = None
         if not a.no_cpu and world == 1:
             cores, blas = cpu_threads()

@@ -139,7 +139,7 @@ def _validate_setup(positions, k, p, N_max, max_depth):
 
 
 def setup(positions, k, p=4, N_max=16, max_depth=None, device=None, tables="device",
-          stream_tables=False):
+          stream_tables=False, m2l_compress=None):
     """Build the plan for ``positions`` and wavenumber ``k`` (HFMM.setup, HFMM.py:55-80).
 
     ``p`` is the number of surface points per cube edge, ``N_max`` the leaf
@@ -151,6 +151,8 @@ def setup(positions, k, p=4, N_max=16, max_depth=None, device=None, tables="devi
     ``stream_tables``: keep no M2L table resident; each evaluate regenerates a
     level's 316 M2L matrices on the device right before its M2L (bit-identical
     to the resident "device" tables; memory per plan drops to one level's worth).
+    ``m2l_compress``: a relative tolerance (e.g. 1e-8) to give the mixed-precision
+    evaluate a low-rank M2L (``hfmm_b200.compress``); the FP64 evaluate is unchanged.
     """
     if tables not in ("device", "host"):
         raise ValueError('tables must be "device" or "host"')
@@ -167,6 +169,8 @@ def setup(positions, k, p=4, N_max=16, max_depth=None, device=None, tables="devi
         state = HFMMState(h.value, pos, kf, p, N_max, dev)
         try:
             _load_tables(state, tables, stream_tables)
+            if m2l_compress is not None:
+                _load_compressed(state, float(m2l_compress))
             _check(_lib.lib.hfmm_plan_finalize(state.handle))
         except Exception:
             state.close()
@@ -202,6 +206,22 @@ def _load_tables(state, mode="device", streamed=False):
             ptrs = [None if a is None else a.ctypes.data for a in arrs]
             _check(_lib.lib.hfmm_plan_set_level(state.handle, fam, level, *ptrs))
             del arrs, t
+
+
+def _load_compressed(state, eps):
+    """Low-rank M2L of every level and family (hfmm_plan_set_m2l_compressed)."""
+    from .compress import level_compressed
+    extent = state.info["domain_extent"]
+    state.m2l_ranks = {}
+    with torch.cuda.device(state.device):
+        for fam in range(state.n_families):
+            for level in range(2, state.max_depth + 1):
+                U, C = level_compressed(state.p, level, extent, state.k, fam == 1, eps, state.device)
+                r = U.shape[1]
+                _check(_lib.lib.hfmm_plan_set_m2l_compressed(state.handle, fam, level, r,
+                                                              U.data_ptr(), C.data_ptr()))
+                state.m2l_ranks[(fam, level)] = r
+                del U, C
 
 
 def evaluate_into(state, q_re, q_im, phi_out, field_out=None, precision=PREC_FP64, stream=None):

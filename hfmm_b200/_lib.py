@@ -13,9 +13,10 @@ LIB_PATH = os.path.join(_HERE, "_lib", "libhfmm_b200.so")
 HFMM_OK = 0
 HFMM_PREC_FP64 = 0
 HFMM_PREC_MIXED = 1
-N_PHASES = 14
+N_PHASES = 15
 PHASES = ("gather", "p2m", "m2m_gemm", "up_decode", "m2l_l2l_gemm", "p2l", "down_decode",
-          "p2p", "l2p", "m2p", "combine", "tf32_split", "m2l_tables", "l2l_gemm")
+          "p2p", "l2p", "m2p", "combine", "tf32_split", "m2l_tables", "l2l_gemm",
+          "m2l_compress")
 
 _c_i32, _c_i64, _c_dbl, _c_vp = ctypes.c_int32, ctypes.c_int64, ctypes.c_double, ctypes.c_void_p
 
@@ -65,6 +66,7 @@ SIGNATURES = [
                                      _c_vp, _c_vp]),
     ("hfmm_plan_set_profiling", _c_i32, [_c_vp, _c_i32]),
     ("hfmm_plan_phase_times", _c_i32, [_c_vp, _c_vp]),
+    ("hfmm_plan_set_m2l_compressed", _c_i32, [_c_vp, _c_i32, _c_i32, _c_i32, _c_vp, _c_vp]),
     ("hfmm_batch_create", _c_i32, [ctypes.POINTER(_c_vp), _c_i32, _c_i32, ctypes.POINTER(_c_vp)]),
     ("hfmm_batch_stream_of", _c_i32, [_c_vp, _c_i32]),
     ("hfmm_batch_set_problem", _c_i32, [_c_vp, _c_i32, _c_vp, _c_vp, _c_vp, _c_vp, _c_i32]),

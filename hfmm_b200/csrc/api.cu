@@ -100,9 +100,10 @@ std::vector<int32_t> nonadjacent_map() {
 }
 
 // A-pointer sets of the GEMM calls: kind 0..3 decode (up U, up Vt, dn U, dn Vt),
-// kind 4 M2M (8 entries), kind 5 downward M2L+L2L (351 entries); per level, families adjacent.
-enum { K_UPU, K_UPV, K_DNU, K_DNV, K_M2M, K_DN, K_L2L, K_COUNT };
-const int k_entries[K_COUNT] = {1, 1, 1, 1, 8, M2L_ENTRIES, 8};
+// kind 4 M2M (8 entries), kind 5 downward M2L+L2L (351 entries), kind 6 L2L alone,
+// kinds 7/8 compress / expand of the compressed M2L; per level, families adjacent.
+enum { K_UPU, K_UPV, K_DNU, K_DNV, K_M2M, K_DN, K_L2L, K_CMP, K_EXP, K_COUNT };
+const int k_entries[K_COUNT] = {1, 1, 1, 1, 8, M2L_ENTRIES, 8, 1, 1};
 
 struct PtrIndex {
     size_t off[K_COUNT][MAX_LEVELS];
@@ -139,6 +140,8 @@ void build_a_ptrs(hfmm_plan* P, PtrIndex& ix) {
                     case K_L2L:
                         for (int o = 0; o < 8; ++o) h.push_back(T.l2l.p ? T.l2l.p + o * mat : nullptr);
                         break;
+                    case K_CMP: h.push_back(T.c_cmp.p); break;
+                    case K_EXP: h.push_back(T.c_exp.p); break;
                 }
             }
         }
@@ -362,17 +365,86 @@ void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double*
         decode(l, true, P->check.p, P->equiv.p);
     }
     const bool use_mx = mixed && P->mixed_ready;
-    if (use_mx) {   // TF32 hi/lo halves of every equivalent density (B operand of the M2L)
+    const bool use_cx = use_mx && P->compressed;
+    // A level's compressed buffers hold [box - level_lo][R][cld]; the GEMMs index boxes
+    // absolutely, so they get the buffer's address shifted back by level_lo rows.
+    auto level_base = [&](auto* buf, int l, int cld) {
+        return buf - (int64_t)P->level_lo[l] * R * cld;
+    };
+    // one-entry GEMM over every box of level l between layouts of different widths
+    auto gemm_1 = [&](int kind, int l, int f, const double* in, int ldk, double* out, int ldm) {
+        GemmCall c{};
+        c.tile_tgt = P->dec_tiles[l][R - 1].tgt.p;
+        c.ntiles = P->dec_tiles[l][R - 1].ntiles;
+        c.src_tab = nullptr;
+        c.n_entries = 1;
+        c.b_split = 1;
+        c.A = P->a_ptrs.p + X->ix.off[kind][l] + f;
+        c.B0 = in;
+        c.out = out;
+        c.accumulate = 0;
+        c.R = R;
+        c.ld = P->ld;
+        c.ldk = ldk;
+        c.ldm = ldm;
+        c.n_s = P->n_s;
+        c.n_fam = 1;
+        c.nb = P->nb;
+        gemm_f64(c, P->d_err.p, s);
+    };
+    if (use_cx) {   // compress every level's densities (x' = U^T x), then split them
+        PhaseTimer pt(X, s, 14);
+        for (int l = 2; l <= P->md; ++l)
+            for (int f = 0; f < NF; ++f) {
+                LevelTables& T = P->tables[f][l];
+                gemm_1(K_CMP, l, f, P->equiv.p + f * fs, P->ld, level_base(T.xc.p, l, T.cld), T.cld);
+                const int64_t cnt = (int64_t)(P->level_hi[l] - P->level_lo[l]) * R * T.cld;
+                split_tf32(T.xc.p, T.xc_hi.p, T.xc_lo.p, cnt, s);
+            }
+    } else if (use_mx) {   // TF32 hi/lo halves of every equivalent density (B operand of the M2L)
         PhaseTimer pt(X, s, 11);
         split_tf32(P->equiv.p, P->e_hi.p, P->e_lo.p, (int64_t)NF * fs, s);
     }
     // ---- downward pass (M2L + L2L in one GEMM, then X-list P2L, then decode)
     for (int l = 2; l <= P->md; ++l) {
-        if (P->streamed) {
+        if (P->streamed && !use_cx) {
             PhaseTimer pt(X, s, 12);
             generate_m2l_stream(P, l, use_mx, P->ws, s);
         }
-        if (use_mx) {
+        if (use_cx) {
+            for (int f = 0; f < NF; ++f) {
+                LevelTables& T = P->tables[f][l];
+                MixedCall mc{};
+                mc.tile_tgt = P->mx_tiles[l][R - 1].tgt.p;
+                mc.ntiles = P->mx_tiles[l][R - 1].ntiles;
+                mc.src_tab = P->m2l_src.p;
+                mc.disp_compact = P->disp_compact.p;
+                mc.Bhi = level_base(T.xc_hi.p, l, T.cld);
+                mc.Blo = level_base(T.xc_lo.p, l, T.cld);
+                mc.Lhi = nullptr;
+                mc.Llo = nullptr;
+                mc.out = level_base(T.yc.p, l, T.cld);
+                mc.src_lo = P->level_lo[l];   // the level's buffers hold its own boxes only
+                mc.src_hi = P->level_hi[l];
+                mc.R = R;
+                mc.ld = T.cld;
+                mc.n_fam = 1;
+                mc.has_l2l = 0;
+                mc.fam_stride = 0;
+                mc.out_fam_stride = 0;
+                mc.nb = P->nb;
+                mc.err = P->d_err.p;
+                {
+                    PhaseTimer pt(X, s, 4);
+                    m2l_tf32x3(static_cast<MixedMaps*>(P->cx_maps)[f * MAX_LEVELS + l], mc, s);
+                }
+                PhaseTimer pt(X, s, 14);   // expand y = U y' into the check potential
+                gemm_1(K_EXP, l, f, level_base(T.yc.p, l, T.cld), T.cld, P->check.p + f * fs, P->ld);
+            }
+            if (l >= 3)   // L2L (phases.py:273-278) in FP64, added to the check potential
+                gemm(K_L2L, l, P->dn_tiles[l][R - 1], P->m2l_src.p + N_DISP, M2L_ENTRIES, P->loc.p,
+                     nullptr, P->check.p, nullptr);
+        } else if (use_mx) {
             MixedCall mc{};
             mc.tile_tgt = P->mx_tiles[l][R - 1].tgt.p;
             mc.ntiles = P->mx_tiles[l][R - 1].ntiles;
@@ -672,8 +744,10 @@ int hfmm_plan_finalize(hfmm_plan* P) {
     P->equiv.zero();
     P->loc.zero();
     P->tmp.zero();
-    // mixed path: TF32 hi/lo tables, tensor maps, split density buffers (needs ld >= 128)
+    // mixed path: TF32 hi/lo tables, tensor maps, split density buffers (needs ld >= 128);
+    // with a compressed M2L on every level the dense TF32 tables are not needed
     P->mixed_ready = false;
+    compressed_prepare(P);
     if (P->ld >= 128) {
         std::vector<int32_t> dc(N_DISP, -1);
         auto madj = nonadjacent_map();
@@ -684,7 +758,9 @@ int hfmm_plan_finalize(hfmm_plan* P) {
         if (!P->mx_maps) P->mx_maps = new MixedMaps[MAX_LEVELS];
         MixedMaps* maps = static_cast<MixedMaps*>(P->mx_maps);
         std::memset(maps, 0, sizeof(MixedMaps) * MAX_LEVELS);
-        if (P->streamed) {
+        if (P->compressed) {
+            // the mixed M2L runs on the compressed tables (compress.cu)
+        } else if (P->streamed) {
             if (P->ws) stream_maps(P);
         } else {
             for (int f = 0; f < P->n_fam; ++f)
@@ -804,6 +880,8 @@ void hfmm_plan_destroy(hfmm_plan* P) {
     drop_extra(P);
     delete[] static_cast<MixedMaps*>(P->mx_maps);
     P->mx_maps = nullptr;
+    delete[] static_cast<MixedMaps*>(P->cx_maps);
+    P->cx_maps = nullptr;
     delete P;
 }
 

@@ -1,0 +1,124 @@
+// Compressed M2L of the mixed path: the 316 M2L matrices of a level share their
+// dominant subspace U (n_s x r), so K_d ~ U C_d U^T with C_d = U^T K_d U (r x r).
+// The M2L of a level then runs as: compress the densities (x' = U^T x, FP64
+// GEMM), apply the C_d per V pair on the tensor cores (3xTF32, the kernel of
+// m2l_tf32x3.cu with ld = the padded rank), expand (y = U y', FP64 GEMM) into
+// the check potential. No counterpart in the reference, which applies every
+// K_d densely (jaxfmm/kifmm/phases.py:176-237); U and C_d come from the host
+// library (hfmm_b200/compress.py: leading eigenvectors of sum_d K_d K_d^T).
+// This file packs them into the layouts the GEMMs read and prepares the buffers.
+#include "hfmm_internal.cuh"
+#include "mixed.cuh"
+
+#include <cstring>
+
+namespace hfmm {
+
+namespace {
+
+constexpr int N_M2L = 316;
+
+// compress table, A^T of U^T: out[k][m] = U[k][m] (k < n_s rows of U, m < r), ld x cld
+__global__ void k_pack_cmp(const double* __restrict__ U, int n_s, int r, int ld, int cld,
+                           double* out) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    const int k = blockIdx.y;
+    if (m >= cld || k >= ld) return;
+    out[(int64_t)k * cld + m] = (k < n_s && m < r) ? U[(int64_t)k * r + m] : 0.0;
+}
+
+// expand table, A^T of U: out[k][m] = U[m][k] (k < r, m < n_s), cld x ld
+__global__ void k_pack_exp(const double* __restrict__ U, int n_s, int r, int ld, int cld,
+                           double* out) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    const int k = blockIdx.y;
+    if (m >= ld || k >= cld) return;
+    out[(int64_t)k * ld + m] = (k < r && m < n_s) ? U[(int64_t)m * r + k] : 0.0;
+}
+
+__device__ __forceinline__ float tf32_round(float x) {
+    return __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xFFFFE000u);
+}
+
+// C_d as TF32 hi/lo halves in the A layout [d][m][k] of the tcgen05 kernel (cld x cld)
+__global__ void k_pack_c(const double* __restrict__ C, int r, int cld, float* hi, float* lo) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int m = blockIdx.y;
+    const int d = blockIdx.z;
+    if (k >= cld || m >= cld) return;
+    const double v = (m < r && k < r) ? C[((int64_t)d * r + m) * r + k] : 0.0;
+    const float h = tf32_round((float)v);
+    const int64_t o = ((int64_t)d * cld + m) * cld + k;
+    hi[o] = h;
+    lo[o] = tf32_round((float)(v - (double)h));
+}
+
+}  // namespace
+
+void compressed_prepare(hfmm_plan* P) {
+    P->compressed = false;
+    if (P->ld < 128) return;
+    for (int f = 0; f < P->n_fam; ++f)
+        for (int l = 2; l <= P->md; ++l)
+            if (!P->tables[f][l].cr) return;
+    if (!P->cx_maps) P->cx_maps = new MixedMaps[2 * MAX_LEVELS];
+    MixedMaps* maps = static_cast<MixedMaps*>(P->cx_maps);
+    std::memset(maps, 0, sizeof(MixedMaps) * 2 * MAX_LEVELS);
+    for (int f = 0; f < P->n_fam; ++f)
+        for (int l = 2; l <= P->md; ++l) {
+            LevelTables& T = P->tables[f][l];
+            const size_t rows = (size_t)(P->level_hi[l] - P->level_lo[l]) * 2;   // R <= 2
+            T.xc.alloc(rows * T.cld);
+            T.yc.alloc(rows * T.cld);
+            T.xc_hi.alloc(rows * T.cld);
+            T.xc_lo.alloc(rows * T.cld);
+            T.xc.zero();
+            T.yc.zero();
+            T.xc_hi.zero();
+            T.xc_lo.zero();
+            make_table_map(&maps[f * MAX_LEVELS + l].a_hi[0], T.c_hi.p, T.cld, N_M2L);
+            make_table_map(&maps[f * MAX_LEVELS + l].a_lo[0], T.c_lo.p, T.cld, N_M2L);
+        }
+    P->compressed = true;
+}
+
+}  // namespace hfmm
+
+using namespace hfmm;
+
+extern "C" {
+
+int hfmm_plan_set_m2l_compressed(hfmm_plan* P, int32_t family, int32_t level, int32_t rank,
+                                 const double* U_dev, const double* C_dev) {
+    if (!P) return fail(HFMM_ERR_ARG, "plan is NULL");
+    if (P->n_s == 0) return fail(HFMM_ERR_STATE, "set the kernel first");
+    if (family < 0 || family >= P->n_fam) return fail(HFMM_ERR_ARG, "family out of range");
+    if (level < 2 || level > P->md) return fail(HFMM_ERR_ARG, "level must be in [2, max_depth]");
+    if (rank < 1 || rank > P->n_s) return fail(HFMM_ERR_ARG, "rank must be in [1, n_s]");
+    if (!U_dev || !C_dev) return fail(HFMM_ERR_ARG, "U and C are required");
+    try {
+        require_device_ptr(U_dev, "U");
+        require_device_ptr(C_dev, "C");
+        LevelTables& T = P->tables[family][level];
+        const int cld = std::max(128, (int)round_up(rank, 32));
+        T.cr = rank;
+        T.cld = cld;
+        T.c_cmp.alloc((size_t)P->ld * cld);
+        T.c_exp.alloc((size_t)cld * P->ld);
+        T.c_hi.alloc((size_t)N_M2L * cld * cld);
+        T.c_lo.alloc((size_t)N_M2L * cld * cld);
+        HFMM_LAUNCH(k_pack_cmp, dim3((unsigned)ceil_div(cld, 128), (unsigned)P->ld), 128, 0, 0, U_dev,
+                    P->n_s, rank, P->ld, cld, T.c_cmp.p);
+        HFMM_LAUNCH(k_pack_exp, dim3((unsigned)ceil_div(P->ld, 128), (unsigned)cld), 128, 0, 0, U_dev,
+                    P->n_s, rank, P->ld, cld, T.c_exp.p);
+        HFMM_LAUNCH(k_pack_c, dim3((unsigned)ceil_div(cld, 128), (unsigned)cld, N_M2L), 128, 0, 0,
+                    C_dev, rank, cld, T.c_hi.p, T.c_lo.p);
+        HFMM_CUDA(cudaDeviceSynchronize());
+        P->finalized = false;
+        return HFMM_OK;
+    } catch (const Error& e) {
+        return fail(e.code, e.msg);
+    }
+}
+
+}  // extern "C"

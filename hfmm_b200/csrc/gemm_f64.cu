@@ -102,7 +102,7 @@ __global__ void __launch_bounds__(128) k_gemm_f64(GemmCall c, int* err) {
     }
     __syncthreads();
     const int n_act = sm.n_act;
-    const int kch = c.ld / KC;
+    const int kch = c.ldk / KC;
     const int nq = n_act * kch;
 
     auto load = [&](int q, int buf) {
@@ -114,8 +114,8 @@ __global__ void __launch_bounds__(128) k_gemm_f64(GemmCall c, int* err) {
         for (int i = 0; i < 4; ++i) {   // A: 16 rows x 64 doubles = 512 x 16 B
             int ch = tid + 128 * i;
             int row = ch >> 5, col = (ch & 31) * 2;
-            bool ok = (m0 + col) < c.ld;
-            const double* g = ok ? Ae + (int64_t)(k0 + row) * c.ld + m0 + col : Ae;
+            bool ok = (m0 + col) < c.ldm;
+            const double* g = ok ? Ae + (int64_t)(k0 + row) * c.ldm + m0 + col : Ae;
             cp_async16(&sm.u.ld.A[buf][row][col], g, ok);
         }
 #pragma unroll
@@ -128,7 +128,7 @@ __global__ void __launch_bounds__(128) k_gemm_f64(GemmCall c, int* err) {
             if (t >= 0) s = c.src_tab ? c.src_tab[(int64_t)t * c.src_ld + e] : t;
             bool ok = s >= 0 && s < c.nb;
             if (s >= c.nb) atomicOr(err, ERRF_BOUNDS);
-            const double* g = ok ? Bsel + ((int64_t)s * R + r) * c.ld + k0 + part : B0;
+            const double* g = ok ? Bsel + ((int64_t)s * R + r) * c.ldk + k0 + part : B0;
             cp_async16(&sm.u.ld.B[buf][col][part], g, ok);
         }
     };
@@ -191,13 +191,13 @@ __global__ void __launch_bounds__(128) k_gemm_f64(GemmCall c, int* err) {
         int j = col / R, r = col % R;
         int t = sm.tgt[j];
         int m = m0 + mm;
-        if (t < 0 || m >= c.ld) continue;
+        if (t < 0 || m >= c.ldm) continue;
         double v0 = sm.u.C[col][mm], v1 = sm.u.C[col][mm + 1];
         if (c.scale) {
             v0 *= c.scale[m];
             v1 *= c.scale[m + 1];
         }
-        double2* o = reinterpret_cast<double2*>(out + ((int64_t)t * R + r) * c.ld + m);
+        double2* o = reinterpret_cast<double2*>(out + ((int64_t)t * R + r) * c.ldm + m);
         if (c.accumulate) {
             double2 old = *o;
             v0 += old.x;
@@ -209,11 +209,15 @@ __global__ void __launch_bounds__(128) k_gemm_f64(GemmCall c, int* err) {
 
 }  // namespace
 
-void gemm_f64(const GemmCall& c, int* d_err, cudaStream_t s) {
-    if (c.ntiles == 0) return;
-    if (c.ld % KC != 0) throw Error{HFMM_ERR_STATE, "gemm_f64: ld must be a multiple of 16"};
+void gemm_f64(const GemmCall& call, int* d_err, cudaStream_t s) {
+    if (call.ntiles == 0) return;
+    GemmCall c = call;
+    if (!c.ldk) c.ldk = c.ld;
+    if (!c.ldm) c.ldm = c.ld;
+    if (c.ldk % KC != 0 || c.ldm % KC != 0)
+        throw Error{HFMM_ERR_STATE, "gemm_f64: ld must be a multiple of 16"};
     if (c.n_entries > MAX_ENTRIES) throw Error{HFMM_ERR_STATE, "gemm_f64: too many entries"};
-    dim3 grid(c.ntiles, (c.ld + TM - 1) / TM, c.n_fam);
+    dim3 grid(c.ntiles, (c.ldm + TM - 1) / TM, c.n_fam);
     if (c.R == 1) HFMM_LAUNCH(k_gemm_f64<1>, grid, 128, 0, s, c, d_err);
     else if (c.R == 2) HFMM_LAUNCH(k_gemm_f64<2>, grid, 128, 0, s, c, d_err);
     else throw Error{HFMM_ERR_ARG, "gemm_f64: R must be 1 or 2"};

@@ -85,12 +85,21 @@ struct LevelTables {
     DevBuf<double> m2l;                 // 316 x (A^T), non-adjacent displacements
     // mixed path: TF32 hi/lo halves of M2L and L2L as A[m][k] (fp32 containers)
     DevBuf<float> m2l_hi, m2l_lo, l2l_hi, l2l_lo;
+    // compressed M2L of the mixed path, K_d ~ U C_d U^T (rank cr, padded to cld)
+    int cr = 0, cld = 0;
+    DevBuf<double> c_cmp, c_exp;   // A^T of U^T (ld -> cld) and of U (cld -> ld)
+    DevBuf<float> c_hi, c_lo;      // C_d halves as A [316][m][k], cld x cld
+    DevBuf<double> xc, yc;         // the level's compressed densities / check potentials
+    DevBuf<float> xc_hi, xc_lo;    // [box of the level][R][cld]
     bool set = false;
     void reset() {
         up_U.release(); up_d.release(); up_Vt.release();
         dn_U.release(); dn_d.release(); dn_Vt.release();
         m2m.release(); l2l.release(); m2l.release();
         m2l_hi.release(); m2l_lo.release(); l2l_hi.release(); l2l_lo.release();
+        cr = cld = 0;
+        c_cmp.release(); c_exp.release(); c_hi.release(); c_lo.release();
+        xc.release(); yc.release(); xc_hi.release(); xc_lo.release();
         set = false;
     }
 };
@@ -159,6 +168,8 @@ struct hfmm_plan {
     hfmm::DevBuf<int32_t> disp_compact;     // 343 -> M2L table index or -1
     hfmm::DevBuf<float> e_hi, e_lo, l_hi, l_lo;   // split densities [fam][box][R][ld]
     void* mx_maps = nullptr;                // MixedMaps per level (host array)
+    bool compressed = false;                // every level has a compressed M2L (mixed path)
+    void* cx_maps = nullptr;                // MixedMaps [2][MAX_LEVELS] of the C_d tables
     bool mixed_ready = false;
     // streamed M2L tables: regenerated per level and evaluate into a workspace
     // (the plan's own, or one bound by the caller and shared by plans that run in turn)
@@ -192,6 +203,7 @@ size_t stream_ws_bytes(const hfmm_plan* P);
 bool plan_profiling(hfmm_plan* P);
 void batch_forget_plan(struct hfmm_batch* B, hfmm_plan* P);
 void generate_m2l_stream(hfmm_plan* P, int level, bool mixed, void* ws, cudaStream_t s);
+void compressed_prepare(hfmm_plan* P);   // finalize: buffers and tensor maps
 void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double* phi,
                    double* fld, cudaStream_t s, bool mixed = false);
 void direct_sum(const double* pos, const double* q_re, const double* q_im, int64_t n,
@@ -216,6 +228,8 @@ struct GemmCall {
     int accumulate;            // 1: out += result, 0: out = result
     int R;
     int ld;                    // padded n_s (multiple of 16)
+    int ldk, ldm;              // rectangular calls: K extent / B row length and M extent /
+                               // out row length (0: both ld); A^T is ldk x ldm
     int n_s;
     int64_t fam_stride;        // elements between the families' B/out arrays
     int64_t a_fam_stride;      // entries between the families' A pointer sets

@@ -216,9 +216,10 @@ __global__ void __launch_bounds__(THREADS, 1) k_m2l_tf32x3(const __grid_constant
     const int tile = blockIdx.x, m0 = blockIdx.y * BM, fam = blockIdx.z;
     volatile int* abort_flag = &ctl.abort_flag;
 
-    if (tid < TT) {
+    if (tid < TT) {   // targets share the sources' box range (a level's own buffers)
         int t = c.tile_tgt[(int64_t)tile * TT + tid];
-        if (t >= c.nb) {
+        const int64_t lo = c.src_hi > 0 ? c.src_lo : 0, hi = c.src_hi > 0 ? c.src_hi : c.nb;
+        if (t >= 0 && (t < lo || t >= hi)) {
             atomicOr(c.err, ERRF_BOUNDS);
             t = -1;
         }
@@ -302,6 +303,8 @@ __global__ void __launch_bounds__(THREADS, 1) k_m2l_tf32x3(const __grid_constant
                 nsrc[i] = t >= 0 ? c.src_tab[(int64_t)t * M2L_ENTRIES + e] : -1;
             }
         };
+        const int64_t src_lo = c.src_hi > 0 ? c.src_lo : 0;
+        const int64_t src_hi = c.src_hi > 0 ? c.src_hi : c.nb;
         if (nq > 0) load_sources(0);
         int pending = -1, cur_entry = -1;
         for (int q = 0; q < nq; ++q) {
@@ -313,7 +316,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_m2l_tf32x3(const __grid_constant
                 for (int i = 0; i < 8; ++i) {
                     const int n = (tid >> 3) + 16 * i;
                     int s_ = nsrc[i];
-                    if (s_ >= c.nb) {
+                    if (s_ >= 0 && (s_ < src_lo || s_ >= src_hi)) {
                         atomicOr(c.err, ERRF_BOUNDS);
                         s_ = -1;
                     }

@@ -24,6 +24,7 @@ struct MixedCall {
     double* out;                   // check potentials [fam][box][R][ld], FP64
     int R, ld, n_fam, has_l2l;
     int64_t fam_stride, out_fam_stride, nb;
+    int64_t src_lo, src_hi;        // valid source boxes [src_lo, src_hi) (0, nb when unset)
     int* err;
 };
 

@@ -171,11 +171,21 @@ int hfmm_direct_noalloc(const double* pos_dev, const double* q_re_dev, const dou
  * 4 M2L (with L2L fused on the FP64 path), 5 X-list P2L, 6 downward decode,
  * 7 P2P, 8 L2P, 9 W-list M2P, 10 combine, 11 TF32 splits of the mixed path,
  * 12 M2L table generation of a streaming plan, 13 the FP64 L2L GEMM of the mixed
- * path. (Replaces the reference's wall-clock phase prints; it has no per-phase
- * timers, util.py:692-724.) */
-#define HFMM_N_PHASES 14
+ * path, 14 compress / expand GEMMs of a compressed M2L. (Replaces the reference's
+ * wall-clock phase prints; it has no per-phase timers, util.py:692-724.) */
+#define HFMM_N_PHASES 15
 int hfmm_plan_set_profiling(hfmm_plan* plan, int32_t enable);
 int hfmm_plan_phase_times(hfmm_plan* plan, double* ms_out);
+
+/* Compressed M2L for the mixed path (no counterpart in the reference, which
+ * applies each of a level's 316 M2L matrices densely, kifmm/phases.py:176-237):
+ * with U (n_s x rank, row-major float64, device) spanning the level's dominant
+ * M2L subspace and C (316 x rank x rank, row-major float64, device) with
+ * C_d = U^T K_d U, the mixed evaluate computes M2L as U (sum_d C_d (U^T x_d)).
+ * Give every level 2..max_depth of every family before hfmm_plan_finalize; the
+ * FP64 evaluate keeps the dense tables (hfmm_b200/compress.py builds U and C). */
+int hfmm_plan_set_m2l_compressed(hfmm_plan* plan, int32_t family, int32_t level, int32_t rank,
+                                 const double* U_dev, const double* C_dev);
 
 /* ---- batches (no counterpart in the reference: one problem per call there) ---- */
 /* Many finalized plans (problems of uneven size and wavenumber) evaluated by one
