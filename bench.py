@@ -334,9 +334,17 @@ def measured_tf32_peak(torch):
 
 def m2l_flops(state, R, NF):
     """Algorithmic FLOPs of M2L alone per evaluate: one n_s x n_s product per V pair,
-    per charge column and kernel family."""
+    per charge column and kernel family -- or, for a plan with the low-rank M2L,
+    one r x r product with the rank r of the pair's level and family."""
     n_s = state.info["n_s"]
-    return 2.0 * n_s * n_s * R * NF * state.info["n_v"]
+    ranks = getattr(state, "m2l_ranks", None)
+    if not ranks:
+        return 2.0 * n_s * n_s * R * NF * state.info["n_v"]
+    lv = state.tree()["lvls"]
+    V = state.pairs("V")
+    per_level = np.bincount(lv[V[:, 0]], minlength=state.max_depth + 1)
+    return float(sum(2.0 * ranks[(f, l)] ** 2 * R * per_level[l]
+                     for f in range(NF) for l in range(2, state.max_depth + 1)))
 
 
 def dominant_flops(state, R, NF):
@@ -634,9 +642,13 @@ def run_auto(a, cfg, rank, world, local_rank):
         achieved = flops / (dom_ms * 1e-3) / 1e12 if dom_ms > 0 else None
         roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                 "frac": (achieved / peak) if achieved else None, "traffic": _traffic(a, "auto"),
-                "kernel": "k_m2l_tf32x3 (M2L, 3xTF32 on tcgen05, all levels)",
+                "kernel": ("k_m2l_tf32x3 (M2L, 3xTF32 on tcgen05, all levels"
+                           + (", on the low-rank C_d tables)" if ap.m2l_compress else ")")),
                 "algorithmic_flops_per_evaluate": flops, "kernel_ms_per_evaluate": dom_ms,
-                "flop_count": "3 TF32 products x 2 n_s^2 per V pair, charge column and family",
+                "flop_count": ("3 TF32 products x 2 r^2 per V pair, charge column and family, "
+                               "r = the rank of the pair's level and family (unpadded)"
+                               if ap.m2l_compress else
+                               "3 TF32 products x 2 n_s^2 per V pair, charge column and family"),
                 "peak_source": "cuBLAS FP32 GEMM with TF32 tensor cores, 8192^3, measured in "
                                "this run (of measured; MEASURED_PEAKS.json has no TF32 figure)"}
         cpu = None
@@ -660,6 +672,9 @@ def run_auto(a, cfg, rank, world, local_rank):
                        "n_points": n, "k": cfg["k"], "tol": a.tol, "p": last["p"],
                        "leaf": last["leaf"], "n_s": st.info["n_s"], "max_depth": st.max_depth,
                        "precision": "mixed" if last["precision"] == 1 else "fp64",
+                       "m2l_compress": ap.m2l_compress,
+                       "m2l_ranks": {f"{'cos' if f == 0 else 'sin'}{l}": r for (f, l), r in
+                                     sorted(getattr(st, "m2l_ranks", {}).items())},
                        "parallelism": f"replicas x{world}",
                        "l2": "inputs larger than L2 (operator tables and expansions of "
                              f"{st.info['n_boxes']} boxes)"},

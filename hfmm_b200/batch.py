@@ -176,15 +176,16 @@ class AutoBatch:
     """Certified batched evaluate of problems [(positions, k), ...] at one tolerance.
 
     ``net``: an OrderNet, None for the bundled weights, or False for the
-    conservative order (the ablation). Every problem's plan streams its M2L
-    tables, so the batch's table memory is one workspace per stream.
+    conservative order (the ablation). Every problem's plan streams its dense M2L
+    tables (only an FP64 evaluate would read them) and keeps the low-rank M2L of
+    the mixed path, so the batch holds no dense M2L table at all.
     """
 
     def __init__(self, problems, tol=1e-6, net=None, n_streams=None, n_check=256, seed=0,
                  device=None, margin=0.5, wisdom=None):
         from . import setup, _device
         from .learned import (OrderNet, features_for, conservative_p, precision_for,
-                              FEATURE_LEAF, TOL_LEARNED)
+                              compress_for, FEATURE_LEAF, TOL_LEARNED)
         self.tol = float(tol)
         self.device = _device(device)
         self.problems = problems
@@ -197,8 +198,9 @@ class AutoBatch:
             choice = [net.choose_from(y, margin) for y in Y]
         self.choice = choice
         self.precisions = [precision_for(self.tol, p) for p, _ in choice]
-        self.states = [setup(x, k, p=p, N_max=leaf, device=self.device, stream_tables=True)
-                       for (x, k), (p, leaf) in zip(problems, choice)]
+        self.states = [setup(x, k, p=p, N_max=leaf, device=self.device, stream_tables=True,
+                             m2l_compress=compress_for(self.tol, prec))
+                       for (x, k), (p, leaf), prec in zip(problems, choice, self.precisions)]
         rng = np.random.default_rng(seed)
         self.checks = [torch.as_tensor(np.sort(rng.choice(st.n, min(n_check, st.n), replace=False))
                                        .astype(np.int32)).to(self.device) for st in self.states]
