@@ -2,7 +2,8 @@
 
 The data are made by the FMM itself (no counterpart in the reference, which
 takes p from the caller): for each synthetic problem the library's evaluate is
-run at every order of a p sweep, in FP64 and in mixed precision, and its
+run at every order of a p sweep, in FP64 and in mixed precision (with the
+low-rank M2L the front doors use, ``learned.compress_for``), and its
 relative L2 error against the FP64 direct sum on 256 sampled targets (the
 referee of test.py:11-18) is recorded, together with the evaluate time at each
 leaf size. Labels for any tolerance are then read off the error curves
@@ -108,8 +109,10 @@ def generate(n_problems, seed=0, n_check=256, verbose=True):
             tg_d = torch.as_tensor(tg).to(dev)
             e64, emx, t64, tmx = [], [], [], []
             ref = None
+            cmp = learned.compress_for(1e-6, hf.PREC_MIXED)
             for p in P_SWEEP:
-                st = hf.setup(x, k, p=p, N_max=learned.FEATURE_LEAF, device=dev)
+                st = hf.setup(x, k, p=p, N_max=learned.FEATURE_LEAF, device=dev,
+                              m2l_compress=cmp if p >= 5 else None)
                 if ref is None:
                     r_phi, r_E = hf.direct_at(st, q_re, q_im, tg_d, field=True)
                     ref = (r_phi.cpu().numpy(), r_E.cpu().numpy())
@@ -129,7 +132,7 @@ def generate(n_problems, seed=0, n_check=256, verbose=True):
             lp = int(min(learned.P_MAX, max(5, math.ceil(label_p(P_SWEEP, emx, TOL_MIXED)))))
             lt = []
             for leaf in LEAVES:
-                st = hf.setup(x, k, p=lp, N_max=leaf, device=dev)
+                st = hf.setup(x, k, p=lp, N_max=leaf, device=dev, m2l_compress=cmp)
                 phi = torch.empty(st.n, dtype=torch.complex128, device=dev)
                 E = torch.empty((st.n, 3), dtype=torch.complex128, device=dev)
                 lt.append(_time_eval(hf, st, q_re, q_im, phi, E, hf.PREC_MIXED, reps=2, warmup=1))
