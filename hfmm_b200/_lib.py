@@ -62,6 +62,9 @@ SIGNATURES = [
     ("hfmm_export_list", _c_i32, [_c_vp, _c_i32, _c_vp, _c_i64]),
     ("hfmm_direct", _c_i32, [_c_vp, _c_vp, _c_vp, _c_i64, _c_vp, _c_i64, _c_dbl, _c_vp, _c_vp,
                              _c_vp]),
+    ("hfmm_direct_scratch_bytes", _c_i64, [_c_i64, _c_i64]),
+    ("hfmm_direct_async", _c_i32, [_c_vp, _c_vp, _c_vp, _c_i64, _c_vp, _c_i64, _c_dbl, _c_vp, _c_vp,
+                                   _c_vp, _c_i64, _c_vp, _c_vp]),
     ("hfmm_direct_noalloc", _c_i32, [_c_vp, _c_vp, _c_vp, _c_i64, _c_vp, _c_i64, _c_dbl, _c_vp,
                                      _c_vp, _c_vp]),
     ("hfmm_plan_set_profiling", _c_i32, [_c_vp, _c_i32]),

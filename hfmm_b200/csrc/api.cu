@@ -937,6 +937,35 @@ int hfmm_export_list(const hfmm_plan* P, int32_t which, int32_t* pairs, int64_t 
     API_END
 }
 
+int64_t hfmm_direct_scratch_bytes(int64_t n, int64_t n_t) {
+    if (n <= 0 || n_t < 0) return fail(HFMM_ERR_ARG, "invalid direct-sum sizes");
+    return (int64_t)direct_splits(n, n_t) * std::max<int64_t>(n_t, 1) * 8 * (int64_t)sizeof(double);
+}
+
+int hfmm_direct_async(const double* pos, const double* q_re, const double* q_im, int64_t n,
+                      const int32_t* targets, int64_t n_t, double k, double* phi, double* fld,
+                      double* scratch, int64_t scratch_bytes, int* err_dev, void* stream) {
+    if (!pos || !q_re || !targets || !phi || !scratch || !err_dev || n <= 0 || n_t < 0)
+        return fail(HFMM_ERR_ARG, "invalid direct-sum arguments");
+    if (!std::isfinite(k)) return fail(HFMM_ERR_ARG, "k must be finite");
+    const int splits = direct_splits(n, n_t);
+    if (scratch_bytes < (int64_t)splits * std::max<int64_t>(n_t, 1) * 8 * (int64_t)sizeof(double))
+        return fail(HFMM_ERR_CAPACITY, "direct-sum scratch too small (hfmm_direct_scratch_bytes)");
+    API_BEGIN
+    require_device_ptr(pos, "positions");
+    require_device_ptr(q_re, "q_re");
+    if (q_im) require_device_ptr(q_im, "q_im");
+    require_device_ptr(targets, "targets");
+    require_device_ptr(phi, "phi_out");
+    if (fld) require_device_ptr(fld, "field_out");
+    require_device_ptr(scratch, "scratch");
+    require_device_ptr(err_dev, "err");
+    direct_sum(pos, q_re, q_im, n, targets, n_t, k, phi, fld, scratch, splits,
+               (cudaStream_t)stream, err_dev);
+    return HFMM_OK;
+    API_END
+}
+
 int hfmm_direct(const double* pos, const double* q_re, const double* q_im, int64_t n,
                 const int32_t* targets, int64_t n_t, double k, double* phi, double* fld,
                 void* stream) {

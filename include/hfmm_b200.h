@@ -152,6 +152,17 @@ int hfmm_direct(const double* pos_dev, const double* q_re_dev, const double* q_i
                 int64_t n, const int32_t* targets_dev, int64_t n_t, double k,
                 double* phi_out_dev, double* field_out_dev, void* stream);
 
+/* hfmm_direct without allocation or synchronisation, for a check that overlaps
+ * other work: the caller gives a device scratch of hfmm_direct_scratch_bytes(n,
+ * n_t) bytes and a device int err_dev that out-of-range targets OR ERRF bits into
+ * (the caller zeroes and reads it). Asynchronous on `stream`. No counterpart in
+ * the reference. */
+int64_t hfmm_direct_scratch_bytes(int64_t n, int64_t n_t);
+int hfmm_direct_async(const double* pos_dev, const double* q_re_dev, const double* q_im_dev,
+                      int64_t n, const int32_t* targets_dev, int64_t n_t, double k,
+                      double* phi_out_dev, double* field_out_dev, double* scratch_dev,
+                      int64_t scratch_bytes, int* err_dev, void* stream);
+
 /* Same result as hfmm_direct without allocating anything, for callers that
  * cannot allocate device memory (a JAX/XLA process that owns the GPU memory, a
  * stream under CUDA-graph capture). No counterpart in the reference. The partial
