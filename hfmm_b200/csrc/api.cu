@@ -397,8 +397,8 @@ void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double*
         for (int l = 2; l <= P->md; ++l)
             for (int f = 0; f < NF; ++f) {
                 LevelTables& T = P->tables[f][l];
-                gemm_1(K_CMP, l, f, P->equiv.p + f * fs, P->ld, level_base(T.xc.p, l, T.cld), T.cld);
-                const int64_t cnt = (int64_t)(P->level_hi[l] - P->level_lo[l]) * R * T.cld;
+                gemm_1(K_CMP, l, f, P->equiv.p + f * fs, P->ld, level_base(T.xc.p, l, T.ckld), T.ckld);
+                const int64_t cnt = (int64_t)(P->level_hi[l] - P->level_lo[l]) * R * T.ckld;
                 split_tf32(T.xc.p, T.xc_hi.p, T.xc_lo.p, cnt, s);
             }
     } else if (use_mx) {   // TF32 hi/lo halves of every equivalent density (B operand of the M2L)
@@ -419,15 +419,17 @@ void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double*
                 mc.ntiles = P->mx_tiles[l][R - 1].ntiles;
                 mc.src_tab = P->m2l_src.p;
                 mc.disp_compact = P->disp_compact.p;
-                mc.Bhi = level_base(T.xc_hi.p, l, T.cld);
-                mc.Blo = level_base(T.xc_lo.p, l, T.cld);
+                mc.Bhi = level_base(T.xc_hi.p, l, T.ckld);
+                mc.Blo = level_base(T.xc_lo.p, l, T.ckld);
                 mc.Lhi = nullptr;
                 mc.Llo = nullptr;
-                mc.out = level_base(T.yc.p, l, T.cld);
+                mc.out = level_base(T.yc.p, l, T.cmld);
                 mc.src_lo = P->level_lo[l];   // the level's buffers hold its own boxes only
                 mc.src_hi = P->level_hi[l];
                 mc.R = R;
-                mc.ld = T.cld;
+                mc.ld = T.cmld;
+                mc.ldk = T.ckld;
+                mc.ldm = T.cmld;
                 mc.n_fam = 1;
                 mc.has_l2l = 0;
                 mc.fam_stride = 0;
@@ -439,7 +441,7 @@ void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double*
                     m2l_tf32x3(static_cast<MixedMaps*>(P->cx_maps)[f * MAX_LEVELS + l], mc, s);
                 }
                 PhaseTimer pt(X, s, 14);   // expand y = U y' into the check potential
-                gemm_1(K_EXP, l, f, level_base(T.yc.p, l, T.cld), T.cld, P->check.p + f * fs, P->ld);
+                gemm_1(K_EXP, l, f, level_base(T.yc.p, l, T.cmld), T.cmld, P->check.p + f * fs, P->ld);
             }
             if (l >= 3)   // L2L (phases.py:273-278) in FP64, added to the check potential
                 gemm(K_L2L, l, P->dn_tiles[l][R - 1], P->m2l_src.p + N_DISP, M2L_ENTRIES, P->loc.p,

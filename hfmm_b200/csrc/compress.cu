@@ -18,21 +18,21 @@ namespace {
 
 constexpr int N_M2L = 316;
 
-// compress table, A^T of U^T: out[k][m] = U[k][m] (k < n_s rows of U, m < r), ld x cld
-__global__ void k_pack_cmp(const double* __restrict__ U, int n_s, int r, int ld, int cld,
+// compress table, A^T of U^T: out[k][m] = U[k][m] (k < n_s rows of U, m < r), ld x cw
+__global__ void k_pack_cmp(const double* __restrict__ U, int n_s, int r, int ld, int cw,
                            double* out) {
     const int m = blockIdx.x * blockDim.x + threadIdx.x;
     const int k = blockIdx.y;
-    if (m >= cld || k >= ld) return;
-    out[(int64_t)k * cld + m] = (k < n_s && m < r) ? U[(int64_t)k * r + m] : 0.0;
+    if (m >= cw || k >= ld) return;
+    out[(int64_t)k * cw + m] = (k < n_s && m < r) ? U[(int64_t)k * r + m] : 0.0;
 }
 
-// expand table, A^T of U: out[k][m] = U[m][k] (k < r, m < n_s), cld x ld
-__global__ void k_pack_exp(const double* __restrict__ U, int n_s, int r, int ld, int cld,
+// expand table, A^T of U: out[k][m] = U[m][k] (k < r, m < n_s), ch x ld
+__global__ void k_pack_exp(const double* __restrict__ U, int n_s, int r, int ld, int ch,
                            double* out) {
     const int m = blockIdx.x * blockDim.x + threadIdx.x;
     const int k = blockIdx.y;
-    if (m >= ld || k >= cld) return;
+    if (m >= ld || k >= ch) return;
     out[(int64_t)k * ld + m] = (k < r && m < n_s) ? U[(int64_t)m * r + k] : 0.0;
 }
 
@@ -40,15 +40,16 @@ __device__ __forceinline__ float tf32_round(float x) {
     return __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xFFFFE000u);
 }
 
-// C_d as TF32 hi/lo halves in the A layout [d][m][k] of the tcgen05 kernel (cld x cld)
-__global__ void k_pack_c(const double* __restrict__ C, int r, int cld, float* hi, float* lo) {
+// C_d as TF32 hi/lo halves in the A layout [d][m][k] of the tcgen05 kernel (cmld x ckld)
+__global__ void k_pack_c(const double* __restrict__ C, int r, int ckld, int cmld, float* hi,
+                         float* lo) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int m = blockIdx.y;
     const int d = blockIdx.z;
-    if (k >= cld || m >= cld) return;
+    if (k >= ckld || m >= cmld) return;
     const double v = (m < r && k < r) ? C[((int64_t)d * r + m) * r + k] : 0.0;
     const float h = tf32_round((float)v);
-    const int64_t o = ((int64_t)d * cld + m) * cld + k;
+    const int64_t o = ((int64_t)d * cmld + m) * ckld + k;
     hi[o] = h;
     lo[o] = tf32_round((float)(v - (double)h));
 }
@@ -68,16 +69,16 @@ void compressed_prepare(hfmm_plan* P) {
         for (int l = 2; l <= P->md; ++l) {
             LevelTables& T = P->tables[f][l];
             const size_t rows = (size_t)(P->level_hi[l] - P->level_lo[l]) * 2;   // R <= 2
-            T.xc.alloc(rows * T.cld);
-            T.yc.alloc(rows * T.cld);
-            T.xc_hi.alloc(rows * T.cld);
-            T.xc_lo.alloc(rows * T.cld);
+            T.xc.alloc(rows * T.ckld);
+            T.yc.alloc(rows * T.cmld);
+            T.xc_hi.alloc(rows * T.ckld);
+            T.xc_lo.alloc(rows * T.ckld);
             T.xc.zero();
             T.yc.zero();
             T.xc_hi.zero();
             T.xc_lo.zero();
-            make_table_map(&maps[f * MAX_LEVELS + l].a_hi[0], T.c_hi.p, T.cld, N_M2L);
-            make_table_map(&maps[f * MAX_LEVELS + l].a_lo[0], T.c_lo.p, T.cld, N_M2L);
+            make_table_map(&maps[f * MAX_LEVELS + l].a_hi[0], T.c_hi.p, T.ckld, N_M2L, T.cmld);
+            make_table_map(&maps[f * MAX_LEVELS + l].a_lo[0], T.c_lo.p, T.ckld, N_M2L, T.cmld);
         }
     P->compressed = true;
 }
@@ -100,19 +101,21 @@ int hfmm_plan_set_m2l_compressed(hfmm_plan* P, int32_t family, int32_t level, in
         require_device_ptr(U_dev, "U");
         require_device_ptr(C_dev, "C");
         LevelTables& T = P->tables[family][level];
-        const int cld = std::max(128, (int)round_up(rank, 32));
+        const int ckld = std::max(32, (int)round_up(rank, 32));    // K: one 32-wide chunk at least
+        const int cmld = std::max(128, (int)round_up(rank, 32));   // M: one 128-row MMA tile at least
         T.cr = rank;
-        T.cld = cld;
-        T.c_cmp.alloc((size_t)P->ld * cld);
-        T.c_exp.alloc((size_t)cld * P->ld);
-        T.c_hi.alloc((size_t)N_M2L * cld * cld);
-        T.c_lo.alloc((size_t)N_M2L * cld * cld);
-        HFMM_LAUNCH(k_pack_cmp, dim3((unsigned)ceil_div(cld, 128), (unsigned)P->ld), 128, 0, 0, U_dev,
-                    P->n_s, rank, P->ld, cld, T.c_cmp.p);
-        HFMM_LAUNCH(k_pack_exp, dim3((unsigned)ceil_div(P->ld, 128), (unsigned)cld), 128, 0, 0, U_dev,
-                    P->n_s, rank, P->ld, cld, T.c_exp.p);
-        HFMM_LAUNCH(k_pack_c, dim3((unsigned)ceil_div(cld, 128), (unsigned)cld, N_M2L), 128, 0, 0,
-                    C_dev, rank, cld, T.c_hi.p, T.c_lo.p);
+        T.ckld = ckld;
+        T.cmld = cmld;
+        T.c_cmp.alloc((size_t)P->ld * ckld);
+        T.c_exp.alloc((size_t)cmld * P->ld);
+        T.c_hi.alloc((size_t)N_M2L * cmld * ckld);
+        T.c_lo.alloc((size_t)N_M2L * cmld * ckld);
+        HFMM_LAUNCH(k_pack_cmp, dim3((unsigned)ceil_div(ckld, 128), (unsigned)P->ld), 128, 0, 0,
+                    U_dev, P->n_s, rank, P->ld, ckld, T.c_cmp.p);
+        HFMM_LAUNCH(k_pack_exp, dim3((unsigned)ceil_div(P->ld, 128), (unsigned)cmld), 128, 0, 0,
+                    U_dev, P->n_s, rank, P->ld, cmld, T.c_exp.p);
+        HFMM_LAUNCH(k_pack_c, dim3((unsigned)ceil_div(ckld, 128), (unsigned)cmld, N_M2L), 128, 0, 0,
+                    C_dev, rank, ckld, cmld, T.c_hi.p, T.c_lo.p);
         HFMM_CUDA(cudaDeviceSynchronize());
         P->finalized = false;
         return HFMM_OK;

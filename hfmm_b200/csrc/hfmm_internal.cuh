@@ -85,19 +85,20 @@ struct LevelTables {
     DevBuf<double> m2l;                 // 316 x (A^T), non-adjacent displacements
     // mixed path: TF32 hi/lo halves of M2L and L2L as A[m][k] (fp32 containers)
     DevBuf<float> m2l_hi, m2l_lo, l2l_hi, l2l_lo;
-    // compressed M2L of the mixed path, K_d ~ U C_d U^T (rank cr, padded to cld)
-    int cr = 0, cld = 0;
-    DevBuf<double> c_cmp, c_exp;   // A^T of U^T (ld -> cld) and of U (cld -> ld)
-    DevBuf<float> c_hi, c_lo;      // C_d halves as A [316][m][k], cld x cld
-    DevBuf<double> xc, yc;         // the level's compressed densities / check potentials
-    DevBuf<float> xc_hi, xc_lo;    // [box of the level][R][cld]
+    // compressed M2L of the mixed path, K_d ~ U C_d U^T (rank cr): the K side padded
+    // to ckld (>= 32), the M side to cmld (>= 128, the MMA tile), both multiples of 32
+    int cr = 0, ckld = 0, cmld = 0;
+    DevBuf<double> c_cmp, c_exp;   // A^T of U^T (ld -> ckld) and of U (cmld -> ld)
+    DevBuf<float> c_hi, c_lo;      // C_d halves as A [316][cmld][ckld]
+    DevBuf<double> xc, yc;         // the level's compressed densities [.][R][ckld] and
+    DevBuf<float> xc_hi, xc_lo;    // check potentials [.][R][cmld] (box - level_lo first)
     bool set = false;
     void reset() {
         up_U.release(); up_d.release(); up_Vt.release();
         dn_U.release(); dn_d.release(); dn_Vt.release();
         m2m.release(); l2l.release(); m2l.release();
         m2l_hi.release(); m2l_lo.release(); l2l_hi.release(); l2l_lo.release();
-        cr = cld = 0;
+        cr = ckld = cmld = 0;
         c_cmp.release(); c_exp.release(); c_hi.release(); c_lo.release();
         xc.release(); yc.release(); xc_hi.release(); xc_lo.release();
         set = false;

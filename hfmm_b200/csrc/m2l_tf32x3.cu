@@ -271,7 +271,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_m2l_tf32x3(const __grid_constant
     }
     __syncthreads();
     const int n_act = ctl.n_act;
-    const int kch = c.ld / BK;
+    const int kch = c.ldk / BK;
     const int nq = n_act * kch;
     const uint32_t tmem = ctl.tmem;
     const int64_t fs = (int64_t)fam * c.fam_stride;
@@ -320,7 +320,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_m2l_tf32x3(const __grid_constant
                         atomicOr(c.err, ERRF_BOUNDS);
                         s_ = -1;
                     }
-                    goff[i] = s_ >= 0 ? ((int64_t)s_ * R + (n % R)) * c.ld + ch * 4 : -1;
+                    goff[i] = s_ >= 0 ? ((int64_t)s_ * R + (n % R)) * c.ldk + ch * 4 : -1;
                 }
                 if (ai + 1 < n_act) load_sources(ai + 1);
             }
@@ -394,7 +394,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_m2l_tf32x3(const __grid_constant
         const bool aborted = !__all_sync(0xffffffffu, ok && !*abort_flag);
         if (aborted) {
             if (lane == 0) atomicOr(c.err, ERRF_TIMEOUT);
-        } else if (m0 + quad * 32 < c.ld) {   // ld % 32 == 0: a warp is all in or all out
+        } else if (m0 + quad * 32 < c.ldm) {   // ldm % 32 == 0: a warp is all in or all out
             for (int cb = c_lo; cb < c_lo + COLS_PER_FOLD_WARP; cb += SUB) {
                 uint32_t w[2 * SUB];
                 if (nq > 0) {
@@ -407,7 +407,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_m2l_tf32x3(const __grid_constant
                     const int n = cb + j;
                     const int t = ctl.tgt[n / R];
                     const double val = nq > 0 ? __hiloint2double((int)w[2 * j + 1], (int)w[2 * j]) : 0.0;
-                    if (t >= 0) out[((int64_t)t * R + (n % R)) * c.ld + m] = val;
+                    if (t >= 0) out[((int64_t)t * R + (n % R)) * c.ldm + m] = val;
                 }
             }
         }
@@ -546,11 +546,13 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
 
 }  // namespace
 
-void make_table_map(CUtensorMap* map, const float* base, int ld, int count) {
-    if (((uintptr_t)base & 15) || (ld * 4) % 16)
-        throw Error{HFMM_ERR_STATE, "tensor map: table not 16-byte aligned"};
-    cuuint64_t dims[3] = {(cuuint64_t)ld, (cuuint64_t)ld, (cuuint64_t)count};
-    cuuint64_t strides[2] = {(cuuint64_t)ld * 4, (cuuint64_t)ld * ld * 4};
+void make_table_map(CUtensorMap* map, const float* base, int ld, int count, int ldm) {
+    // [count][ldm][ld] fp32 (ldm = 0: square), boxes of 32 k x 128 m
+    if (!ldm) ldm = ld;
+    if (((uintptr_t)base & 15) || (ld * 4) % 16 || ld < BK || ldm < BM)
+        throw Error{HFMM_ERR_STATE, "tensor map: table not 16-byte aligned or smaller than a box"};
+    cuuint64_t dims[3] = {(cuuint64_t)ld, (cuuint64_t)ldm, (cuuint64_t)count};
+    cuuint64_t strides[2] = {(cuuint64_t)ld * 4, (cuuint64_t)ld * ldm * 4};
     cuuint32_t box[3] = {BK, BM, 1};
     cuuint32_t estr[3] = {1, 1, 1};
     CUresult r = encode_fn()(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, (void*)base, dims, strides,
@@ -571,11 +573,15 @@ void split_transpose_tables(const double* at, float* hi, float* lo, int ld, int 
 
 size_t m2l_tf32x3_smem() { return (size_t)STAGES * STAGE_BYTES + sizeof(Ctl) + 1024; }
 
-void m2l_tf32x3(const MixedMaps& maps, const MixedCall& c, cudaStream_t s) {
-    if (c.ntiles == 0) return;
-    if (c.ld % BK) throw Error{HFMM_ERR_STATE, "m2l_tf32x3: ld must be a multiple of 32"};
+void m2l_tf32x3(const MixedMaps& maps, const MixedCall& call, cudaStream_t s) {
+    if (call.ntiles == 0) return;
+    MixedCall c = call;
+    if (!c.ldk) c.ldk = c.ld;
+    if (!c.ldm) c.ldm = c.ld;
+    if (c.ldk % BK || c.ldm % BK)
+        throw Error{HFMM_ERR_STATE, "m2l_tf32x3: ld must be a multiple of 32"};
     const size_t smem = m2l_tf32x3_smem();
-    dim3 grid(c.ntiles, (c.ld + BM - 1) / BM, c.n_fam);
+    dim3 grid(c.ntiles, (c.ldm + BM - 1) / BM, c.n_fam);
     if (c.R == 1) {
         HFMM_CUDA(cudaFuncSetAttribute(k_m2l_tf32x3<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         HFMM_LAUNCH(k_m2l_tf32x3<1>, grid, THREADS, smem, s, maps, c);

@@ -23,12 +23,14 @@ struct MixedCall {
     const float* Llo;
     double* out;                   // check potentials [fam][box][R][ld], FP64
     int R, ld, n_fam, has_l2l;
+    int ldk, ldm;                  // rectangular tables: K extent (B rows) and M extent (out
+                                   // rows); 0 = ld. A tables are [count][ldm][ldk]
     int64_t fam_stride, out_fam_stride, nb;
     int64_t src_lo, src_hi;        // valid source boxes [src_lo, src_hi) (0, nb when unset)
     int* err;
 };
 
-void make_table_map(CUtensorMap* map, const float* base, int ld, int count);
+void make_table_map(CUtensorMap* map, const float* base, int ld, int count, int ldm = 0);
 void split_tf32(const double* src, float* hi, float* lo, int64_t n, cudaStream_t s);
 void split_transpose_tables(const double* at, float* hi, float* lo, int ld, int count);
 void m2l_tf32x3(const MixedMaps& maps, const MixedCall& c, cudaStream_t s);
