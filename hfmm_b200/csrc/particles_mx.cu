@@ -17,20 +17,29 @@ namespace hfmm {
 
 namespace {
 
-constexpr int STAGE = 128;
+#ifndef HFMM_P2P_TPL
+#define HFMM_P2P_TPL 2
+#endif
+constexpr int WARPS = 4;               // target leaves per CTA, one warp each
+constexpr int TPL = HFMM_P2P_TPL;      // targets per lane held at once (32 * TPL per pass)
+constexpr int CHAIN = 128;             // sources per FP32 partial-sum chain
 
+// One warp per target leaf: each lane keeps TPL targets in registers; the sources
+// of each near leaf are loaded 32 at a time, one per lane, and broadcast with warp
+// shuffles, so the kernel needs neither shared memory nor CTA barriers.
 template <int NF, int R, bool FIELD>
-__global__ void __launch_bounds__(128) k_p2p_mx(EvalView v, const int32_t* __restrict__ leaves,
-                                               const int32_t* __restrict__ off,
-                                               const int32_t* __restrict__ srcs, double* pot,
-                                               double* fld) {
+__global__ void __launch_bounds__(WARPS * 32) k_p2p_mx(EvalView v, const int32_t* __restrict__ leaves,
+                                                      int64_t nrows, const int32_t* __restrict__ off,
+                                                      const int32_t* __restrict__ srcs, double* pot,
+                                                      double* fld) {
     // Pair separations come from the FP32 hi/lo position pairs, (hi - hi') + (lo - lo'),
     // so each carries a relative error of about eps32 however close the points are
     // (clustered clouds); everything after that runs in FP32. The phase k r is an
     // FP32 product: r itself carries eps32, so a wider product would add nothing.
-    __shared__ float sxh[STAGE], syh[STAGE], szh[STAGE], sxl[STAGE], syl[STAGE], szl[STAGE];
-    __shared__ float sq[R][STAGE];
-    const int row = blockIdx.x;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t row = (int64_t)blockIdx.x * WARPS + warp;
+    if (row >= nrows) return;   // the whole warp leaves together
+    const unsigned FULL = 0xffffffffu;
     const int t = leaves[row];
     const int s0t = v.leaf_start[t], cnt_t = v.counts[t];
     constexpr int NA = NF * R * (FIELD ? 4 : 1);
@@ -38,89 +47,110 @@ __global__ void __launch_bounds__(128) k_p2p_mx(EvalView v, const int32_t* __res
     const double rt = v.rmax[t];
     const float kf = (float)v.k;
     const int64_t n = v.n;
-    for (int i0 = 0; i0 < cnt_t; i0 += blockDim.x) {
-        const int i = i0 + threadIdx.x;
-        const bool act = i < cnt_t;
-        float xh = 0, yh = 0, zh = 0, xl = 0, yl = 0, zl = 0;
-        if (act) {
-            const int64_t gi = s0t + i;
-            xh = v.pos_f[gi];
-            yh = v.pos_f[n + gi];
-            zh = v.pos_f[2 * n + gi];
-            xl = v.pos_f[3 * n + gi];
-            yl = v.pos_f[4 * n + gi];
-            zl = v.pos_f[5 * n + gi];
-        }
-        double acc[NA];
+    const int e0 = off[row], e1 = off[row + 1];
+    for (int i0 = 0; i0 < cnt_t; i0 += 32 * TPL) {
+        float xh[TPL], yh[TPL], zh[TPL], xl[TPL], yl[TPL], zl[TPL];
+        bool act[TPL];
+        double acc[TPL][NA];
 #pragma unroll
-        for (int q = 0; q < NA; ++q) acc[q] = 0.0;
-        for (int e = off[row]; e < off[row + 1]; ++e) {
+        for (int u = 0; u < TPL; ++u) {
+            const int i = i0 + 32 * u + lane;
+            act[u] = i < cnt_t;
+            const int64_t gi = s0t + (act[u] ? i : 0);
+            xh[u] = v.pos_f[gi];
+            yh[u] = v.pos_f[n + gi];
+            zh[u] = v.pos_f[2 * n + gi];
+            xl[u] = v.pos_f[3 * n + gi];
+            yl[u] = v.pos_f[4 * n + gi];
+            zl[u] = v.pos_f[5 * n + gi];
+#pragma unroll
+            for (int q = 0; q < NA; ++q) acc[u][q] = 0.0;
+        }
+        for (int e = e0; e < e1; ++e) {
             const int sb = srcs[e];
             const int s0 = v.leaf_start[sb], cnt = v.counts[sb];
             const double rs = rt + v.rmax[sb];
             const float thr = (float)(C16 * rs * rs);
-            for (int p0 = 0; p0 < cnt; p0 += STAGE) {
-                __syncthreads();
-                for (int k = threadIdx.x; k < STAGE && p0 + k < cnt; k += blockDim.x) {
-                    const int64_t gi = s0 + p0 + k;
-                    sxh[k] = v.pos_f[gi];
-                    syh[k] = v.pos_f[n + gi];
-                    szh[k] = v.pos_f[2 * n + gi];
-                    sxl[k] = v.pos_f[3 * n + gi];
-                    syl[k] = v.pos_f[4 * n + gi];
-                    szl[k] = v.pos_f[5 * n + gi];
+            for (int c0 = 0; c0 < cnt; c0 += CHAIN) {
+                const int cend = min(cnt, c0 + CHAIN);
+                float a32[TPL][NA];
 #pragma unroll
-                    for (int r = 0; r < R; ++r) sq[r][k] = (float)v.q_s[r * n + gi];
-                }
-                __syncthreads();
-                if (!act) continue;
-                const int np = min(STAGE, cnt - p0);
-                float a32[NA];
+                for (int u = 0; u < TPL; ++u)
 #pragma unroll
-                for (int q = 0; q < NA; ++q) a32[q] = 0.f;
-                for (int k = 0; k < np; ++k) {
-                    const float dx = (xh - sxh[k]) + (xl - sxl[k]);
-                    const float dy = (yh - syh[k]) + (yl - syl[k]);
-                    const float dz = (zh - szh[k]) + (zl - szl[k]);
-                    const float d2 = dx * dx + dy * dy + dz * dz;
-                    if (!(d2 > thr)) continue;
-                    const float ir = rsqrtf(d2);
-                    const float rr = d2 * ir;
-                    const float kr = kf * rr;
-                    float sn, cs_;
-                    sincosf(kr, &sn, &cs_);
-                    const float w[2] = {cs_ * ir, sn * ir};
-                    float wf[2] = {0.f, 0.f};
-                    if (FIELD) {
-                        const float ir3 = ir * ir * ir;
-                        wf[0] = (cs_ + kr * sn) * ir3;
-                        wf[1] = (sn - kr * cs_) * ir3;
+                    for (int q = 0; q < NA; ++q) a32[u][q] = 0.f;
+                for (int b0 = c0; b0 < cend; b0 += 32) {
+                    const int nbat = min(32, cend - b0);
+                    float pxh = 0, pyh = 0, pzh = 0, pxl = 0, pyl = 0, pzl = 0, pq[R];
+#pragma unroll
+                    for (int r = 0; r < R; ++r) pq[r] = 0.f;
+                    if (lane < nbat) {
+                        const int64_t gs = s0 + b0 + lane;
+                        pxh = v.pos_f[gs];
+                        pyh = v.pos_f[n + gs];
+                        pzh = v.pos_f[2 * n + gs];
+                        pxl = v.pos_f[3 * n + gs];
+                        pyl = v.pos_f[4 * n + gs];
+                        pzl = v.pos_f[5 * n + gs];
+#pragma unroll
+                        for (int r = 0; r < R; ++r) pq[r] = (float)v.q_s[r * n + gs];
                     }
+                    for (int j = 0; j < nbat; ++j) {
+                        const float sxh = __shfl_sync(FULL, pxh, j), syh = __shfl_sync(FULL, pyh, j);
+                        const float szh = __shfl_sync(FULL, pzh, j), sxl = __shfl_sync(FULL, pxl, j);
+                        const float syl = __shfl_sync(FULL, pyl, j), szl = __shfl_sync(FULL, pzl, j);
+                        float sq[R];
 #pragma unroll
-                    for (int f = 0; f < NF; ++f)
+                        for (int r = 0; r < R; ++r) sq[r] = __shfl_sync(FULL, pq[r], j);
 #pragma unroll
-                        for (int r = 0; r < R; ++r) {
-                            const float qv = sq[r][k];
-                            a32[f * R + r] += qv * w[f];
+                        for (int u = 0; u < TPL; ++u) {
+                            const float dx = (xh[u] - sxh) + (xl[u] - sxl);
+                            const float dy = (yh[u] - syh) + (yl[u] - syl);
+                            const float dz = (zh[u] - szh) + (zl[u] - szl);
+                            const float d2 = dx * dx + dy * dy + dz * dz;
+                            if (!(d2 > thr)) continue;
+                            const float ir = rsqrtf(d2);
+                            const float rr = d2 * ir;
+                            const float kr = kf * rr;
+                            float sn, cs_;
+                            sincosf(kr, &sn, &cs_);
+                            const float w[2] = {cs_ * ir, sn * ir};
+                            float wf[2] = {0.f, 0.f};
                             if (FIELD) {
-                                const float qw = qv * wf[f];
-                                a32[NF * R + (f * R + r) * 3 + 0] += qw * dx;
-                                a32[NF * R + (f * R + r) * 3 + 1] += qw * dy;
-                                a32[NF * R + (f * R + r) * 3 + 2] += qw * dz;
+                                const float ir3 = ir * ir * ir;
+                                wf[0] = (cs_ + kr * sn) * ir3;
+                                wf[1] = (sn - kr * cs_) * ir3;
                             }
+#pragma unroll
+                            for (int f = 0; f < NF; ++f)
+#pragma unroll
+                                for (int r = 0; r < R; ++r) {
+                                    const float qv = sq[r];
+                                    a32[u][f * R + r] += qv * w[f];
+                                    if (FIELD) {
+                                        const float qw = qv * wf[f];
+                                        a32[u][NF * R + (f * R + r) * 3 + 0] += qw * dx;
+                                        a32[u][NF * R + (f * R + r) * 3 + 1] += qw * dy;
+                                        a32[u][NF * R + (f * R + r) * 3 + 2] += qw * dz;
+                                    }
+                                }
                         }
+                    }
                 }
 #pragma unroll
-                for (int q = 0; q < NA; ++q) acc[q] += (double)a32[q];
+                for (int u = 0; u < TPL; ++u)
+#pragma unroll
+                    for (int q = 0; q < NA; ++q) acc[u][q] += (double)a32[u][q];
             }
         }
-        if (act) {
-            const int64_t gi = s0t + i;
 #pragma unroll
-            for (int q = 0; q < NF * R; ++q) pot[q * n + gi] = acc[q];
+        for (int u = 0; u < TPL; ++u) {
+            if (!act[u]) continue;
+            const int64_t gi = s0t + i0 + 32 * u + lane;
+#pragma unroll
+            for (int q = 0; q < NF * R; ++q) pot[q * n + gi] = acc[u][q];
             if (FIELD)
 #pragma unroll
-                for (int q = 0; q < NF * R * 3; ++q) fld[q * n + gi] = acc[NF * R + q];
+                for (int q = 0; q < NF * R * 3; ++q) fld[q * n + gi] = acc[u][NF * R + q];
         }
     }
 }
@@ -129,8 +159,8 @@ template <int NF, int R, bool FIELD>
 void impl(const ParticlePass& p, cudaStream_t s) {
     if (p.op != ParticleOp::P2P)
         throw Error{HFMM_ERR_STATE, "particles_mixed: only the near field runs in FP32"};
-    HFMM_LAUNCH((k_p2p_mx<NF, R, FIELD>), p.nrows, 128, 0, s, p.v, p.rows, p.off, p.srcs,
-                p.pot, p.fld);
+    HFMM_LAUNCH((k_p2p_mx<NF, R, FIELD>), (unsigned)ceil_div(p.nrows, WARPS), WARPS * 32, 0, s, p.v,
+                p.rows, p.nrows, p.off, p.srcs, p.pot, p.fld);
 }
 
 }  // namespace
