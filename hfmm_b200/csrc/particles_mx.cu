@@ -18,10 +18,13 @@ namespace hfmm {
 namespace {
 
 #ifndef HFMM_P2P_TPL
-#define HFMM_P2P_TPL 2
+#define HFMM_P2P_TPL 1
 #endif
 constexpr int WARPS = 4;               // target leaves per CTA, one warp each
-constexpr int TPL = HFMM_P2P_TPL;      // targets per lane held at once (32 * TPL per pass)
+// targets per lane held at once (32 * TPL per pass); on the 1M-point p = 8 near
+// field 1 was fastest (5.0 ms, against 6.6 for 2 and 8.0 for the former
+// one-CTA-per-leaf kernel; same bits)
+constexpr int TPL = HFMM_P2P_TPL;
 constexpr int CHAIN = 128;             // sources per FP32 partial-sum chain
 
 // One warp per target leaf: each lane keeps TPL targets in registers; the sources

@@ -6,7 +6,8 @@ never checks the result. Here a 3 x 64 FP32 network (the CUDA kernels of
 
 * output 0: the smallest expansion order ``p`` (surface points per cube edge)
   whose evaluate meets the requested tolerance, as a real number;
-* output 1: log2 of the fastest leaf size ``N_max`` (16..128, automatic depth).
+* output 1: log2 of the fastest leaf size ``N_max`` (automatic depth), used as 64
+  or 128 (``OrderNet.choose_from``).
 
 The mixed-precision plans also get a low-rank M2L (``hfmm_b200.compress``) at a
 hundredth of the tolerance.
@@ -213,9 +214,14 @@ class OrderNet:
 
     @staticmethod
     def choose_from(y, margin=0.5):
-        """(p, N_max) from one output row (fractional p, log2 leaf size)."""
+        """(p, N_max) from one output row (fractional p, log2 leaf size).
+
+        The leaf size is kept to 64 or 128: p is predicted from the tree at leaf 64,
+        and a smaller leaf can deepen the tree beyond what that prediction saw (on a
+        1M-point cloud, outside the sweep's sizes, leaf 16 gave a depth-6 tree whose
+        mixed evaluate missed 1e-6 at the predicted p)."""
         p = int(min(P_MAX, max(P_MIN, math.ceil(float(y[0]) + margin))))
-        leaf = int(2 ** min(7, max(4, round(float(y[1])))))
+        leaf = int(2 ** min(7, max(6, round(float(y[1])))))
         return p, leaf
 
 

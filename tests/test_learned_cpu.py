@@ -113,3 +113,11 @@ def test_training_samples_from_sweep():
     assert T[1, 0] == pytest.approx(6.0)          # mixed curve at 1e-6
     assert T[2, 0] == pytest.approx(7.0)          # FP64 curve at 1e-8
     assert T[0, 1] == 5.0 and T[3, 1] == 4.0      # log2 of the fastest leaf size
+
+
+def test_choose_keeps_the_leaf_at_64_or_128():
+    from hfmm_b200.learned import OrderNet
+    assert OrderNet.choose_from([7.6, 4.0]) == (9, 64)      # p rounded up after the margin
+    assert OrderNet.choose_from([7.4, 7.6]) == (8, 128)
+    assert OrderNet.choose_from([2.0, 9.0]) == (4, 128)     # p clamped to [4, 16]
+    assert OrderNet.choose_from([30.0, 6.4]) == (16, 64)
