@@ -372,7 +372,8 @@ void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double*
         return buf - (int64_t)P->level_lo[l] * R * cld;
     };
     // one-entry GEMM over every box of level l between layouts of different widths
-    auto gemm_1 = [&](int kind, int l, int f, const double* in, int ldk, double* out, int ldm) {
+    auto gemm_1 = [&](int kind, int l, int f, const double* in, int ldk, double* out, int ldm,
+                      cudaStream_t st) {
         GemmCall c{};
         c.tile_tgt = P->dec_tiles[l][R - 1].tgt.p;
         c.ntiles = P->dec_tiles[l][R - 1].ntiles;
@@ -390,14 +391,15 @@ void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double*
         c.n_s = P->n_s;
         c.n_fam = 1;
         c.nb = P->nb;
-        gemm_f64(c, P->d_err.p, s);
+        gemm_f64(c, P->d_err.p, st);
     };
     if (use_cx) {   // compress every level's densities (x' = U^T x), then split them
         PhaseTimer pt(X, s, 14);
         for (int l = 2; l <= P->md; ++l)
             for (int f = 0; f < NF; ++f) {
                 LevelTables& T = P->tables[f][l];
-                gemm_1(K_CMP, l, f, P->equiv.p + f * fs, P->ld, level_base(T.xc.p, l, T.ckld), T.ckld);
+                gemm_1(K_CMP, l, f, P->equiv.p + f * fs, P->ld, level_base(T.xc.p, l, T.ckld), T.ckld,
+                       s);
                 const int64_t cnt = (int64_t)(P->level_hi[l] - P->level_lo[l]) * R * T.ckld;
                 split_tf32(T.xc.p, T.xc_hi.p, T.xc_lo.p, cnt, s);
             }
@@ -405,14 +407,20 @@ void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double*
         PhaseTimer pt(X, s, 11);
         split_tf32(P->equiv.p, P->e_hi.p, P->e_lo.p, (int64_t)NF * fs, s);
     }
-    // ---- downward pass (M2L + L2L in one GEMM, then X-list P2L, then decode)
-    for (int l = 2; l <= P->md; ++l) {
-        if (P->streamed && !use_cx) {
-            PhaseTimer pt(X, s, 12);
-            generate_m2l_stream(P, l, use_mx, P->ws, s);
-        }
-        if (use_cx) {
+    if (use_cx) {
+        // A level's M2L reads only the compressed densities of the upward pass, so the
+        // M2Ls of every level and family run at once on the plan's side streams (the
+        // coarse levels have a handful of tiles each and would otherwise run alone on
+        // a few SMs); each expands into its own level's check potentials. The downward
+        // chain below starts after the join.
+        PhaseTimer pt(X, s, 4);
+        HFMM_CUDA(cudaEventRecord(P->cx_fork, s));
+        for (int k = 0; k < hfmm_plan::CX_STREAMS; ++k)
+            HFMM_CUDA(cudaStreamWaitEvent(P->cx_side[k], P->cx_fork, 0));
+        int slot = 0;
+        for (int l = P->md; l >= 2; --l)   // the largest levels first
             for (int f = 0; f < NF; ++f) {
+                cudaStream_t ss = P->cx_side[slot++ % hfmm_plan::CX_STREAMS];
                 LevelTables& T = P->tables[f][l];
                 MixedCall mc{};
                 mc.tile_tgt = P->mx_tiles[l][R - 1].tgt.p;
@@ -436,13 +444,23 @@ void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double*
                 mc.out_fam_stride = 0;
                 mc.nb = P->nb;
                 mc.err = P->d_err.p;
-                {
-                    PhaseTimer pt(X, s, 4);
-                    m2l_tf32x3(static_cast<MixedMaps*>(P->cx_maps)[f * MAX_LEVELS + l], mc, s);
-                }
-                PhaseTimer pt(X, s, 14);   // expand y = U y' into the check potential
-                gemm_1(K_EXP, l, f, level_base(T.yc.p, l, T.cmld), T.cmld, P->check.p + f * fs, P->ld);
+                m2l_tf32x3(static_cast<MixedMaps*>(P->cx_maps)[f * MAX_LEVELS + l], mc, ss);
+                // expand y = U y' into the check potential (overwrites the upward leftovers)
+                gemm_1(K_EXP, l, f, level_base(T.yc.p, l, T.cmld), T.cmld, P->check.p + f * fs,
+                       P->ld, ss);
             }
+        for (int k = 0; k < hfmm_plan::CX_STREAMS; ++k) {
+            HFMM_CUDA(cudaEventRecord(P->cx_join[k], P->cx_side[k]));
+            HFMM_CUDA(cudaStreamWaitEvent(s, P->cx_join[k], 0));
+        }
+    }
+    // ---- downward pass (M2L + L2L in one GEMM, then X-list P2L, then decode)
+    for (int l = 2; l <= P->md; ++l) {
+        if (P->streamed && !use_cx) {
+            PhaseTimer pt(X, s, 12);
+            generate_m2l_stream(P, l, use_mx, P->ws, s);
+        }
+        if (use_cx) {   // M2L done above, concurrently for every level
             if (l >= 3)   // L2L (phases.py:273-278) in FP64, added to the check potential
                 gemm(K_L2L, l, P->dn_tiles[l][R - 1], P->m2l_src.p + N_DISP, M2L_ENTRIES, P->loc.p,
                      nullptr, P->check.p, nullptr);
@@ -884,6 +902,7 @@ void hfmm_plan_destroy(hfmm_plan* P) {
     P->mx_maps = nullptr;
     delete[] static_cast<MixedMaps*>(P->cx_maps);
     P->cx_maps = nullptr;
+    compressed_release(P);
     delete P;
 }
 

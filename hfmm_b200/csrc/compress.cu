@@ -80,7 +80,25 @@ void compressed_prepare(hfmm_plan* P) {
             make_table_map(&maps[f * MAX_LEVELS + l].a_hi[0], T.c_hi.p, T.ckld, N_M2L, T.cmld);
             make_table_map(&maps[f * MAX_LEVELS + l].a_lo[0], T.c_lo.p, T.ckld, N_M2L, T.cmld);
         }
+    if (!P->cx_fork) {   // side streams and fork/join events of the concurrent M2L
+        HFMM_CUDA(cudaEventCreateWithFlags(&P->cx_fork, cudaEventDisableTiming));
+        for (int k = 0; k < hfmm_plan::CX_STREAMS; ++k) {
+            HFMM_CUDA(cudaStreamCreateWithFlags(&P->cx_side[k], cudaStreamNonBlocking));
+            HFMM_CUDA(cudaEventCreateWithFlags(&P->cx_join[k], cudaEventDisableTiming));
+        }
+    }
     P->compressed = true;
+}
+
+void compressed_release(hfmm_plan* P) {
+    if (P->cx_fork) cudaEventDestroy(P->cx_fork);
+    for (int k = 0; k < hfmm_plan::CX_STREAMS; ++k) {
+        if (P->cx_side[k]) cudaStreamDestroy(P->cx_side[k]);
+        if (P->cx_join[k]) cudaEventDestroy(P->cx_join[k]);
+        P->cx_side[k] = nullptr;
+        P->cx_join[k] = nullptr;
+    }
+    P->cx_fork = nullptr;
 }
 
 }  // namespace hfmm

@@ -171,6 +171,9 @@ struct hfmm_plan {
     void* mx_maps = nullptr;                // MixedMaps per level (host array)
     bool compressed = false;                // every level has a compressed M2L (mixed path)
     void* cx_maps = nullptr;                // MixedMaps [2][MAX_LEVELS] of the C_d tables
+    static constexpr int CX_STREAMS = 4;    // side streams of the concurrent compressed M2L
+    cudaStream_t cx_side[CX_STREAMS] = {};
+    cudaEvent_t cx_fork = nullptr, cx_join[CX_STREAMS] = {};
     bool mixed_ready = false;
     // streamed M2L tables: regenerated per level and evaluate into a workspace
     // (the plan's own, or one bound by the caller and shared by plans that run in turn)
@@ -204,7 +207,8 @@ size_t stream_ws_bytes(const hfmm_plan* P);
 bool plan_profiling(hfmm_plan* P);
 void batch_forget_plan(struct hfmm_batch* B, hfmm_plan* P);
 void generate_m2l_stream(hfmm_plan* P, int level, bool mixed, void* ws, cudaStream_t s);
-void compressed_prepare(hfmm_plan* P);   // finalize: buffers and tensor maps
+void compressed_prepare(hfmm_plan* P);   // finalize: buffers, tensor maps, side streams
+void compressed_release(hfmm_plan* P);   // plan destroy: side streams and events
 void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double* phi,
                    double* fld, cudaStream_t s, bool mixed = false);
 void direct_sum(const double* pos, const double* q_re, const double* q_im, int64_t n,
