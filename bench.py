@@ -642,6 +642,7 @@ def run_auto(a, cfg, rank, world, local_rank):
         achieved = flops / (dom_ms * 1e-3) / 1e12 if dom_ms > 0 else None
         roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                 "frac": (achieved / peak) if achieved else None, "traffic": _traffic(a, "auto"),
+                "traffic_unit": "bytes per evaluate (all M2L launches), from profiles/traffic.json",
                 "kernel": ("k_m2l_tf32x3 (M2L, 3xTF32 on tcgen05, all levels"
                            + (", on the low-rank C_d tables)" if ap.m2l_compress else ")")),
                 "algorithmic_flops_per_evaluate": flops, "kernel_ms_per_evaluate": dom_ms,
@@ -773,11 +774,14 @@ def run_batch(a, cfg, rank, world, local_rank):
 
 
 def _traffic(a, mode):
+    """DRAM bytes per evaluate of the roofline kernel from a committed ncu capture
+    (profiles/traffic.json), or None when no capture covers this configuration."""
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
     if not os.path.exists(tpath):
         return None
     try:
-        return json.load(open(tpath)).get(f"{a.config}:{mode}")
+        e = json.load(open(tpath)).get(f"{a.config}:{mode}")
+        return float(e["bytes"]) if e else None
     except Exception:
         return None
 
