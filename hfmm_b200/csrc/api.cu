@@ -278,9 +278,9 @@ void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double*
     // feed the damped decodes and L2P/M2P read their output; for the sin component
     // (eps_rel 1e-12) FP32 noise there is amplified along near-null singular
     // directions, so those phases stay FP64.
-    auto particles = [&](const ParticlePass& p) {
-        if (mixed && p.op == ParticleOp::P2P) particles_mixed(p, s);
-        else particles_f64(p, s);
+    auto particles = [&](const ParticlePass& p, cudaStream_t st) {
+        if (mixed && p.op == ParticleOp::P2P) particles_mixed(p, st);
+        else particles_f64(p, st);
     };
     ParticlePass base;
     base.v = v;
@@ -290,6 +290,23 @@ void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double*
     base.fam_stride = fs;
     base.pot = P->pot.p;
     base.fld = P->fld.p;
+
+    // The near field needs only the gathered charges: it runs on the plan's side
+    // stream beside the whole far field and joins before L2P, which adds into the
+    // potentials and fields P2P stores.
+    HFMM_CUDA(cudaEventRecord(P->nf_fork, s));
+    HFMM_CUDA(cudaStreamWaitEvent(P->nf_side, P->nf_fork, 0));
+    {
+        ParticlePass p = base;
+        p.op = ParticleOp::P2P;
+        p.rows = P->leaves.p;
+        p.nrows = P->n_leaves;
+        p.off = P->near_off.p;
+        p.srcs = P->near_src.p;
+        PhaseTimer pt(X, P->nf_side, 7);
+        particles(p, P->nf_side);
+    }
+    HFMM_CUDA(cudaEventRecord(P->nf_join, P->nf_side));
 
     auto gemm = [&](int kind, int l, const hfmm_plan::Tiles& tiles, const int32_t* src_tab,
                     int src_ld, const double* B0, const double* B1, double* out,
@@ -356,7 +373,7 @@ void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double*
         p.surf = P->check_pts.p;
         p.out = P->check.p;
         PhaseTimer pt(X, s, 1);
-        particles(p);
+        particles(p, s);
     }
     for (int l = P->md; l >= 2; --l) {
         if (l < P->md)
@@ -505,23 +522,14 @@ void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double*
             p.out = P->check.p;
             p.level = l;
             PhaseTimer pt(X, s, 5);
-            particles(p);
+            particles(p, s);
         }
         decode(l, false, P->check.p, P->loc.p);
     }
-    // ---- particle outputs: near field stores, far field and W list add
+    // ---- particle outputs: the near field (above) stores, far field and W list add
+    HFMM_CUDA(cudaStreamWaitEvent(s, P->nf_join, 0));
     {
         ParticlePass p = base;
-        p.op = ParticleOp::P2P;
-        p.rows = P->leaves.p;
-        p.nrows = P->n_leaves;
-        p.off = P->near_off.p;
-        p.srcs = P->near_src.p;
-        {
-            PhaseTimer pt(X, s, 7);
-            particles(p);
-        }
-        p = base;
         p.op = ParticleOp::L2P;
         p.rows = P->leaves.p;
         p.nrows = P->n_leaves;
@@ -529,7 +537,7 @@ void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double*
         p.dens = P->loc.p;
         {
             PhaseTimer pt(X, s, 8);
-            particles(p);
+            particles(p, s);
         }
         if (P->nW) {
             p = base;
@@ -541,7 +549,7 @@ void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double*
             p.surf = P->equiv_pts.p;
             p.dens = P->equiv.p;
             PhaseTimer pt(X, s, 9);
-            particles(p);
+            particles(p, s);
         }
         p = base;
         p.op = ParticleOp::COMBINE;
@@ -549,7 +557,7 @@ void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double*
         p.phi = phi;
         p.E = E;
         PhaseTimer pt(X, s, 10);
-        particles(p);
+        particles(p, s);
     }
 }
 
@@ -755,6 +763,11 @@ int hfmm_plan_finalize(hfmm_plan* P) {
     }
     PlanExtra* X = extra(P, true);
     build_a_ptrs(P, X->ix);   // streamed plans without a workspace yet: see evaluate
+    if (!P->nf_side) {
+        HFMM_CUDA(cudaStreamCreateWithFlags(&P->nf_side, cudaStreamNonBlocking));
+        HFMM_CUDA(cudaEventCreateWithFlags(&P->nf_fork, cudaEventDisableTiming));
+        HFMM_CUDA(cudaEventCreateWithFlags(&P->nf_join, cudaEventDisableTiming));
+    }
     const size_t exp = (size_t)P->n_fam * P->nb * 2 * P->ld;
     P->check.alloc(exp);
     P->equiv.alloc(exp);
@@ -903,6 +916,9 @@ void hfmm_plan_destroy(hfmm_plan* P) {
     delete[] static_cast<MixedMaps*>(P->cx_maps);
     P->cx_maps = nullptr;
     compressed_release(P);
+    if (P->nf_side) cudaStreamDestroy(P->nf_side);
+    if (P->nf_fork) cudaEventDestroy(P->nf_fork);
+    if (P->nf_join) cudaEventDestroy(P->nf_join);
     delete P;
 }
 

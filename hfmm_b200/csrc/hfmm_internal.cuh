@@ -171,6 +171,8 @@ struct hfmm_plan {
     void* mx_maps = nullptr;                // MixedMaps per level (host array)
     bool compressed = false;                // every level has a compressed M2L (mixed path)
     void* cx_maps = nullptr;                // MixedMaps [2][MAX_LEVELS] of the C_d tables
+    cudaStream_t nf_side = nullptr;         // the near field's stream (runs beside the far field)
+    cudaEvent_t nf_fork = nullptr, nf_join = nullptr;
     static constexpr int CX_STREAMS = 4;    // side streams of the concurrent compressed M2L
     cudaStream_t cx_side[CX_STREAMS] = {};
     cudaEvent_t cx_fork = nullptr, cx_join[CX_STREAMS] = {};
