@@ -195,7 +195,7 @@ struct __align__(8) Ctl {
     uint64_t full[STAGES];
     uint64_t empty[STAGES];
     uint64_t acc_full[2];    // a unit's FP32 sum is complete in buffer b (MMA commit)
-    uint64_t acc_empty[2];   // buffer b has been folded into the FP64 sum (128 arrivals)
+    uint64_t acc_empty[2];   // buffer b has been folded into the FP64 sum (one per fold warp)
     uint64_t done;
     uint32_t tmem;
     int abort_flag;
@@ -228,12 +228,12 @@ __global__ void __launch_bounds__(THREADS, 1) k_m2l_tf32x3(const __grid_constant
     if (tid == 0) {
         ctl.abort_flag = 0;
         for (int s = 0; s < STAGES; ++s) {
-            mbar_init(smem_u32(&ctl.full[s]), 1 + 128);   // TMA arrive + 128 gather threads
+            mbar_init(smem_u32(&ctl.full[s]), 1 + 4);     // TMA arrive + one per gather warp
             mbar_init(smem_u32(&ctl.empty[s]), 1);       // MMA commit
         }
         for (int b = 0; b < 2; ++b) {
             mbar_init(smem_u32(&ctl.acc_full[b]), 1);
-            mbar_init(smem_u32(&ctl.acc_empty[b]), 32 * N_FOLD_WARPS);
+            mbar_init(smem_u32(&ctl.acc_empty[b]), N_FOLD_WARPS);   // one per fold warp
         }
         mbar_init(smem_u32(&ctl.done), 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -324,7 +324,9 @@ __global__ void __launch_bounds__(THREADS, 1) k_m2l_tf32x3(const __grid_constant
                 }
                 if (ai + 1 < n_act) load_sources(ai + 1);
             }
-            if (!mbar_wait(smem_u32(&ctl.empty[st]), ((q / STAGES) & 1) ^ 1, abort_flag)) break;
+            // the warp arrives once per stage (below), so it leaves the loop as one
+            const bool got = mbar_wait(smem_u32(&ctl.empty[st]), ((q / STAGES) & 1) ^ 1, abort_flag);
+            if (!__all_sync(0xffffffffu, got)) break;
             const int k0 = (q % kch) * BK;
             const uint32_t sbh = smem_u32(sm + st * STAGE_BYTES + 2 * TILE_BYTES);
             const uint32_t sbl = sbh + TILE_BYTES;
@@ -337,16 +339,21 @@ __global__ void __launch_bounds__(THREADS, 1) k_m2l_tf32x3(const __grid_constant
             }
             asm volatile("cp.async.commit_group;\n" ::);
             if (pending >= 0) {
+                // each lane's copies of the previous stage have landed: fence them for
+                // the tensor core, then one arrive per warp (128 arrives on one barrier
+                // word serialise)
                 asm volatile("cp.async.wait_group 1;\n" ::);
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                mbar_arrive(smem_u32(&ctl.full[pending % STAGES]));
+                __syncwarp();
+                if (lane == 0) mbar_arrive(smem_u32(&ctl.full[pending % STAGES]));
             }
             pending = q;
         }
         asm volatile("cp.async.wait_all;\n" ::);
         if (pending >= 0) {
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            mbar_arrive(smem_u32(&ctl.full[pending % STAGES]));
+            __syncwarp();
+            if (lane == 0) mbar_arrive(smem_u32(&ctl.full[pending % STAGES]));
         }
     } else if (warp >= 6) {
         // ---------------- fold entries into the FP64 sums; store at the end
@@ -389,7 +396,8 @@ __global__ void __launch_bounds__(THREADS, 1) k_m2l_tf32x3(const __grid_constant
             }
             asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
             asm volatile("tcgen05.fence::before_thread_sync;");
-            mbar_arrive(smem_u32(&ctl.acc_empty[b]));
+            __syncwarp();   // one arrive per fold warp
+            if (lane == 0) mbar_arrive(smem_u32(&ctl.acc_empty[b]));
         }
         const bool aborted = !__all_sync(0xffffffffu, ok && !*abort_flag);
         if (aborted) {
