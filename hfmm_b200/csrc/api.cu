@@ -18,6 +18,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <memory>
 #include <mutex>
 
 namespace hfmm {
@@ -424,52 +425,54 @@ void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double*
         PhaseTimer pt(X, s, 11);
         split_tf32(P->equiv.p, P->e_hi.p, P->e_lo.p, (int64_t)NF * fs, s);
     }
+    std::unique_ptr<PhaseTimer> m2l_timer;
     if (use_cx) {
         // A level's M2L reads only the compressed densities of the upward pass, so the
         // M2Ls of every level and family run at once on the plan's side streams (the
         // coarse levels have a handful of tiles each and would otherwise run alone on
-        // a few SMs); each expands into its own level's check potentials. The downward
-        // chain below starts after the join.
-        PhaseTimer pt(X, s, 4);
+        // a few SMs); each expands into its own level's check potentials. The finest
+        // level takes streams 0 and 1; the coarse levels queue on streams 2 and 3,
+        // coarsest first, so the downward chain below can start on them while the
+        // finest level's M2L still runs: it waits for each level's events in turn.
+        m2l_timer.reset(new PhaseTimer(X, s, 4));   // until the finest level has joined
         HFMM_CUDA(cudaEventRecord(P->cx_fork, s));
         for (int k = 0; k < hfmm_plan::CX_STREAMS; ++k)
             HFMM_CUDA(cudaStreamWaitEvent(P->cx_side[k], P->cx_fork, 0));
-        int slot = 0;
-        for (int l = P->md; l >= 2; --l)   // the largest levels first
-            for (int f = 0; f < NF; ++f) {
-                cudaStream_t ss = P->cx_side[slot++ % hfmm_plan::CX_STREAMS];
-                LevelTables& T = P->tables[f][l];
-                MixedCall mc{};
-                mc.tile_tgt = P->mx_tiles[l][R - 1].tgt.p;
-                mc.ntiles = P->mx_tiles[l][R - 1].ntiles;
-                mc.src_tab = P->m2l_src.p;
-                mc.disp_compact = P->disp_compact.p;
-                mc.Bhi = level_base(T.xc_hi.p, l, T.ckld);
-                mc.Blo = level_base(T.xc_lo.p, l, T.ckld);
-                mc.Lhi = nullptr;
-                mc.Llo = nullptr;
-                mc.out = level_base(T.yc.p, l, T.cmld);
-                mc.src_lo = P->level_lo[l];   // the level's buffers hold its own boxes only
-                mc.src_hi = P->level_hi[l];
-                mc.R = R;
-                mc.ld = T.cmld;
-                mc.ldk = T.ckld;
-                mc.ldm = T.cmld;
-                mc.n_fam = 1;
-                mc.has_l2l = 0;
-                mc.fam_stride = 0;
-                mc.out_fam_stride = 0;
-                mc.nb = P->nb;
-                mc.err = P->d_err.p;
-                m2l_tf32x3(static_cast<MixedMaps*>(P->cx_maps)[f * MAX_LEVELS + l], mc, ss);
-                // expand y = U y' into the check potential (overwrites the upward leftovers)
-                gemm_1(K_EXP, l, f, level_base(T.yc.p, l, T.cmld), T.cmld, P->check.p + f * fs,
-                       P->ld, ss);
-            }
-        for (int k = 0; k < hfmm_plan::CX_STREAMS; ++k) {
+        auto launch = [&](int l, int f, cudaStream_t ss) {
+            LevelTables& T = P->tables[f][l];
+            MixedCall mc{};
+            mc.tile_tgt = P->mx_tiles[l][R - 1].tgt.p;
+            mc.ntiles = P->mx_tiles[l][R - 1].ntiles;
+            mc.src_tab = P->m2l_src.p;
+            mc.disp_compact = P->disp_compact.p;
+            mc.Bhi = level_base(T.xc_hi.p, l, T.ckld);
+            mc.Blo = level_base(T.xc_lo.p, l, T.ckld);
+            mc.Lhi = nullptr;
+            mc.Llo = nullptr;
+            mc.out = level_base(T.yc.p, l, T.cmld);
+            mc.src_lo = P->level_lo[l];   // the level's buffers hold its own boxes only
+            mc.src_hi = P->level_hi[l];
+            mc.R = R;
+            mc.ld = T.cmld;
+            mc.ldk = T.ckld;
+            mc.ldm = T.cmld;
+            mc.n_fam = 1;
+            mc.has_l2l = 0;
+            mc.fam_stride = 0;
+            mc.out_fam_stride = 0;
+            mc.nb = P->nb;
+            mc.err = P->d_err.p;
+            m2l_tf32x3(static_cast<MixedMaps*>(P->cx_maps)[f * MAX_LEVELS + l], mc, ss);
+            // expand y = U y' into the check potential (overwrites the upward leftovers)
+            gemm_1(K_EXP, l, f, level_base(T.yc.p, l, T.cmld), T.cmld, P->check.p + f * fs, P->ld,
+                   ss);
+            HFMM_CUDA(cudaEventRecord(P->cx_level[l][f], ss));
+        };
+        for (int f = 0; f < NF; ++f) launch(P->md, f, P->cx_side[f]);
+        for (int l = 2; l < P->md; ++l)
+            for (int f = 0; f < NF; ++f) launch(l, f, P->cx_side[2 + f]);
+        for (int k = 0; k < hfmm_plan::CX_STREAMS; ++k)   // every side stream rejoins
             HFMM_CUDA(cudaEventRecord(P->cx_join[k], P->cx_side[k]));
-            HFMM_CUDA(cudaStreamWaitEvent(s, P->cx_join[k], 0));
-        }
     }
     // ---- downward pass (M2L + L2L in one GEMM, then X-list P2L, then decode)
     for (int l = 2; l <= P->md; ++l) {
@@ -477,7 +480,13 @@ void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double*
             PhaseTimer pt(X, s, 12);
             generate_m2l_stream(P, l, use_mx, P->ws, s);
         }
-        if (use_cx) {   // M2L done above, concurrently for every level
+        if (use_cx) {   // this level's M2L ran above, on a side stream
+            for (int f = 0; f < NF; ++f) HFMM_CUDA(cudaStreamWaitEvent(s, P->cx_level[l][f], 0));
+            if (l == P->md) {
+                for (int k = 0; k < hfmm_plan::CX_STREAMS; ++k)
+                    HFMM_CUDA(cudaStreamWaitEvent(s, P->cx_join[k], 0));
+                m2l_timer.reset();
+            }
             if (l >= 3)   // L2L (phases.py:273-278) in FP64, added to the check potential
                 gemm(K_L2L, l, P->dn_tiles[l][R - 1], P->m2l_src.p + N_DISP, M2L_ENTRIES, P->loc.p,
                      nullptr, P->check.p, nullptr);

@@ -86,6 +86,9 @@ void compressed_prepare(hfmm_plan* P) {
             HFMM_CUDA(cudaStreamCreateWithFlags(&P->cx_side[k], cudaStreamNonBlocking));
             HFMM_CUDA(cudaEventCreateWithFlags(&P->cx_join[k], cudaEventDisableTiming));
         }
+        for (int l = 0; l < MAX_LEVELS; ++l)
+            for (int f = 0; f < 2; ++f)
+                HFMM_CUDA(cudaEventCreateWithFlags(&P->cx_level[l][f], cudaEventDisableTiming));
     }
     P->compressed = true;
 }
@@ -99,6 +102,11 @@ void compressed_release(hfmm_plan* P) {
         P->cx_join[k] = nullptr;
     }
     P->cx_fork = nullptr;
+    for (int l = 0; l < MAX_LEVELS; ++l)
+        for (int f = 0; f < 2; ++f) {
+            if (P->cx_level[l][f]) cudaEventDestroy(P->cx_level[l][f]);
+            P->cx_level[l][f] = nullptr;
+        }
 }
 
 }  // namespace hfmm

@@ -176,6 +176,7 @@ struct hfmm_plan {
     static constexpr int CX_STREAMS = 4;    // side streams of the concurrent compressed M2L
     cudaStream_t cx_side[CX_STREAMS] = {};
     cudaEvent_t cx_fork = nullptr, cx_join[CX_STREAMS] = {};
+    cudaEvent_t cx_level[hfmm::MAX_LEVELS][2] = {};   // a level's M2L + expansion is done
     bool mixed_ready = false;
     // streamed M2L tables: regenerated per level and evaluate into a workspace
     // (the plan's own, or one bound by the caller and shared by plans that run in turn)
