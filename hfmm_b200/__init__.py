@@ -71,7 +71,7 @@ class HFMMState:
         return self._h
 
     def _pinned(self, name, shape, dtype):
-        """A reused page-locked host buffer for NumPy inputs and outputs."""
+        """A reused page-locked host buffer (the staging of NumPy charges)."""
         t = self._pin.get(name)
         if t is None or tuple(t.shape) != tuple(shape) or t.dtype != dtype:
             t = torch.empty(tuple(shape), dtype=dtype, pin_memory=True)
@@ -243,6 +243,32 @@ def check_errors(state, stream=None):
     _check(_lib.lib.hfmm_plan_check(state.handle, s.cuda_stream))
 
 
+def _stage_charges(owner, q, is_cplx, dev):
+    """NumPy charges -> device tensor, through the owner's reused page-locked buffer
+    (pageable copies run far slower); the host copy into it is torch's threaded one
+    where the array allows. The owner's previous call has synchronised, so the
+    buffer is free."""
+    dt = torch.complex128 if is_cplx else torch.float64
+    qp = owner._pinned("q", q.shape, dt)
+    if q.dtype == (np.complex128 if is_cplx else np.float64) and q.flags.c_contiguous \
+            and q.flags.writeable:
+        qp.copy_(torch.from_numpy(q))
+    else:
+        qp.numpy()[...] = q
+    return qp.to(dev, non_blocking=True)
+
+
+def _to_host(t):
+    """Start the copy of device tensor ``t`` into a new page-locked host tensor from
+    torch's caching host allocator; ``.numpy()`` of it, after a synchronise, is the
+    result handed to the caller. No host-side copy and no page faults on fresh
+    memory: the array keeps its block, which goes back to the cache (and to a later
+    call) only when the caller drops the array."""
+    h = torch.empty(tuple(t.shape), dtype=t.dtype, pin_memory=True)
+    h.copy_(t, non_blocking=True)
+    return h
+
+
 def _run(state, charges, complex_ok, field, precision):
     numpy_in = not isinstance(charges, torch.Tensor)
     if numpy_in:
@@ -255,10 +281,8 @@ def _run(state, charges, complex_ok, field, precision):
         raise ValueError("charges must be a real array of shape (N,)")
     dev = state.device
     with torch.cuda.device(dev):
-        if numpy_in:          # through pinned staging: pageable copies run far slower
-            qp = state._pinned("q", q.shape, torch.complex128 if is_cplx else torch.float64)
-            qp.numpy()[...] = q
-            q = qp.to(dev, non_blocking=True)
+        if numpy_in:
+            q = _stage_charges(state, q, is_cplx, dev)
         else:
             q = q.detach().to(dev)
         if is_cplx:
@@ -272,14 +296,11 @@ def _run(state, charges, complex_ok, field, precision):
         evaluate_into(state, q_re, q_im, phi, E, precision)
         check_errors(state)
         if numpy_in:
-            php = state._pinned("phi", phi.shape, phi.dtype)
-            php.copy_(phi, non_blocking=True)
-            if E is not None:
-                Ep = state._pinned("E", E.shape, E.dtype)
-                Ep.copy_(E, non_blocking=True)
+            php = _to_host(phi)
+            Ep = _to_host(E) if E is not None else None
             torch.cuda.current_stream(dev).synchronize()
-            phi = php.numpy().copy()
-            E = Ep.numpy().copy() if E is not None else None
+            phi = php.numpy()
+            E = Ep.numpy() if E is not None else None
     return (phi, E) if field else phi
 
 

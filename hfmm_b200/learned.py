@@ -325,18 +325,15 @@ class AutoPlan:
 
         The error checked is the relative L2 error over the check targets of the
         potential, and of the field when it is computed (the larger of the two)."""
-        from . import evaluate_into, check_errors, PREC_FP64
+        from . import evaluate_into, check_errors, PREC_FP64, _stage_charges, _to_host
         numpy_in = not isinstance(charges, torch.Tensor)
         dev = self.device
         with torch.cuda.device(dev):
-            if numpy_in:      # through pinned staging: pageable copies run far slower
+            if numpy_in:
                 qn = np.asarray(charges)
                 if qn.shape != (self.state.n,):
                     raise ValueError(f"charges must have shape ({self.state.n},)")
-                qp = self._pinned("q", qn.shape, torch.complex128 if np.iscomplexobj(qn)
-                                  else torch.float64)
-                qp.numpy()[...] = qn
-                q = qp.to(dev, non_blocking=True)
+                q = _stage_charges(self, qn, np.iscomplexobj(qn), dev)
             else:
                 q = charges.to(dev)
             if q.is_complex():
@@ -363,17 +360,14 @@ class AutoPlan:
             rep["certified"] = bool(err <= self.tol)
             self.report = rep
         if numpy_in:
-            php = self._pinned("phi", phi.shape, phi.dtype)
-            php.copy_(phi, non_blocking=True)
-            if E is not None:
-                Ep = self._pinned("E", E.shape, E.dtype)
-                Ep.copy_(E, non_blocking=True)
+            php = _to_host(phi)
+            Ep = _to_host(E) if E is not None else None
             torch.cuda.current_stream(dev).synchronize()
-            return php.numpy().copy(), (Ep.numpy().copy() if E is not None else None)
+            return php.numpy(), (Ep.numpy() if E is not None else None)
         return phi, E
 
     def _pinned(self, name, shape, dtype):
-        """A reused page-locked host buffer (one per role, shape and dtype)."""
+        """A reused page-locked host buffer (the staging of NumPy charges)."""
         t = self._pin.get(name)
         if t is None or tuple(t.shape) != tuple(shape) or t.dtype != dtype:
             t = torch.empty(tuple(shape), dtype=dtype, pin_memory=True)
