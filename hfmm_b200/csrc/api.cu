@@ -103,8 +103,8 @@ std::vector<int32_t> nonadjacent_map() {
 // A-pointer sets of the GEMM calls: kind 0..3 decode (up U, up Vt, dn U, dn Vt),
 // kind 4 M2M (8 entries), kind 5 downward M2L+L2L (351 entries), kind 6 L2L alone,
 // kinds 7/8 compress / expand of the compressed M2L; per level, families adjacent.
-enum { K_UPU, K_UPV, K_DNU, K_DNV, K_M2M, K_DN, K_L2L, K_CMP, K_EXP, K_COUNT };
-const int k_entries[K_COUNT] = {1, 1, 1, 1, 8, M2L_ENTRIES, 8, 1, 1};
+enum { K_UPU, K_UPV, K_DNU, K_DNV, K_M2M, K_DN, K_L2L, K_CMP, K_EXP, K_M2MF, K_L2LF, K_COUNT };
+const int k_entries[K_COUNT] = {1, 1, 1, 1, 8, M2L_ENTRIES, 8, 1, 1, 8, 8};
 
 struct PtrIndex {
     size_t off[K_COUNT][MAX_LEVELS];
@@ -141,8 +141,14 @@ void build_a_ptrs(hfmm_plan* P, PtrIndex& ix) {
                     case K_L2L:
                         for (int o = 0; o < 8; ++o) h.push_back(T.l2l.p ? T.l2l.p + o * mat : nullptr);
                         break;
-                    case K_CMP: h.push_back(T.c_cmp.p); break;
-                    case K_EXP: h.push_back(T.c_exp.p); break;
+                    case K_CMP: h.push_back(T.cmp_f.p); break;   // folded (compress.cu)
+                    case K_EXP: h.push_back(T.exp_f.p); break;
+                    case K_M2MF:
+                        for (int o = 0; o < 8; ++o) h.push_back(T.m2m_f.p ? T.m2m_f.p + o * mat : nullptr);
+                        break;
+                    case K_L2LF:
+                        for (int o = 0; o < 8; ++o) h.push_back(T.l2l_f.p ? T.l2l_f.p + o * mat : nullptr);
+                        break;
                 }
             }
         }
@@ -309,10 +315,18 @@ void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double*
     }
     HFMM_CUDA(cudaEventRecord(P->nf_join, P->nf_side));
 
+    // scale_up / scale_dn: multiply row m of family f's result by the level's decode
+    // scale d (the folded low-rank plan's GEMMs end in scaled SVD coordinates)
+    enum { NO_SCALE, SCALE_UP, SCALE_DN };
     auto gemm = [&](int kind, int l, const hfmm_plan::Tiles& tiles, const int32_t* src_tab,
                     int src_ld, const double* B0, const double* B1, double* out,
-                    const double* scale_set) {
-        PhaseTimer pt(X, s, kind == K_M2M ? 2 : kind == K_DN ? 4 : kind == K_L2L ? 13 : (kind <= K_UPV ? 3 : 6));
+                    int scale_kind = NO_SCALE, int accumulate = -1) {
+        const int phase = (kind == K_M2M || kind == K_M2MF) ? 2
+                          : kind == K_DN                    ? 4
+                          : (kind == K_L2L || kind == K_L2LF) ? 13
+                          : kind <= K_UPV                   ? 3
+                                                            : 6;
+        PhaseTimer pt(X, s, phase);
         GemmCall c{};
         c.tile_tgt = tiles.tgt.p;
         c.ntiles = tiles.ntiles;
@@ -320,12 +334,18 @@ void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double*
         c.src_ld = src_ld;
         c.n_entries = k_entries[kind];
         c.b_split = kind == K_DN ? N_DISP : c.n_entries;
-        c.accumulate = kind == K_L2L ? 1 : 0;
+        c.accumulate = accumulate >= 0 ? accumulate : (kind == K_L2L ? 1 : 0);
         c.A = P->a_ptrs.p + X->ix.off[kind][l];
         c.B0 = B0;
         c.B1 = B1;
         c.out = out;
-        c.scale = scale_set;
+        if (scale_kind != NO_SCALE) {
+            auto pick = [&](int f) {
+                return scale_kind == SCALE_UP ? P->tables[f][l].up_d.p : P->tables[f][l].dn_d.p;
+            };
+            c.scale = pick(0);
+            c.scale_f1 = NF > 1 ? pick(1) : nullptr;
+        }
         c.R = R;
         c.ld = P->ld;
         c.n_s = P->n_s;
@@ -362,7 +382,7 @@ void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double*
             c.nb = P->nb;
             gemm_f64(c, P->d_err.p, s);
         }
-        gemm(up ? K_UPV : K_DNV, l, tiles, nullptr, 0, P->tmp.p, nullptr, out, nullptr);
+        gemm(up ? K_UPV : K_DNV, l, tiles, nullptr, 0, P->tmp.p, nullptr, out);
     };
 
     // ---- upward pass
@@ -376,14 +396,28 @@ void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double*
         PhaseTimer pt(X, s, 1);
         particles(p, s);
     }
-    for (int l = P->md; l >= 2; --l) {
-        if (l < P->md)
-            gemm(K_M2M, l, P->m2m_tiles[l][R - 1], P->m2m_src.p, 8, P->equiv.p, nullptr,
-                 P->check.p, nullptr);
-        decode(l, true, P->check.p, P->equiv.p);
-    }
     const bool use_mx = mixed && P->mixed_ready;
     const bool use_cx = use_mx && P->compressed;
+    if (use_cx) {
+        // folded tables (compress.cu): P->equiv holds y = d .* (U^T x) per box, from the
+        // leaf check potentials (U, leaves) or the children's y (folded M2M, the rest)
+        for (int l = P->md; l >= 2; --l) {
+            gemm(K_UPU, l, P->leaf_tiles[l][R - 1], nullptr, 0, P->check.p, nullptr, P->equiv.p,
+                 SCALE_UP);
+            if (l < P->md)
+                gemm(K_M2MF, l, P->m2m_tiles[l][R - 1], P->m2m_src.p, 8, P->equiv.p, nullptr,
+                     P->equiv.p, SCALE_UP);
+            if (P->nW)   // the W list's M2P reads the equivalent densities themselves
+                gemm(K_UPV, l, P->dec_tiles[l][R - 1], nullptr, 0, P->equiv.p, nullptr, P->tmp.p);
+        }
+    } else {
+        for (int l = P->md; l >= 2; --l) {
+            if (l < P->md)
+                gemm(K_M2M, l, P->m2m_tiles[l][R - 1], P->m2m_src.p, 8, P->equiv.p, nullptr,
+                     P->check.p);
+            decode(l, true, P->check.p, P->equiv.p);
+        }
+    }
     // A level's compressed buffers hold [box - level_lo][R][cld]; the GEMMs index boxes
     // absolutely, so they get the buffer's address shifted back by level_lo rows.
     auto level_base = [&](auto* buf, int l, int cld) {
@@ -391,8 +425,9 @@ void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double*
     };
     // one-entry GEMM over every box of level l between layouts of different widths
     auto gemm_1 = [&](int kind, int l, int f, const double* in, int ldk, double* out, int ldm,
-                      cudaStream_t st) {
+                      cudaStream_t st, const double* scale = nullptr) {
         GemmCall c{};
+        c.scale = scale;
         c.tile_tgt = P->dec_tiles[l][R - 1].tgt.p;
         c.ntiles = P->dec_tiles[l][R - 1].ntiles;
         c.src_tab = nullptr;
@@ -411,7 +446,7 @@ void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double*
         c.nb = P->nb;
         gemm_f64(c, P->d_err.p, st);
     };
-    if (use_cx) {   // compress every level's densities (x' = U^T x), then split them
+    if (use_cx) {   // compress every level's densities (x' = y Vt_up U_c), then split them
         PhaseTimer pt(X, s, 14);
         for (int l = 2; l <= P->md; ++l)
             for (int f = 0; f < NF; ++f) {
@@ -463,9 +498,10 @@ void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double*
             mc.nb = P->nb;
             mc.err = P->d_err.p;
             m2l_tf32x3(static_cast<MixedMaps*>(P->cx_maps)[f * MAX_LEVELS + l], mc, ss);
-            // expand y = U y' into the check potential (overwrites the upward leftovers)
-            gemm_1(K_EXP, l, f, level_base(T.yc.p, l, T.cmld), T.cmld, P->check.p + f * fs, P->ld,
-                   ss);
+            // expand into the level's downward coordinates: y_dn = d_dn .* (y' U_c^T U_dn)
+            // (overwrites; the L2L and X list add to it on the main stream)
+            gemm_1(K_EXP, l, f, level_base(T.yc.p, l, T.cmld), T.cmld, P->loc.p + f * fs, P->ld,
+                   ss, T.dn_d.p);
             HFMM_CUDA(cudaEventRecord(P->cx_level[l][f], ss));
         };
         for (int f = 0; f < NF; ++f) launch(P->md, f, P->cx_side[f]);
@@ -487,9 +523,9 @@ void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double*
                     HFMM_CUDA(cudaStreamWaitEvent(s, P->cx_join[k], 0));
                 m2l_timer.reset();
             }
-            if (l >= 3)   // L2L (phases.py:273-278) in FP64, added to the check potential
-                gemm(K_L2L, l, P->dn_tiles[l][R - 1], P->m2l_src.p + N_DISP, M2L_ENTRIES, P->loc.p,
-                     nullptr, P->check.p, nullptr);
+            if (l >= 3)   // folded L2L (phases.py:273-278): y_dn += d_dn .* (y_dn(parent) F_o)
+                gemm(K_L2LF, l, P->dn_tiles[l][R - 1], P->m2l_src.p + N_DISP, M2L_ENTRIES,
+                     P->loc.p, nullptr, P->loc.p, SCALE_DN, 1);
         } else if (use_mx) {
             MixedCall mc{};
             mc.tile_tgt = P->mx_tiles[l][R - 1].tgt.p;
@@ -515,12 +551,17 @@ void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double*
             }
             if (l >= 3)   // L2L (phases.py:273-278) in FP64, added to the check potential
                 gemm(K_L2L, l, P->dn_tiles[l][R - 1], P->m2l_src.p + N_DISP, M2L_ENTRIES, P->loc.p,
-                     nullptr, P->check.p, nullptr);
+                     nullptr, P->check.p);
         } else {
             gemm(K_DN, l, P->dn_tiles[l][R - 1], P->m2l_src.p, M2L_ENTRIES, P->equiv.p, P->loc.p,
-                 P->check.p, nullptr);
+                 P->check.p);
         }
         if (P->nX) {
+            if (use_cx)   // the X list's check potentials alone, decoded into y_dn below
+                for (int f = 0; f < NF; ++f)
+                    HFMM_CUDA(cudaMemsetAsync(
+                        P->check.p + f * fs + (int64_t)P->level_lo[l] * R * P->ld, 0,
+                        (size_t)(P->level_hi[l] - P->level_lo[l]) * R * P->ld * sizeof(double), s));
             ParticlePass p = base;
             p.op = ParticleOp::P2L;
             p.rows = P->x_tgt.p;
@@ -530,10 +571,18 @@ void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double*
             p.surf = P->equiv_pts.p;
             p.out = P->check.p;
             p.level = l;
-            PhaseTimer pt(X, s, 5);
-            particles(p, s);
+            {
+                PhaseTimer pt(X, s, 5);
+                particles(p, s);
+            }
+            if (use_cx)
+                gemm(K_DNU, l, P->dec_tiles[l][R - 1], nullptr, 0, P->check.p, nullptr, P->loc.p,
+                     SCALE_DN, 1);
         }
-        decode(l, false, P->check.p, P->loc.p);
+        if (use_cx)   // leaves leave the coordinates: local densities for L2P, into P->check
+            gemm(K_DNV, l, P->leaf_tiles[l][R - 1], nullptr, 0, P->loc.p, nullptr, P->check.p);
+        else
+            decode(l, false, P->check.p, P->loc.p);
     }
     // ---- particle outputs: the near field (above) stores, far field and W list add
     HFMM_CUDA(cudaStreamWaitEvent(s, P->nf_join, 0));
@@ -543,7 +592,7 @@ void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double*
         p.rows = P->leaves.p;
         p.nrows = P->n_leaves;
         p.surf = P->check_pts.p;
-        p.dens = P->loc.p;
+        p.dens = use_cx ? P->check.p : P->loc.p;
         {
             PhaseTimer pt(X, s, 8);
             particles(p, s);
@@ -556,7 +605,7 @@ void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double*
             p.off = P->w_off.p;
             p.srcs = P->w_src.p;
             p.surf = P->equiv_pts.p;
-            p.dens = P->equiv.p;
+            p.dens = use_cx ? P->tmp.p : P->equiv.p;
             PhaseTimer pt(X, s, 9);
             particles(p, s);
         }
@@ -770,6 +819,10 @@ int hfmm_plan_finalize(hfmm_plan* P) {
         lists_build(P);
         schedules_build(P);
     }
+    // mixed path: the low-rank M2L's buffers and folded tables (compress.cu), before the
+    // A pointer table that points at them
+    P->mixed_ready = false;
+    compressed_prepare(P);
     PlanExtra* X = extra(P, true);
     build_a_ptrs(P, X->ix);   // streamed plans without a workspace yet: see evaluate
     if (!P->nf_side) {
@@ -788,8 +841,6 @@ int hfmm_plan_finalize(hfmm_plan* P) {
     P->tmp.zero();
     // mixed path: TF32 hi/lo tables, tensor maps, split density buffers (needs ld >= 128);
     // with a compressed M2L on every level the dense TF32 tables are not needed
-    P->mixed_ready = false;
-    compressed_prepare(P);
     if (P->ld >= 128) {
         std::vector<int32_t> dc(N_DISP, -1);
         auto madj = nonadjacent_map();

@@ -54,6 +54,70 @@ __global__ void k_pack_c(const double* __restrict__ C, int r, int ckld, int cmld
     lo[o] = tf32_round((float)(v - (double)h));
 }
 
+// C = A B for row-major FP64 matrices, batched over blockIdx.z with element strides
+// (0: the operand is shared). Setup only: it builds the folded tables.
+__global__ void k_matmul(const double* __restrict__ A, int lda, int64_t sa,
+                         const double* __restrict__ B, int ldb, int64_t sb, double* C, int ldc,
+                         int64_t scs, int M, int N, int K) {
+    __shared__ double As[16][17], Bs[16][17];
+    const int z = blockIdx.z;
+    A += z * sa;
+    B += z * sb;
+    C += z * scs;
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int row = blockIdx.y * 16 + ty, col = blockIdx.x * 16 + tx;
+    double acc = 0.0;
+    for (int k0 = 0; k0 < K; k0 += 16) {
+        As[ty][tx] = (row < M && k0 + tx < K) ? A[(int64_t)row * lda + k0 + tx] : 0.0;
+        Bs[ty][tx] = (k0 + ty < K && col < N) ? B[(int64_t)(k0 + ty) * ldb + col] : 0.0;
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < 16; ++kk) acc = fma(As[ty][kk], Bs[kk][tx], acc);
+        __syncthreads();
+    }
+    if (row < M && col < N) C[(int64_t)row * ldc + col] = acc;
+}
+
+void matmul(const double* A, int lda, int64_t sa, const double* B, int ldb, int64_t sb, double* C,
+            int ldc, int64_t scs, int M, int N, int K, int batch) {
+    const dim3 grid((unsigned)ceil_div(N, 16), (unsigned)ceil_div(M, 16), (unsigned)batch);
+    HFMM_LAUNCH(k_matmul, grid, dim3(16, 16), 0, 0, A, lda, sa, B, ldb, sb, C, ldc, scs, M, N, K);
+}
+
+// The folded tables of one level and family. Every operator is kept as the row-major
+// right multiplier of a box's row vector (the A^T layout the GEMMs read), so
+//   y(parent) = d_up .* sum_o y(child_o) [Vt_up(l+1) M2M_o^T U_up(l)]
+//   x'        = y Vt_up(l) U_c
+//   y_dn      = d_dn .* (y' U_c^T U_dn(l) + y_dn(parent) [Vt_dn(l-1) L2L_o^T U_dn(l)])
+// and only leaves leave the coordinates: U_up after P2M, Vt_dn before L2P. The scale d
+// is never multiplied into a table: the decodes' rounding then stays along the
+// directions their small singular values damp, as in the two-step decode.
+void fold_level(hfmm_plan* P, int f, int l, DevBuf<double>& tmp) {
+    LevelTables& T = P->tables[f][l];
+    const int ld = P->ld;
+    const int64_t mat = (int64_t)ld * ld;
+    if (l < P->md) {
+        const LevelTables& C = P->tables[f][l + 1];
+        T.m2m_f.alloc(8 * (size_t)mat);
+        matmul(C.up_Vt.p, ld, 0, T.m2m.p, ld, mat, tmp.p, ld, mat, ld, ld, ld, 8);
+        matmul(tmp.p, ld, mat, T.up_U.p, ld, 0, T.m2m_f.p, ld, mat, ld, ld, ld, 8);
+    } else {
+        T.m2m_f.release();
+    }
+    if (l >= 3) {
+        const LevelTables& Pa = P->tables[f][l - 1];
+        T.l2l_f.alloc(8 * (size_t)mat);
+        matmul(Pa.dn_Vt.p, ld, 0, T.l2l.p, ld, mat, tmp.p, ld, mat, ld, ld, ld, 8);
+        matmul(tmp.p, ld, mat, T.dn_U.p, ld, 0, T.l2l_f.p, ld, mat, ld, ld, ld, 8);
+    } else {
+        T.l2l_f.release();
+    }
+    T.cmp_f.alloc((size_t)ld * T.ckld);
+    matmul(T.up_Vt.p, ld, 0, T.c_cmp.p, T.ckld, 0, T.cmp_f.p, T.ckld, 0, ld, T.ckld, ld, 1);
+    T.exp_f.alloc((size_t)T.cmld * ld);
+    matmul(T.c_exp.p, ld, 0, T.dn_U.p, ld, 0, T.exp_f.p, ld, 0, T.cmld, ld, ld, 1);
+}
+
 }  // namespace
 
 void compressed_prepare(hfmm_plan* P) {
@@ -80,6 +144,13 @@ void compressed_prepare(hfmm_plan* P) {
             make_table_map(&maps[f * MAX_LEVELS + l].a_hi[0], T.c_hi.p, T.ckld, N_M2L, T.cmld);
             make_table_map(&maps[f * MAX_LEVELS + l].a_lo[0], T.c_lo.p, T.ckld, N_M2L, T.cmld);
         }
+    {
+        DevBuf<double> tmp;
+        tmp.alloc(8 * (size_t)P->ld * P->ld);
+        for (int f = 0; f < P->n_fam; ++f)
+            for (int l = 2; l <= P->md; ++l) fold_level(P, f, l, tmp);
+        HFMM_CUDA(cudaDeviceSynchronize());   // tmp is freed on return
+    }
     if (!P->cx_fork) {   // side streams and fork/join events of the concurrent M2L
         HFMM_CUDA(cudaEventCreateWithFlags(&P->cx_fork, cudaEventDisableTiming));
         for (int k = 0; k < hfmm_plan::CX_STREAMS; ++k) {

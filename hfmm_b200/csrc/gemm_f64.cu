@@ -186,6 +186,7 @@ __global__ void __launch_bounds__(128) k_gemm_f64(GemmCall c, int* err) {
             sm.u.C[n + 1][m + 8] = acc[mi][ni][3];
         }
     __syncthreads();
+    const double* sc = (fam == 1 && c.scale_f1) ? c.scale_f1 : c.scale;
     for (int idx = tid; idx < TN * (TM / 2); idx += 128) {
         int col = idx / (TM / 2), mm = (idx % (TM / 2)) * 2;
         int j = col / R, r = col % R;
@@ -193,9 +194,9 @@ __global__ void __launch_bounds__(128) k_gemm_f64(GemmCall c, int* err) {
         int m = m0 + mm;
         if (t < 0 || m >= c.ldm) continue;
         double v0 = sm.u.C[col][mm], v1 = sm.u.C[col][mm + 1];
-        if (c.scale) {
-            v0 *= c.scale[m];
-            v1 *= c.scale[m + 1];
+        if (sc) {
+            v0 *= sc[m];
+            v1 *= sc[m + 1];
         }
         double2* o = reinterpret_cast<double2*>(out + ((int64_t)t * R + r) * c.ldm + m);
         if (c.accumulate) {

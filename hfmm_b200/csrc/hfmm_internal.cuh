@@ -92,6 +92,12 @@ struct LevelTables {
     DevBuf<float> c_hi, c_lo;      // C_d halves as A [316][cmld][ckld]
     DevBuf<double> xc, yc;         // the level's compressed densities [.][R][ckld] and
     DevBuf<float> xc_hi, xc_lo;    // check potentials [.][R][cmld] (box - level_lo first)
+    // the low-rank plan's folded tables (row-major right multipliers, zero padded):
+    // the decodes' Vt and U taken into the operators next to them, so a box keeps its
+    // densities as scaled SVD coordinates (d .* (U^T x)) through both passes
+    DevBuf<double> m2m_f;          // 8 x Vt_up(l+1) M2M^T U_up(l), this level as PARENT
+    DevBuf<double> l2l_f;          // 8 x Vt_dn(l-1) L2L^T U_dn(l), this level as CHILD
+    DevBuf<double> cmp_f, exp_f;   // Vt_up(l) c_cmp (ld x ckld); c_exp U_dn(l) (cmld x ld)
     bool set = false;
     void reset() {
         up_U.release(); up_d.release(); up_Vt.release();
@@ -101,6 +107,7 @@ struct LevelTables {
         cr = ckld = cmld = 0;
         c_cmp.release(); c_exp.release(); c_hi.release(); c_lo.release();
         xc.release(); yc.release(); xc_hi.release(); xc_lo.release();
+        m2m_f.release(); l2l_f.release(); cmp_f.release(); exp_f.release();
         set = false;
     }
 };
@@ -165,6 +172,7 @@ struct hfmm_plan {
     Tiles m2m_tiles[hfmm::MAX_LEVELS][2];   // [level][R-1]
     Tiles dn_tiles[hfmm::MAX_LEVELS][2];
     Tiles dec_tiles[hfmm::MAX_LEVELS][2];
+    Tiles leaf_tiles[hfmm::MAX_LEVELS][2];  // the level's leaves only
     Tiles mx_tiles[hfmm::MAX_LEVELS][2];    // mixed M2L tiles: 128 / R targets, by octant
     hfmm::DevBuf<int32_t> disp_compact;     // 343 -> M2L table index or -1
     hfmm::DevBuf<float> e_hi, e_lo, l_hi, l_lo;   // split densities [fam][box][R][ld]
@@ -233,6 +241,7 @@ struct GemmCall {
     const double* B1;
     double* out;
     const double* scale;       // nullable, length ld
+    const double* scale_f1;    // family 1's scale when it differs (nullable: scale)
     int accumulate;            // 1: out += result, 0: out = result
     int R;
     int ld;                    // padded n_s (multiple of 16)

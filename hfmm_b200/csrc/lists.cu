@@ -448,13 +448,14 @@ void schedules_build(hfmm_plan* P) {
                 T.ntiles = (int)(t.size() / TT);
                 upload(T.tgt, t);
             };
-            std::vector<int32_t> all, nonleaf;
+            std::vector<int32_t> all, nonleaf, leaf;
             for (int b = lo; b < hi; ++b) {
                 all.push_back(b);
-                if (!P->h_is_leaf[b]) nonleaf.push_back(b);
+                (P->h_is_leaf[b] ? leaf : nonleaf).push_back(b);
             }
             make(all, P->dec_tiles[l][r]);
             make(nonleaf, P->m2m_tiles[l][r]);
+            make(leaf, P->leaf_tiles[l][r]);
             // downward tiles: grouped by octant so the 189 active displacements and
             // the L2L matrix coincide within a tile
             std::vector<int32_t> byoct;

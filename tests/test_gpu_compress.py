@@ -1,6 +1,7 @@
 """The compressed M2L of the mixed path (K_d ~ U C_d U^T per level, U from the
-level's M2L Gram matrix): close to the dense mixed M2L, within tolerance of the
-FP64 direct sum, and without effect on the FP64 evaluate."""
+level's M2L Gram matrix, with the decodes folded into the neighbouring operators):
+close to the dense mixed M2L, within tolerance of the FP64 direct sum, and without
+effect on the FP64 evaluate."""
 import numpy as np
 import pytest
 import torch
@@ -34,6 +35,8 @@ def test_compressed_mixed_m2l_matches_dense(clustered):
     assert all(1 <= r <= comp.info["n_s"] for r in ranks.values())
     md = comp.max_depth
     assert all(ranks[(1, l)] < ranks[(0, l)] for l in range(2, md + 1))   # sin is smoother
+    if clustered:   # the folded tables' W (M2P) and X (P2L) branches run
+        assert comp.info["n_w"] > 0 and comp.info["n_x"] > 0
     pd, ed = hf.evaluate_field(dense, q, hf.PREC_MIXED)
     pc, ec = hf.evaluate_field(comp, q, hf.PREC_MIXED)
     assert _rel(pc, pd) < 3e-7 and _rel(ec, ed) < 3e-7
