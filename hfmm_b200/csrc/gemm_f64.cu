@@ -56,6 +56,7 @@ struct __align__(16) Smem {
     } u;
     int tgt[TN];
     short act[MAX_ENTRIES];
+    unsigned char used[MAX_ENTRIES];   // entry has a source for some target of the tile
     int n_act;
 };
 
@@ -79,21 +80,35 @@ __global__ void __launch_bounds__(128) k_gemm_f64(GemmCall c, int* err) {
         sm.tgt[tid] = t;
     }
     if (tid == 0) sm.n_act = 0;
+    for (int e = tid; e < c.n_entries; e += 128) sm.used[e] = c.src_tab ? 0 : 1;
     __syncthreads();
-    // active entries: A present and at least one target of the tile has a source
+    // active entries: A present and at least one target of the tile has a source. Every
+    // thread tests (target, entry) pairs, the loads of a batch independent of each other
+    if (c.src_tab) {
+        constexpr int BATCH = 8;
+        const int pairs = TT * c.n_entries;
+        for (int i0 = tid; i0 < pairs; i0 += 128 * BATCH) {
+            int src[BATCH];
+#pragma unroll
+            for (int u = 0; u < BATCH; ++u) {
+                const int i = i0 + u * 128;
+                src[u] = -1;
+                if (i < pairs) {
+                    const int t = sm.tgt[i / c.n_entries];
+                    if (t >= 0) src[u] = __ldg(c.src_tab + (int64_t)t * c.src_ld + i % c.n_entries);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < BATCH; ++u)
+                if (src[u] >= 0) sm.used[(i0 + u * 128) % c.n_entries] = 1;
+        }
+        __syncthreads();
+    }
     if (warp == 0) {
         int base = 0;
         for (int e0 = 0; e0 < c.n_entries; e0 += 32) {
             int e = e0 + lane;
-            bool act = false;
-            if (e < c.n_entries && A[e] != nullptr) {
-                if (!c.src_tab) act = true;
-                else
-                    for (int j = 0; j < TT && !act; ++j) {
-                        int t = sm.tgt[j];
-                        if (t >= 0 && c.src_tab[(int64_t)t * c.src_ld + e] >= 0) act = true;
-                    }
-            }
+            const bool act = e < c.n_entries && A[e] != nullptr && sm.used[e];
             unsigned bal = __ballot_sync(0xffffffffu, act);
             if (act) sm.act[base + __popc(bal & ((1u << lane) - 1))] = (short)e;
             base += __popc(bal);

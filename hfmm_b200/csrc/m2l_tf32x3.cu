@@ -203,6 +203,7 @@ struct __align__(8) Ctl {
     int tgt[BN];
     short act[M2L_ENTRIES + 1];
     short zidx[M2L_ENTRIES + 1];   // A-table index of each active entry (M2L or L2L table)
+    unsigned char used[M2L_ENTRIES + 1];   // entry has a source for some target of the tile
 };
 
 template <int R>
@@ -225,6 +226,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_m2l_tf32x3(const __grid_constant
         }
         ctl.tgt[tid] = t;
     }
+    for (int e = tid; e < M2L_ENTRIES; e += THREADS) ctl.used[e] = 0;
     if (tid == 0) {
         ctl.abort_flag = 0;
         for (int s = 0; s < STAGES; ++s) {
@@ -247,18 +249,35 @@ __global__ void __launch_bounds__(THREADS, 1) k_m2l_tf32x3(const __grid_constant
     asm volatile("tcgen05.fence::before_thread_sync;");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;");
-    // active entries (ballot compaction by warp 0)
+    // active entries: every thread tests (target, entry) pairs, entries fastest (the
+    // source table's rows are read coalesced) and the loads of a batch independent of
+    // each other; warp 0 then compacts the flags with ballots
+    {
+        constexpr int BATCH = 8;
+        constexpr int PAIRS = TT * M2L_ENTRIES;
+        for (int i0 = tid; i0 < PAIRS; i0 += THREADS * BATCH) {
+            int src[BATCH];
+#pragma unroll
+            for (int u = 0; u < BATCH; ++u) {
+                const int i = i0 + u * THREADS;
+                src[u] = -1;
+                if (i < PAIRS) {
+                    const int t = ctl.tgt[i / M2L_ENTRIES];
+                    if (t >= 0) src[u] = __ldg(c.src_tab + (int64_t)t * M2L_ENTRIES + i % M2L_ENTRIES);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < BATCH; ++u)
+                if (src[u] >= 0) ctl.used[(i0 + u * THREADS) % M2L_ENTRIES] = 1;
+        }
+    }
+    __syncthreads();
     if (warp == 0) {
         int base = 0;
         for (int e0 = 0; e0 < M2L_ENTRIES; e0 += 32) {
             int e = e0 + lane;
-            bool act = false;
-            if (e < M2L_ENTRIES && (e < N_DISP ? c.disp_compact[e] >= 0 : c.has_l2l != 0)) {
-                for (int j = 0; j < TT && !act; ++j) {
-                    int t = ctl.tgt[j];
-                    if (t >= 0 && c.src_tab[(int64_t)t * M2L_ENTRIES + e] >= 0) act = true;
-                }
-            }
+            const bool act = e < M2L_ENTRIES && ctl.used[e] &&
+                             (e < N_DISP ? c.disp_compact[e] >= 0 : c.has_l2l != 0);
             unsigned bal = __ballot_sync(0xffffffffu, act);
             if (act) {
                 const int slot = base + __popc(bal & ((1u << lane) - 1));
