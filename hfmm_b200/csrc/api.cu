@@ -491,6 +491,7 @@ void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double*
             mc.ld = T.cmld;
             mc.ldk = T.ckld;
             mc.ldm = T.cmld;
+            mc.m_valid = T.cr;   // rows r..cmld of the C_d tables are zero
             mc.n_fam = 1;
             mc.has_l2l = 0;
             mc.fam_stride = 0;

@@ -12,8 +12,9 @@
 //   * warp 4 (one lane) loads A_hi and A_lo with TMA (3-D tensor maps over the
 //     level's tables, SWIZZLE_128B, K-major) -> mbarrier complete_tx;
 //   * warps 0-3 gather the B columns (source boxes' equivalent densities) with
-//     16-byte cp.async into the same SWIZZLE_128B K-major layout, then fence the
-//     generic->async proxy and arrive on the stage's mbarrier;
+//     16-byte cp.async into the same SWIZZLE_128B K-major layout; each thread's
+//     cp.async.mbarrier.arrive counts on the stage's mbarrier once its copies land
+//     (the MMA warp fences the generic->async proxy after its wait);
 //   * warp 5 (one lane) issues 4 k-steps x 3 tcgen05.mma and commits the stage
 //     back to its "empty" mbarrier;
 // three stages in flight.
@@ -187,9 +188,18 @@ __device__ __forceinline__ void tmem_st(uint32_t taddr, const uint32_t* v) {
     else tmem_st16(taddr, v);
 }
 
-// Instruction descriptor: D = F32, A = B = TF32, both K-major, M = 128, N = BN.
-constexpr uint32_t IDESC = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(BN >> 3) << 17) |
-                           ((uint32_t)(BM >> 4) << 24);
+// Instruction descriptor: D = F32, A = B = TF32, both K-major, M = 128 (or 64), N = BN.
+constexpr uint32_t idesc_m(int m) {
+    return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(BN >> 3) << 17) |
+           ((uint32_t)(m >> 4) << 24);
+}
+constexpr uint32_t IDESC = idesc_m(BM);
+// A row block with at most 64 rows that can be nonzero (the last block of a level whose
+// rank r leaves r - m0 <= 64, e.g. r = 185 in two blocks, or a low-rank sin table)
+// runs the M = 64 shape: half the tensor work. Its accumulator occupies TMEM lanes
+// 0-15 of each 32-lane quadrant (row i at lane 32 (i / 16) + i % 16), the layout
+// CUTLASS's 1-SM UMMA fragments give M = 64.
+constexpr uint32_t IDESC64 = idesc_m(64);
 
 struct __align__(8) Ctl {
     uint64_t full[STAGES];
@@ -216,6 +226,8 @@ __global__ void __launch_bounds__(THREADS, 1) k_m2l_tf32x3(const __grid_constant
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int tile = blockIdx.x, m0 = blockIdx.y * BM, fam = blockIdx.z;
     volatile int* abort_flag = &ctl.abort_flag;
+    const bool half = (c.m_valid > 0 ? c.m_valid : c.ldm) - m0 <= 64;
+    const uint32_t idesc = half ? IDESC64 : IDESC;
 
     if (tid < TT) {   // targets share the sources' box range (a level's own buffers)
         int t = c.tile_tgt[(int64_t)tile * TT + tid];
@@ -230,7 +242,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_m2l_tf32x3(const __grid_constant
     if (tid == 0) {
         ctl.abort_flag = 0;
         for (int s = 0; s < STAGES; ++s) {
-            mbar_init(smem_u32(&ctl.full[s]), 1 + 4);     // TMA arrive + one per gather warp
+            mbar_init(smem_u32(&ctl.full[s]), 1 + 128);   // TMA arrive + each gather thread's copies
             mbar_init(smem_u32(&ctl.empty[s]), 1);       // MMA commit
         }
         for (int b = 0; b < 2; ++b) {
@@ -325,7 +337,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_m2l_tf32x3(const __grid_constant
         const int64_t src_lo = c.src_hi > 0 ? c.src_lo : 0;
         const int64_t src_hi = c.src_hi > 0 ? c.src_hi : c.nb;
         if (nq > 0) load_sources(0);
-        int pending = -1, cur_entry = -1;
+        int cur_entry = -1;
         for (int q = 0; q < nq; ++q) {
             const int st = q % STAGES;
             const int ai = q / kch;
@@ -343,9 +355,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_m2l_tf32x3(const __grid_constant
                 }
                 if (ai + 1 < n_act) load_sources(ai + 1);
             }
-            // the warp arrives once per stage (below), so it leaves the loop as one
-            const bool got = mbar_wait(smem_u32(&ctl.empty[st]), ((q / STAGES) & 1) ^ 1, abort_flag);
-            if (!__all_sync(0xffffffffu, got)) break;
+            if (!mbar_wait(smem_u32(&ctl.empty[st]), ((q / STAGES) & 1) ^ 1, abort_flag)) break;
             const int k0 = (q % kch) * BK;
             const uint32_t sbh = smem_u32(sm + st * STAGE_BYTES + 2 * TILE_BYTES);
             const uint32_t sbl = sbh + TILE_BYTES;
@@ -356,31 +366,22 @@ __global__ void __launch_bounds__(THREADS, 1) k_m2l_tf32x3(const __grid_constant
                 cp_async16(sbh + soff[i], Bh + o, ok);
                 cp_async16(sbl + soff[i], Bl + o, ok);
             }
-            asm volatile("cp.async.commit_group;\n" ::);
-            if (pending >= 0) {
-                // each lane's copies of the previous stage have landed: fence them for
-                // the tensor core, then one arrive per warp (128 arrives on one barrier
-                // word serialise)
-                asm volatile("cp.async.wait_group 1;\n" ::);
-                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                __syncwarp();
-                if (lane == 0) mbar_arrive(smem_u32(&ctl.full[pending % STAGES]));
-            }
-            pending = q;
+            // the stage's barrier counts this thread's arrival when its copies have
+            // landed: no thread waits for its own copies, so every stage can be in flight
+            asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(
+                             smem_u32(&ctl.full[st]))
+                         : "memory");
         }
         asm volatile("cp.async.wait_all;\n" ::);
-        if (pending >= 0) {
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            __syncwarp();
-            if (lane == 0) mbar_arrive(smem_u32(&ctl.full[pending % STAGES]));
-        }
     } else if (warp >= 6) {
         // ---------------- fold entries into the FP64 sums; store at the end
         // Warp w may touch TMEM lanes 32 (w % 4) .. + 31 only: the NFW fold warps
         // cover each lane quadrant NFW / 4 times, each folding its share of columns.
         const int quad = warp & 3;                 // TMEM lane quadrant of this warp
         const int c_lo = ((warp - 6) >> 2) * COLS_PER_FOLD_WARP;
-        const int m = m0 + quad * 32 + lane;
+        // the row of this lane (M = 64 blocks: lanes 16-31 of a quadrant hold none)
+        const int m = half ? m0 + quad * 16 + lane : m0 + quad * 32 + lane;
+        const bool row_ok = half ? (lane < 16 && m < c.ldm) : (m0 + quad * 32 < c.ldm);
         const uint32_t lane_base = tmem + ((uint32_t)(quad * 32) << 16);
         double* out = c.out + (int64_t)fam * c.out_fam_stride;
         bool ok = true;
@@ -421,7 +422,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_m2l_tf32x3(const __grid_constant
         const bool aborted = !__all_sync(0xffffffffu, ok && !*abort_flag);
         if (aborted) {
             if (lane == 0) atomicOr(c.err, ERRF_TIMEOUT);
-        } else if (m0 + quad * 32 < c.ldm) {   // ldm % 32 == 0: a warp is all in or all out
+        } else if (__any_sync(0xffffffffu, row_ok)) {   // the TMEM loads are warp-collective
             for (int cb = c_lo; cb < c_lo + COLS_PER_FOLD_WARP; cb += SUB) {
                 uint32_t w[2 * SUB];
                 if (nq > 0) {
@@ -434,7 +435,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_m2l_tf32x3(const __grid_constant
                     const int n = cb + j;
                     const int t = ctl.tgt[n / R];
                     const double val = nq > 0 ? __hiloint2double((int)w[2 * j + 1], (int)w[2 * j]) : 0.0;
-                    if (t >= 0) out[((int64_t)t * R + (n % R)) * c.ldm + m] = val;
+                    if (t >= 0 && row_ok) out[((int64_t)t * R + (n % R)) * c.ldm + m] = val;
                 }
             }
         }
@@ -482,6 +483,9 @@ __global__ void __launch_bounds__(THREADS, 1) k_m2l_tf32x3(const __grid_constant
                     ok = false;
                     break;
                 }
+                // the gathered B halves were written by cp.async (generic proxy): order them
+                // before the tensor core's (async proxy) reads of the stage
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
                 asm volatile("tcgen05.fence::after_thread_sync;");
                 const uint32_t base = smem_u32(sm + st * STAGE_BYTES);
                 const uint64_t ah = sw128_desc(base), al = sw128_desc(base + TILE_BYTES);
@@ -491,9 +495,9 @@ __global__ void __launch_bounds__(THREADS, 1) k_m2l_tf32x3(const __grid_constant
 #pragma unroll
                 for (int ks = 0; ks < BK / 8; ++ks) {   // 8 tf32 = 32 bytes per k-step
                     const uint64_t d = (uint64_t)(ks * 2);
-                    umma_tf32(dt, ah + d, bh + d, IDESC, (uq > 0 || ks > 0) ? 1u : 0u);
-                    umma_tf32(dt, ah + d, bl + d, IDESC, 1u);
-                    umma_tf32(dt, al + d, bh + d, IDESC, 1u);
+                    umma_tf32(dt, ah + d, bh + d, idesc, (uq > 0 || ks > 0) ? 1u : 0u);
+                    umma_tf32(dt, ah + d, bl + d, idesc, 1u);
+                    umma_tf32(dt, al + d, bh + d, idesc, 1u);
                 }
                 umma_commit(smem_u32(&ctl.empty[st]));
                 if (uq == FOLD - 1 || q == nq - 1) umma_commit(smem_u32(&ctl.acc_full[b]));

@@ -25,6 +25,8 @@ struct MixedCall {
     int R, ld, n_fam, has_l2l;
     int ldk, ldm;                  // rectangular tables: K extent (B rows) and M extent (out
                                    // rows); 0 = ld. A tables are [count][ldm][ldk]
+    int m_valid;                   // rows of A that can be nonzero (0 = ldm): a row block
+                                   // with at most 64 of them runs the M = 64 MMA shape
     int64_t fam_stride, out_fam_stride, nb;
     int64_t src_lo, src_hi;        // valid source boxes [src_lo, src_hi) (0, nb when unset)
     int* err;
