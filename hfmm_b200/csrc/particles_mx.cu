@@ -27,9 +27,37 @@ constexpr int WARPS = 4;               // target leaves per CTA, one warp each
 constexpr int TPL = HFMM_P2P_TPL;
 constexpr int CHAIN = 128;             // sources per FP32 partial-sum chain
 
+// sin and cos of a phase |x| <= SMALL_PHASE by their Taylor series about 0 (Horner
+// form in x^2): the first omitted terms, x^13 / 13! and x^14 / 14!, stay below 3.2e-8
+// and 3.3e-9 there, under the FP32 rounding of the pair arithmetic. Larger phases
+// (big leaves at coarse levels, large k) take sincosf.
+constexpr float SMALL_PHASE = 1.5f;
+__device__ __forceinline__ void sincos_phase(float x, float* s, float* c) {
+    if (fabsf(x) <= SMALL_PHASE) {
+        const float x2 = x * x;
+        float ps = -1.f / 39916800.f;
+        ps = fmaf(ps, x2, 1.f / 362880.f);
+        ps = fmaf(ps, x2, -1.f / 5040.f);
+        ps = fmaf(ps, x2, 1.f / 120.f);
+        ps = fmaf(ps, x2, -1.f / 6.f);
+        ps = fmaf(ps, x2, 1.f);
+        float pc = 1.f / 479001600.f;
+        pc = fmaf(pc, x2, -1.f / 3628800.f);
+        pc = fmaf(pc, x2, 1.f / 40320.f);
+        pc = fmaf(pc, x2, -1.f / 720.f);
+        pc = fmaf(pc, x2, 1.f / 24.f);
+        pc = fmaf(pc, x2, -0.5f);
+        *s = x * ps;
+        *c = fmaf(pc, x2, 1.f);
+    } else {
+        sincosf(x, s, c);
+    }
+}
+
 // One warp per target leaf: each lane keeps TPL targets in registers; the sources
-// of each near leaf are loaded 32 at a time, one per lane, and broadcast with warp
-// shuffles, so the kernel needs neither shared memory nor CTA barriers.
+// of each near leaf are staged 32 at a time in the warp's slice of shared memory
+// (hi position + first charge column, lo position + second) and read back as
+// broadcast loads, two per source; only __syncwarp orders the warp's own slice.
 template <int NF, int R, bool FIELD>
 __global__ void __launch_bounds__(WARPS * 32) k_p2p_mx(EvalView v, const int32_t* __restrict__ leaves,
                                                       int64_t nrows, const int32_t* __restrict__ off,
@@ -39,10 +67,10 @@ __global__ void __launch_bounds__(WARPS * 32) k_p2p_mx(EvalView v, const int32_t
     // so each carries a relative error of about eps32 however close the points are
     // (clustered clouds); everything after that runs in FP32. The phase k r is an
     // FP32 product: r itself carries eps32, so a wider product would add nothing.
+    __shared__ float4 stage[WARPS][32][2];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t row = (int64_t)blockIdx.x * WARPS + warp;
     if (row >= nrows) return;   // the whole warp leaves together
-    const unsigned FULL = 0xffffffffu;
     const int t = leaves[row];
     const int s0t = v.leaf_start[t], cnt_t = v.counts[t];
     constexpr int NA = NF * R * (FIELD ? 4 : 1);
@@ -51,6 +79,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_p2p_mx(EvalView v, const int32_t
     const float kf = (float)v.k;
     const int64_t n = v.n;
     const int e0 = off[row], e1 = off[row + 1];
+    float4(&sw)[32][2] = stage[warp];
     for (int i0 = 0; i0 < cnt_t; i0 += 32 * TPL) {
         float xh[TPL], yh[TPL], zh[TPL], xl[TPL], yl[TPL], zl[TPL];
         bool act[TPL];
@@ -83,39 +112,31 @@ __global__ void __launch_bounds__(WARPS * 32) k_p2p_mx(EvalView v, const int32_t
                     for (int q = 0; q < NA; ++q) a32[u][q] = 0.f;
                 for (int b0 = c0; b0 < cend; b0 += 32) {
                     const int nbat = min(32, cend - b0);
-                    float pxh = 0, pyh = 0, pzh = 0, pxl = 0, pyl = 0, pzl = 0, pq[R];
-#pragma unroll
-                    for (int r = 0; r < R; ++r) pq[r] = 0.f;
+                    __syncwarp();   // the previous batch has been read
                     if (lane < nbat) {
                         const int64_t gs = s0 + b0 + lane;
-                        pxh = v.pos_f[gs];
-                        pyh = v.pos_f[n + gs];
-                        pzh = v.pos_f[2 * n + gs];
-                        pxl = v.pos_f[3 * n + gs];
-                        pyl = v.pos_f[4 * n + gs];
-                        pzl = v.pos_f[5 * n + gs];
-#pragma unroll
-                        for (int r = 0; r < R; ++r) pq[r] = (float)v.q_s[r * n + gs];
+                        const float q0 = (float)v.q_s[gs];
+                        const float q1 = R > 1 ? (float)v.q_s[n + gs] : 0.f;
+                        sw[lane][0] = make_float4(v.pos_f[gs], v.pos_f[n + gs], v.pos_f[2 * n + gs], q0);
+                        sw[lane][1] = make_float4(v.pos_f[3 * n + gs], v.pos_f[4 * n + gs],
+                                                  v.pos_f[5 * n + gs], q1);
                     }
+                    __syncwarp();
                     for (int j = 0; j < nbat; ++j) {
-                        const float sxh = __shfl_sync(FULL, pxh, j), syh = __shfl_sync(FULL, pyh, j);
-                        const float szh = __shfl_sync(FULL, pzh, j), sxl = __shfl_sync(FULL, pxl, j);
-                        const float syl = __shfl_sync(FULL, pyl, j), szl = __shfl_sync(FULL, pzl, j);
-                        float sq[R];
-#pragma unroll
-                        for (int r = 0; r < R; ++r) sq[r] = __shfl_sync(FULL, pq[r], j);
+                        const float4 ph = sw[j][0], pl = sw[j][1];
+                        const float sq[2] = {ph.w, pl.w};
 #pragma unroll
                         for (int u = 0; u < TPL; ++u) {
-                            const float dx = (xh[u] - sxh) + (xl[u] - sxl);
-                            const float dy = (yh[u] - syh) + (yl[u] - syl);
-                            const float dz = (zh[u] - szh) + (zl[u] - szl);
+                            const float dx = (xh[u] - ph.x) + (xl[u] - pl.x);
+                            const float dy = (yh[u] - ph.y) + (yl[u] - pl.y);
+                            const float dz = (zh[u] - ph.z) + (zl[u] - pl.z);
                             const float d2 = dx * dx + dy * dy + dz * dz;
-                            if (!(d2 > thr)) continue;
-                            const float ir = rsqrtf(d2);
+                            // pairs under the floor (the target itself) contribute nothing
+                            const float ir = d2 > thr ? rsqrtf(d2) : 0.f;
                             const float rr = d2 * ir;
                             const float kr = kf * rr;
                             float sn, cs_;
-                            sincosf(kr, &sn, &cs_);
+                            sincos_phase(kr, &sn, &cs_);
                             const float w[2] = {cs_ * ir, sn * ir};
                             float wf[2] = {0.f, 0.f};
                             if (FIELD) {

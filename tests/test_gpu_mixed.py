@@ -29,6 +29,8 @@ CASES = [
     ("small_cplx_field", complex_uniform, 5000, 5.0, 6, 32, None, True),
     ("c1_shape", complex_uniform, 20000, 2 * np.pi, 8, 64, None, True),
     ("adaptive", sphere_clusters, 12000, 10.0, 6, 24, None, True),
+    # near-field phases k r up to about 10: the P2P's series sin/cos hands over to sincosf
+    ("large_phase", complex_uniform, 20000, 60.0, 6, 64, None, True),
 ]
 
 
