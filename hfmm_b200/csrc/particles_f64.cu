@@ -21,7 +21,7 @@ constexpr int STAGE = 128;   // particles staged in shared memory per pass
 // Also P2L (phases.py:1755-1769) when `surf` is the equivalent surface of a
 // target box and the sources are the particles of its X-list leaves.
 template <int NF, int R>
-__global__ void __launch_bounds__(256) k_surface_from_particles(
+__global__ void __launch_bounds__(512) k_surface_from_particles(
     EvalView v, const int32_t* __restrict__ tgt_boxes, const int32_t* __restrict__ off,
     const int32_t* __restrict__ srcs, const double* __restrict__ surf, int only_level,
     double* check, int64_t fam_stride, int accumulate) {
@@ -66,10 +66,10 @@ __global__ void __launch_bounds__(256) k_surface_from_particles(
                     for (int i = 0; i < np; ++i) {
                         double dx = px - sx[i], dy = py - sy[i], dz = pz - sz[i];
                         double r2 = dx * dx + dy * dy + dz * dz;
-                        double rr = sqrt(r2);
+                        double ir = rsqrt(r2);
+                        double rr = r2 * ir;
                         double sn, cs;
-                        sincos(v.k * rr, &sn, &cs);
-                        double ir = 1.0 / rr;
+                        sincos_phase64(v.k * rr, &sn, &cs);
                         double wc = cs * ir, ws = sn * ir;
 #pragma unroll
                         for (int r = 0; r < R; ++r) {
@@ -94,7 +94,10 @@ __global__ void __launch_bounds__(256) k_surface_from_particles(
 
 // Particle potentials (and field) from surface densities: L2P (phases.py:1571-1582,
 // downward equivalent surface R_CHECK of the leaf itself) and M2P (phases.py:1101-1140,
-// upward equivalent surface R_EQUIV of each W-list source box).
+// upward equivalent surface R_EQUIV of each W-list source box). One CTA per target
+// leaf; a group of GL lanes shares a particle, each lane taking every GL-th surface
+// point, so a warp works on 32 / GL particles at once and reduces over GL lanes only.
+constexpr int GL = 8;
 template <int NF, int R, bool FIELD>
 __global__ void __launch_bounds__(256) k_particles_from_surface(
     EvalView v, const int32_t* __restrict__ tgt_leaves, const int32_t* __restrict__ off,
@@ -108,6 +111,8 @@ __global__ void __launch_bounds__(256) k_particles_from_surface(
     if (v.lvls[t] < 2 && !off) return;        // L2P: no local expansion above level 2
     const int s0 = v.leaf_start[t], cnt = v.counts[t];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int grp = lane / GL, gl = lane % GL;   // particle slot of the warp, lane within it
+    constexpr int PW = 32 / GL;                  // particles per warp at once
     const int e0 = off ? off[row] : 0, e1 = off ? off[row + 1] : 1;
     constexpr int NA = NF * R * (FIELD ? 4 : 1);
     for (int e = e0; e < e1; ++e) {
@@ -125,20 +130,22 @@ __global__ void __launch_bounds__(256) k_particles_from_surface(
                     dn[(f * R + r) * v.n_s + j] = dens[f * fam_stride + ((int64_t)sb * R + r) * v.ld + j];
         }
         __syncthreads();
-        for (int i = warp; i < cnt; i += nw) {
-            const int64_t gi = s0 + i;
+        for (int i0 = warp * PW; i0 < cnt; i0 += nw * PW) {
+            const int i = i0 + grp;
+            const bool act = i < cnt;
+            const int64_t gi = s0 + (act ? i : 0);
             const double x = v.pos_s[gi], y = v.pos_s[v.n + gi], z = v.pos_s[2 * v.n + gi];
             double acc[NA];
 #pragma unroll
             for (int q = 0; q < NA; ++q) acc[q] = 0.0;
-            for (int j = lane; j < v.n_s; j += 32) {
+            for (int j = gl; j < v.n_s; j += GL) {
                 double dx = x - ex[j], dy = y - ex[v.n_s + j], dz = z - ex[2 * v.n_s + j];
                 double r2 = dx * dx + dy * dy + dz * dz;
-                double rr = sqrt(r2);
+                double ir = rsqrt(r2);
+                double rr = r2 * ir;
                 double sn, cs;
                 double kr = v.k * rr;
-                sincos(kr, &sn, &cs);
-                double ir = 1.0 / rr;
+                sincos_phase64(kr, &sn, &cs);
                 double w[2] = {cs * ir, sn * ir};
                 double wf[2] = {0.0, 0.0};
                 if (FIELD) {
@@ -163,8 +170,8 @@ __global__ void __launch_bounds__(256) k_particles_from_surface(
 #pragma unroll
             for (int q = 0; q < NA; ++q)
 #pragma unroll
-                for (int o = 16; o > 0; o >>= 1) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], o);
-            if (lane == 0) {
+                for (int o = GL / 2; o > 0; o >>= 1) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], o);
+            if (gl == 0 && act) {
 #pragma unroll
                 for (int q = 0; q < NF * R; ++q) pot[q * v.n + gi] += acc[q];
                 if (FIELD)
@@ -300,17 +307,24 @@ __global__ void k_combine(int64_t n, const int32_t* __restrict__ sidx, const dou
 
 inline int nblk(int64_t n, int t) { return (int)std::max<int64_t>(1, ceil_div(n, t)); }
 
+// threads of a surface kernel: one per surface point in as few passes as possible
+// (n_s = 296 at p = 8 takes 320 threads in one pass, not 256 + 40 in two)
+inline int surface_threads(int n_s) {
+    const int passes = (int)ceil_div(n_s, 512);
+    return (int)std::min<int64_t>(512, round_up(ceil_div(n_s, passes), 32));
+}
+
 template <int NF, int R, bool FIELD>
 void particles_impl(const ParticlePass& p, cudaStream_t s) {
     const EvalView& v = p.v;
     switch (p.op) {
         case ParticleOp::P2M:
-            HFMM_LAUNCH((k_surface_from_particles<NF, R>), p.nrows, 256, 0, s, v, p.rows, p.off,
-                        p.srcs, p.surf, -1, p.out, p.fam_stride, 0);
+            HFMM_LAUNCH((k_surface_from_particles<NF, R>), p.nrows, surface_threads(v.n_s), 0, s, v,
+                        p.rows, p.off, p.srcs, p.surf, -1, p.out, p.fam_stride, 0);
             break;
         case ParticleOp::P2L:
-            HFMM_LAUNCH((k_surface_from_particles<NF, R>), p.nrows, 256, 0, s, v, p.rows, p.off,
-                        p.srcs, p.surf, p.level, p.out, p.fam_stride, 1);
+            HFMM_LAUNCH((k_surface_from_particles<NF, R>), p.nrows, surface_threads(v.n_s), 0, s, v,
+                        p.rows, p.off, p.srcs, p.surf, p.level, p.out, p.fam_stride, 1);
             break;
         case ParticleOp::L2P:
         case ParticleOp::M2P: {
