@@ -46,10 +46,21 @@ namespace {
 
 constexpr int BM = 128;          // UMMA M (check points per CTA)
 constexpr int BN = 128;          // UMMA N (target columns per CTA)
-constexpr int BK = 32;           // fp32 elements per k-chunk (128-byte rows)
-constexpr int STAGES = 3;
-constexpr int TILE_BYTES = BM * BK * 4;   // 16 KiB, one operand half
+// fp32 elements per k-chunk: 32 (128-byte rows, SWIZZLE_128B, three 64 KiB stages) or
+// 16 (64-byte rows, SWIZZLE_64B, six 32 KiB stages), the same 192 KiB of operands in
+// flight. Same results bit for bit; on the 1M-point p = 8 low-rank M2L 32 took 11.5 ms
+// and 16 took 14.0: each stage carries a fixed cost of about 0.3 us that the MMAs do
+// not hide, so fewer, larger stages win.
+#ifndef HFMM_MX_BK
+#define HFMM_MX_BK 32
+#endif
+constexpr int BK = HFMM_MX_BK;
+static_assert(BK == 16 || BK == 32, "k-chunk");
+constexpr int ROW_BYTES = BK * 4;           // one K-major row of a tile
+constexpr int CPR = ROW_BYTES / 16;         // 16-byte chunks per row
+constexpr int TILE_BYTES = BM * ROW_BYTES;  // one operand half
 constexpr int STAGE_BYTES = 4 * TILE_BYTES;
+constexpr int STAGES = (3 * 64 * 1024) / STAGE_BYTES;
 #ifndef HFMM_MX_FOLD_WARPS
 #define HFMM_MX_FOLD_WARPS 16
 #endif
@@ -59,10 +70,7 @@ constexpr int COLS_PER_FOLD_WARP = BN * 4 / N_FOLD_WARPS;
 constexpr int SUB = N_FOLD_WARPS >= 16 ? 16 : 32;  // columns per TMEM access of a fold warp
 static_assert(N_FOLD_WARPS == 4 || N_FOLD_WARPS == 8 || N_FOLD_WARPS == 16, "fold warps");
 constexpr int TMEM_COLS = 512;
-#ifndef HFMM_MX_FOLD
-#define HFMM_MX_FOLD 2
-#endif
-constexpr int FOLD = HFMM_MX_FOLD;   // k-chunks per FP32 accumulation unit
+constexpr int FOLD = 64 / BK;   // k-chunks per FP32 accumulation unit: 64 K values, 24 MMAs
 constexpr uint64_t WAIT_NS = 2000000000ull;   // bounded waits: 2 s
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -118,10 +126,12 @@ __device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap* map
         "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(bar)
         : "memory");
 }
-// UMMA shared-memory descriptor: K-major, SWIZZLE_128B, 8-row groups 1024 B apart.
-__device__ __forceinline__ uint64_t sw128_desc(uint32_t addr) {
-    return (uint64_t)((addr & 0x3FFFF) >> 4) | (1ull << 16) | (64ull << 32) | (1ull << 46) |
-           (2ull << 61);
+// UMMA shared-memory descriptor: K-major, swizzled rows of ROW_BYTES (layout type 2 =
+// SWIZZLE_128B, 4 = SWIZZLE_64B), 8-row groups 8 * ROW_BYTES apart.
+__device__ __forceinline__ uint64_t sw_desc(uint32_t addr) {
+    constexpr uint64_t layout = BK == 32 ? 2 : 4;
+    return (uint64_t)((addr & 0x3FFFF) >> 4) | (1ull << 16) |
+           ((uint64_t)(8 * ROW_BYTES / 16) << 32) | (1ull << 46) | (layout << 61);
 }
 __device__ __forceinline__ void umma_tf32(uint32_t tmem, uint64_t a, uint64_t b, uint32_t idesc,
                                           uint32_t acc) {
@@ -311,26 +321,30 @@ __global__ void __launch_bounds__(THREADS, 1) k_m2l_tf32x3(const __grid_constant
         // ---------------- B gathers (cp.async, manual SWIZZLE_128B placement)
         const float* Bh = c.Bhi + fs;
         const float* Bl = c.Blo + fs;
-        // Each thread always serves chunk ch of the same 8 rows (columns) of the B tile:
-        // rows n_i = (tid >> 3) + 16 i. Their swizzled shared-memory offsets are fixed;
+        // Each thread always serves chunk ch of the same CPR rows (columns) of the B
+        // tile: rows n_i = tid / CPR + (128 / CPR) i. Their swizzled shared-memory
+        // offsets are fixed (the 16-byte chunk index XORs with the row's bits: all three
+        // for 128-byte rows, the upper two for 64-byte rows, as TMA and the MMA read them);
         // their global sources change only when the displacement entry changes.
-        const int ch = tid & 7;
-        uint32_t soff[8];
-        int64_t goff[8];
+        constexpr int RSTEP = 128 / CPR;
+        const int ch = tid % CPR;
+        uint32_t soff[CPR];
+        int64_t goff[CPR];
 #pragma unroll
-        for (int i = 0; i < 8; ++i) {
-            const int n = (tid >> 3) + 16 * i;
-            soff[i] = (uint32_t)((n >> 3) * 1024 + (n & 7) * 128 + ((ch ^ (n & 7)) << 4));
+        for (int i = 0; i < CPR; ++i) {
+            const int n = tid / CPR + RSTEP * i;
+            const int sw = BK == 32 ? (n & 7) : ((n & 7) >> 1);
+            soff[i] = (uint32_t)((n >> 3) * 8 * ROW_BYTES + (n & 7) * ROW_BYTES + ((ch ^ sw) << 4));
             goff[i] = -1;
         }
         // The source boxes of the next entry are loaded while the current one streams,
         // so the table lookups' latency stays off the copy pipeline.
-        int nsrc[8];
+        int nsrc[CPR];
         auto load_sources = [&](int ai) {
             const int e = ctl.act[ai];
 #pragma unroll
-            for (int i = 0; i < 8; ++i) {
-                const int t = ctl.tgt[((tid >> 3) + 16 * i) / R];
+            for (int i = 0; i < CPR; ++i) {
+                const int t = ctl.tgt[(tid / CPR + RSTEP * i) / R];
                 nsrc[i] = t >= 0 ? c.src_tab[(int64_t)t * M2L_ENTRIES + e] : -1;
             }
         };
@@ -344,8 +358,8 @@ __global__ void __launch_bounds__(THREADS, 1) k_m2l_tf32x3(const __grid_constant
             if (ai != cur_entry) {   // new displacement entry: this thread's 8 sources
                 cur_entry = ai;
 #pragma unroll
-                for (int i = 0; i < 8; ++i) {
-                    const int n = (tid >> 3) + 16 * i;
+                for (int i = 0; i < CPR; ++i) {
+                    const int n = tid / CPR + RSTEP * i;
                     int s_ = nsrc[i];
                     if (s_ >= 0 && (s_ < src_lo || s_ >= src_hi)) {
                         atomicOr(c.err, ERRF_BOUNDS);
@@ -360,7 +374,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_m2l_tf32x3(const __grid_constant
             const uint32_t sbh = smem_u32(sm + st * STAGE_BYTES + 2 * TILE_BYTES);
             const uint32_t sbl = sbh + TILE_BYTES;
 #pragma unroll
-            for (int i = 0; i < 8; ++i) {
+            for (int i = 0; i < CPR; ++i) {
                 const bool ok = goff[i] >= 0;
                 const int64_t o = ok ? goff[i] + k0 : 0;
                 cp_async16(sbh + soff[i], Bh + o, ok);
@@ -488,9 +502,9 @@ __global__ void __launch_bounds__(THREADS, 1) k_m2l_tf32x3(const __grid_constant
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
                 asm volatile("tcgen05.fence::after_thread_sync;");
                 const uint32_t base = smem_u32(sm + st * STAGE_BYTES);
-                const uint64_t ah = sw128_desc(base), al = sw128_desc(base + TILE_BYTES);
-                const uint64_t bh = sw128_desc(base + 2 * TILE_BYTES),
-                               bl = sw128_desc(base + 3 * TILE_BYTES);
+                const uint64_t ah = sw_desc(base), al = sw_desc(base + TILE_BYTES);
+                const uint64_t bh = sw_desc(base + 2 * TILE_BYTES),
+                               bl = sw_desc(base + 3 * TILE_BYTES);
                 const uint32_t dt = tmem + b * BN;
 #pragma unroll
                 for (int ks = 0; ks < BK / 8; ++ks) {   // 8 tf32 = 32 bytes per k-step
@@ -578,7 +592,7 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
 }  // namespace
 
 void make_table_map(CUtensorMap* map, const float* base, int ld, int count, int ldm) {
-    // [count][ldm][ld] fp32 (ldm = 0: square), boxes of 32 k x 128 m
+    // [count][ldm][ld] fp32 (ldm = 0: square), boxes of BK k x 128 m
     if (!ldm) ldm = ld;
     if (((uintptr_t)base & 15) || (ld * 4) % 16 || ld < BK || ldm < BM)
         throw Error{HFMM_ERR_STATE, "tensor map: table not 16-byte aligned or smaller than a box"};
@@ -587,7 +601,8 @@ void make_table_map(CUtensorMap* map, const float* base, int ld, int count, int 
     cuuint32_t box[3] = {BK, BM, 1};
     cuuint32_t estr[3] = {1, 1, 1};
     CUresult r = encode_fn()(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, (void*)base, dims, strides,
-                             box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                             box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                             BK == 32 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B,
                              CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) throw Error{HFMM_ERR_CUDA, "cuTensorMapEncodeTiled failed: " + std::to_string((int)r)};
 }
