@@ -12,6 +12,46 @@ namespace hfmm {
 
 namespace {
 
+// sin and cos of a phase: Cody-Waite reduction against pi/2 with a two-part constant
+// (1.5707963267948966 + 6.123233995736766e-17, the first being pi/2 rounded to FP64,
+// both from pi itself) done with FMAs, so r = x - n pi/2 is exact to about 1e-28 for
+// |x| <= 1e5; then the Taylor series of sin and cos on |r| <= pi/4 (through r^15 and
+// r^16: the first omitted terms stay under 4.7e-17 and 2.1e-18) and the quadrant
+// n mod 4. Larger phases take sincos.
+__device__ __forceinline__ void sincos_reduced(double x, double* s, double* c) {
+    if (!(fabs(x) <= 1.0e5)) {
+        sincos(x, s, c);
+        return;
+    }
+    const double n = rint(x * 0.6366197723675814);   // x / (pi / 2), rounded
+    double r = fma(-n, 1.5707963267948966, x);
+    r = fma(-n, 6.123233995736766e-17, r);
+    const double r2 = r * r;
+    double ps = 1.0 / 1307674368000.0;               // 1/15!
+    ps = fma(ps, r2, -1.0 / 6227020800.0);           // -1/13!
+    ps = fma(ps, r2, 1.0 / 39916800.0);              // 1/11!
+    ps = fma(ps, r2, -1.0 / 362880.0);               // -1/9!
+    ps = fma(ps, r2, 1.0 / 5040.0);                  // 1/7!
+    ps = fma(ps, r2, -1.0 / 120.0);                  // -1/5!
+    ps = fma(ps, r2, 1.0 / 6.0);                     // 1/3!
+    double pc = -1.0 / 20922789888000.0;             // -1/16!
+    pc = fma(pc, r2, 1.0 / 87178291200.0);           // 1/14!
+    pc = fma(pc, r2, -1.0 / 479001600.0);            // -1/12!
+    pc = fma(pc, r2, 1.0 / 3628800.0);               // 1/10!
+    pc = fma(pc, r2, -1.0 / 40320.0);                // -1/8!
+    pc = fma(pc, r2, 1.0 / 720.0);                   // 1/6!
+    pc = fma(pc, r2, -1.0 / 24.0);                   // -1/4!
+    pc = fma(pc, r2, 0.5);                           // 1/2!
+    const double sr = fma(-r * r2, ps, r);           // sin r = r - r^3 (1/3! - ...)
+    const double cr = fma(-r2, pc, 1.0);             // cos r = 1 - r^2 (1/2! - ...)
+    switch ((int)((long long)n & 3)) {
+        case 0: *s = sr; *c = cr; break;
+        case 1: *s = cr; *c = -sr; break;
+        case 2: *s = -sr; *c = -cr; break;
+        default: *s = -cr; *c = sr; break;
+    }
+}
+
 constexpr int DT = 128;        // targets per CTA
 constexpr int DSTAGE = 256;    // sources staged per pass
 constexpr int NV = 8;          // phi re/im + field 3 x re/im
@@ -60,9 +100,9 @@ __global__ void __launch_bounds__(DT) k_direct_partial(const double* __restrict_
             double dx = x - sx[i], dy = y - sy[i], dz = z - sz[i];
             double r2 = dx * dx + dy * dy + dz * dz;
             if (!(r2 > 0.0)) continue;
-            double r = sqrt(r2), ir = 1.0 / r;
+            double ir = rsqrt(r2), r = r2 * ir;
             double kr = k * r, sn, cs;
-            sincos(kr, &sn, &cs);
+            sincos_reduced(kr, &sn, &cs);
             // w = e^{ikr}/r; q w
             double wr = cs * ir, wi = sn * ir;
             acc[0] += sqr[i] * wr - sqi[i] * wi;

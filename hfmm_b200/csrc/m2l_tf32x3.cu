@@ -224,6 +224,7 @@ struct __align__(8) Ctl {
     short act[M2L_ENTRIES + 1];
     short zidx[M2L_ENTRIES + 1];   // A-table index of each active entry (M2L or L2L table)
     unsigned char used[M2L_ENTRIES + 1];   // entry has a source for some target of the tile
+    short ztab[M2L_ENTRIES + 1];           // A-table index of every entry (-1: none)
 };
 
 template <int R>
@@ -248,7 +249,10 @@ __global__ void __launch_bounds__(THREADS, 1) k_m2l_tf32x3(const __grid_constant
         }
         ctl.tgt[tid] = t;
     }
-    for (int e = tid; e < M2L_ENTRIES; e += THREADS) ctl.used[e] = 0;
+    for (int e = tid; e < M2L_ENTRIES; e += THREADS) {
+        ctl.used[e] = 0;
+        ctl.ztab[e] = (short)(e < N_DISP ? c.disp_compact[e] : (c.has_l2l ? e - N_DISP : -1));
+    }
     if (tid == 0) {
         ctl.abort_flag = 0;
         for (int s = 0; s < STAGES; ++s) {
@@ -275,7 +279,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_m2l_tf32x3(const __grid_constant
     // source table's rows are read coalesced) and the loads of a batch independent of
     // each other; warp 0 then compacts the flags with ballots
     {
-        constexpr int BATCH = 8;
+        constexpr int BATCH = 16;
         constexpr int PAIRS = TT * M2L_ENTRIES;
         for (int i0 = tid; i0 < PAIRS; i0 += THREADS * BATCH) {
             int src[BATCH];
@@ -298,13 +302,12 @@ __global__ void __launch_bounds__(THREADS, 1) k_m2l_tf32x3(const __grid_constant
         int base = 0;
         for (int e0 = 0; e0 < M2L_ENTRIES; e0 += 32) {
             int e = e0 + lane;
-            const bool act = e < M2L_ENTRIES && ctl.used[e] &&
-                             (e < N_DISP ? c.disp_compact[e] >= 0 : c.has_l2l != 0);
+            const bool act = e < M2L_ENTRIES && ctl.used[e] && ctl.ztab[e] >= 0;
             unsigned bal = __ballot_sync(0xffffffffu, act);
             if (act) {
                 const int slot = base + __popc(bal & ((1u << lane) - 1));
                 ctl.act[slot] = (short)e;
-                ctl.zidx[slot] = (short)(e < N_DISP ? c.disp_compact[e] : e - N_DISP);
+                ctl.zidx[slot] = ctl.ztab[e];
             }
             base += __popc(bal);
         }
