@@ -349,6 +349,7 @@ void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double*
         c.R = R;
         c.ld = P->ld;
         c.n_s = P->n_s;
+        c.k_valid = P->n_s;   // every table's rows past n_s are zero
         c.fam_stride = fs;
         c.a_fam_stride = k_entries[kind];
         c.n_fam = NF;
@@ -376,6 +377,7 @@ void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double*
             c.R = R;
             c.ld = P->ld;
             c.n_s = P->n_s;
+            c.k_valid = P->n_s;
             c.fam_stride = 0;
             c.a_fam_stride = 0;
             c.n_fam = 1;
@@ -428,6 +430,7 @@ void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double*
                       cudaStream_t st, const double* scale = nullptr) {
         GemmCall c{};
         c.scale = scale;
+        c.k_valid = kind == K_EXP ? P->tables[f][l].cr : P->n_s;   // compress reads y (n_s)
         c.tile_tgt = P->dec_tiles[l][R - 1].tgt.p;
         c.ntiles = P->dec_tiles[l][R - 1].ntiles;
         c.src_tab = nullptr;

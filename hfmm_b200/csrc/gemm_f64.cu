@@ -117,7 +117,7 @@ __global__ void __launch_bounds__(128) k_gemm_f64(GemmCall c, int* err) {
     }
     __syncthreads();
     const int n_act = sm.n_act;
-    const int kch = c.ldk / KC;
+    const int kch = c.k_valid > 0 ? (c.k_valid + KC - 1) / KC : c.ldk / KC;
     const int nq = n_act * kch;
 
     auto load = [&](int q, int buf) {
@@ -232,6 +232,7 @@ void gemm_f64(const GemmCall& call, int* d_err, cudaStream_t s) {
     if (!c.ldm) c.ldm = c.ld;
     if (c.ldk % KC != 0 || c.ldm % KC != 0)
         throw Error{HFMM_ERR_STATE, "gemm_f64: ld must be a multiple of 16"};
+    if (c.k_valid > c.ldk) throw Error{HFMM_ERR_STATE, "gemm_f64: k_valid beyond ldk"};
     if (c.n_entries > MAX_ENTRIES) throw Error{HFMM_ERR_STATE, "gemm_f64: too many entries"};
     dim3 grid(c.ntiles, (c.ldm + TM - 1) / TM, c.n_fam);
     if (c.R == 1) HFMM_LAUNCH(k_gemm_f64<1>, grid, 128, 0, s, c, d_err);

@@ -247,6 +247,8 @@ struct GemmCall {
     int ld;                    // padded n_s (multiple of 16)
     int ldk, ldm;              // rectangular calls: K extent / B row length and M extent /
                                // out row length (0: both ld); A^T is ldk x ldm
+    int k_valid;               // rows of A^T that can be nonzero (0: ldk); the K loop stops
+                               // after the last chunk that holds one
     int n_s;
     int64_t fam_stride;        // elements between the families' B/out arrays
     int64_t a_fam_stride;      // entries between the families' A pointer sets
