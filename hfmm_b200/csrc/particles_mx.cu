@@ -59,8 +59,9 @@ __device__ __forceinline__ void sincos_phase(float x, float* s, float* c) {
 // (hi position + first charge column, lo position + second) and read back as
 // broadcast loads, two per source; only __syncwarp orders the warp's own slice.
 // The FP64 per-target sums live in shared memory, read and written once per chain of
-// up to CHAIN sources, which keeps the kernel at 64 registers and 8 CTAs per SM (1M points, p = 8: the near
-// field took 4.5 ms beside the upward pass at 96 registers, 4.2 at 72, 4.15 at 64).
+// up to CHAIN sources, which keeps the kernel at 64 registers and 8 CTAs per SM (1M
+// points, p = 8: the near field took 4.5 ms beside the upward pass at 96 registers,
+// 4.2 at 72, 4.15 at 64).
 template <int NF, int R, bool FIELD>
 __global__ void __launch_bounds__(WARPS * 32, 8) k_p2p_mx(EvalView v, const int32_t* __restrict__ leaves,
                                                       int64_t nrows, const int32_t* __restrict__ off,
