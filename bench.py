@@ -52,6 +52,18 @@ CONFIGS = {
     "c1": dict(n=20_000, k=2 * np.pi, p=8, leaf=64, max_depth=None,
                workload="uniform cube, N=2e4, complex N(0,1) charges, k=2pi, p=8, leaf 64, "
                         "potential+field"),
+    # adaptive workloads (W/X lists active), measured like c2 (learned p, certified)
+    "c3": dict(n=2_000_000, k=20.0, p=12, leaf=64, max_depth=None, dist="sphere_clusters",
+               metric="points/s per evaluate at rel-L2 1e-6, C3 (sphere + clusters, k=20): "
+                      "mixed+learned-p vs plain FP64",
+               workload="N=2e6: half uniform on the sphere of radius 0.5 about (0.5,0.5,0.5), "
+                        "half in 8 Gaussian clusters (sigma 0.03, centres U[0.1,0.9]^3), "
+                        "complex N(0,1) charges, k=20, potential+field"),
+    "c5": dict(n=8_000_000, k=40.0, p=12, leaf=64, max_depth=None, dist="clusters16",
+               metric="points/s per evaluate at rel-L2 1e-6, C5 (16 clusters, k=40): "
+                      "mixed+learned-p vs plain conservative p in FP64",
+               workload="N=8e6 in 16 Gaussian clusters (sigma 0.05, centres U[0.1,0.9]^3), "
+                        "complex N(0,1) charges, k=40, potential+field"),
     "c4": dict(n=64, k=None, p=12, leaf=64, max_depth=None,
                workload="64 problems, N log-uniform in [1e4, 5e5], uniform cube, k ~ U[1, 30], "
                         "complex N(0,1) charges, tol 1e-6, learned p, mixed, one graph launch, "
@@ -101,7 +113,19 @@ def make_problem(cfg, rank=0):
     """Seeded synthetic input of the workload's shape (test.py:40 convention)."""
     n = cfg["n"]
     rng = np.random.default_rng(42 + n + 1000 * rank)
-    pos = rng.uniform(0.0, 1.0, (n, 3))
+    dist = cfg.get("dist")
+    if dist == "sphere_clusters":        # C3
+        ns = n // 2
+        d = rng.normal(size=(ns, 3))
+        sph = 0.5 + 0.5 * d / np.linalg.norm(d, axis=1, keepdims=True)
+        c = rng.uniform(0.1, 0.9, (8, 3))
+        cl = c[rng.integers(0, 8, n - ns)] + 0.03 * rng.normal(size=(n - ns, 3))
+        pos = np.concatenate([sph, cl])
+    elif dist == "clusters16":           # C5
+        c = rng.uniform(0.1, 0.9, (16, 3))
+        pos = c[rng.integers(0, 16, n)] + 0.05 * rng.normal(size=(n, 3))
+    else:
+        pos = rng.uniform(0.0, 1.0, (n, 3))
     q = rng.normal(size=n) + 1j * rng.normal(size=n)
     return pos, q
 
@@ -609,6 +633,16 @@ def run_auto(a, cfg, rank, world, local_rank):
                "h2d_bytes_per_step": int(16 * n), "d2h_bytes_per_step": int(16 * n + 48 * n),
                "ms_per_step": ms_e2e, "call": "AutoPlan.evaluate_field(numpy complex128 charges)"}
 
+    # what the line needs from the learned plan; then free it before the plain plan is
+    # built (at 8M points the two plans do not fit together)
+    NF, R = st.n_families, 2
+    flops = 3.0 * m2l_flops(st, R, NF) if rank == 0 else None
+    st_info = dict(n_s=st.info["n_s"], max_depth=st.max_depth, n_boxes=st.info["n_boxes"],
+                   ranks=dict(getattr(st, "m2l_ranks", {})))
+    ap_cmp, ap_report, n_check = ap.m2l_compress, dict(ap.report), int(len(ap.check_idx))
+    ap.close()
+    torch.cuda.empty_cache()
+
     plain = None
     if not a.no_plain:        # the plain FP64 path at the configuration's p, same points
         sp = hfmm_b200.setup(pos, cfg["k"], p=cfg["p"], N_max=cfg["leaf"],
@@ -635,8 +669,6 @@ def run_auto(a, cfg, rank, world, local_rank):
 
     out = None
     if rank == 0:
-        NF, R = st.n_families, 2
-        flops = 3.0 * m2l_flops(st, R, NF)
         dom_ms = float(phase[_lib.PHASES.index("m2l_l2l_gemm")])
         peak = measured_tf32_peak(torch)
         achieved = flops / (dom_ms * 1e-3) / 1e12 if dom_ms > 0 else None
@@ -644,11 +676,11 @@ def run_auto(a, cfg, rank, world, local_rank):
                 "frac": (achieved / peak) if achieved else None, "traffic": _traffic(a, "auto"),
                 "traffic_unit": "bytes per evaluate (all M2L launches), from profiles/traffic.json",
                 "kernel": ("k_m2l_tf32x3 (M2L, 3xTF32 on tcgen05, all levels"
-                           + (", on the low-rank C_d tables)" if ap.m2l_compress else ")")),
+                           + (", on the low-rank C_d tables)" if ap_cmp else ")")),
                 "algorithmic_flops_per_evaluate": flops, "kernel_ms_per_evaluate": dom_ms,
                 "flop_count": ("3 TF32 products x 2 r^2 per V pair, charge column and family, "
                                "r = the rank of the pair's level and family (unpadded)"
-                               if ap.m2l_compress else
+                               if ap_cmp else
                                "3 TF32 products x 2 n_s^2 per V pair, charge column and family"),
                 "peak_source": "cuBLAS FP32 GEMM with TF32 tensor cores, 8192^3, measured in "
                                "this run (of measured; MEASURED_PEAKS.json has no TF32 figure)"}
@@ -660,26 +692,27 @@ def run_auto(a, cfg, rank, world, local_rank):
             cpu = {"value": n / t_cpu, "unit": "points/s", "cores": int(blas), "kind": "port",
                    "sample": sample + f"; the reference's path at the configuration's p={cfg['p']}",
                    "seconds_per_evaluate": t_cpu, "host_cores": cores}
-        last = reports[-1] if reports else ap.report
+        last = reports[-1] if reports else ap_report
+        workload = (f"uniform cube, N={n:.0e}, complex N(0,1) charges, k={cfg['k']:g}"
+                    if "dist" not in cfg else cfg["workload"].replace(", potential+field", ""))
         out = {
-            "metric": METRIC, "value": world * n / (ms * 1e-3), "unit": "points/s",
+            "metric": cfg.get("metric", METRIC), "value": world * n / (ms * 1e-3), "unit": "points/s",
             "n_gpus": world, "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32+tf32x3+f64",
-            "data": "synthetic (seeded uniform points and N(0,1) complex charges)",
-            "config": {"workload": f"uniform cube, N={n:.0e}, complex N(0,1) charges, "
-                                   f"k={cfg['k']:g}, tol {a.tol:g}, learned p and leaf, "
+            "data": "synthetic (seeded points of the workload's distribution, N(0,1) complex charges)",
+            "config": {"workload": f"{workload}, tol {a.tol:g}, learned p and leaf, "
                                    "mixed precision, certified on 256 targets, potential+field",
                        "n_points": n, "k": cfg["k"], "tol": a.tol, "p": last["p"],
-                       "leaf": last["leaf"], "n_s": st.info["n_s"], "max_depth": st.max_depth,
+                       "leaf": last["leaf"], "n_s": st_info["n_s"], "max_depth": st_info["max_depth"],
                        "precision": "mixed" if last["precision"] == 1 else "fp64",
-                       "m2l_compress": ap.m2l_compress,
+                       "m2l_compress": ap_cmp,
                        "m2l_ranks": {f"{'cos' if f == 0 else 'sin'}{l}": r for (f, l), r in
-                                     sorted(getattr(st, "m2l_ranks", {}).items())},
+                                     sorted(st_info["ranks"].items())},
                        "parallelism": f"replicas x{world}",
                        "l2": "inputs larger than L2 (operator tables and expansions of "
-                             f"{st.info['n_boxes']} boxes)"},
-            "certification": {"targets": int(len(ap.check_idx)), "tol": a.tol,
+                             f"{st_info['n_boxes']} boxes)"},
+            "certification": {"targets": n_check, "tol": a.tol,
                               "steps_certified": int(sum(r["certified"] for r in reports)),
                               "steps_fallback": int(sum(r["fallback"] for r in reports)),
                               "error_256": last["error"]},
@@ -690,7 +723,6 @@ def run_auto(a, cfg, rank, world, local_rank):
             "gpu_launches": int(launches), "clocks": clocks, "e2e": e2e,
             "roofline": roof, "cpu_baseline": cpu,
         }
-    ap.close()
     if dist:
         dist.barrier()
         dist.destroy_process_group()

@@ -114,12 +114,21 @@ def _compact(arr, scatter, mb):
     return out
 
 
+class _Overflow(Exception):
+    pass
+
+
 def build_fmm_tree(positions, max_boxes, max_depth, N_max):
     """One fixed-buffer build (cubic.py:316-527).
 
     Returns dict with m_id (u64), p_id (i32), lvls (i32), counts (i32),
     is_leaf (bool), sort_idx (i32), domain_extent, pmin, overflow flag and the
     largest box id touched (``max_box_count``).
+
+    A pass whose box ids reach the buffer size is discarded by the caller
+    (cubic.py:586-595 retries with a doubled buffer); the reference's JAX gathers
+    clamp the out-of-range ids of such a pass, NumPy's would raise, so the pass
+    stops there and only reports the overflow.
     """
     pos = np.asarray(positions, dtype=np.float64)
     mb = int(max_boxes)
@@ -140,6 +149,8 @@ def build_fmm_tree(positions, max_boxes, max_depth, N_max):
     changes = np.concatenate([[False], sm[1:] != sm[:-1]])
     node_ids = np.cumsum(changes).astype(np.int64)
 
+    if int(node_ids[-1]) >= mb:
+        return dict(max_boxes_exceeded=True, max_box_count=int(node_ids[-1]))
     counts = _segment_sum(None, node_ids, mb).astype(np.int32)
     m_id = _segment_max_u64(sm, node_ids, mb)
     lvls = (counts > 0).astype(np.int32) * md
@@ -147,6 +158,8 @@ def build_fmm_tree(positions, max_boxes, max_depth, N_max):
     is_leaf = counts > 0
     max_box_count = int(node_ids[-1])
     allids = np.arange(mb, dtype=np.int64)
+    if max_box_count >= mb:
+        return dict(max_boxes_exceeded=True, max_box_count=max_box_count)
 
     def step(i, check_balance):
         nonlocal m_id, p_id, lvls, counts, is_leaf, max_box_count
@@ -160,6 +173,8 @@ def build_fmm_tree(positions, max_boxes, max_depth, N_max):
         par_m = np.where(on, par_m, U64(0))
         tn = (np.cumsum(cc) + ofs).astype(np.int64)
         max_box_count = max(max_box_count, int(tn[-1]))
+        if max_box_count >= mb:
+            raise _Overflow()
         this_c = _segment_sum(prev_c.astype(np.int64), tn, mb).astype(np.int32)
         this_m = _segment_max_u64(par_m, tn, mb)
         m_id = m_id + this_m
@@ -193,9 +208,12 @@ def build_fmm_tree(positions, max_boxes, max_depth, N_max):
         p_id = _compact(p_id, sc, mb)
         is_leaf = _compact(is_leaf | mark, sc, mb)
 
-    step(0, False)
-    for i in range(1, md - 1):
-        step(i, True)
+    try:
+        step(0, False)
+        for i in range(1, md - 1):
+            step(i, True)
+    except _Overflow:
+        return dict(max_boxes_exceeded=True, max_box_count=max_box_count)
     lvl1 = lvls == 1
     p_id = np.where(lvl1, np.arange(mb, dtype=np.int32), p_id).astype(np.int32)
     return dict(m_id=m_id, p_id=p_id, lvls=lvls.astype(np.int32), counts=counts.astype(np.int32),

@@ -56,3 +56,20 @@ def plane(n, seed=5):
     pos = rng.uniform(0.0, 1.0, (n, 3))
     pos[:, 2] = 0.5 + 1e-3 * pos[:, 2]
     return pos, rng.normal(size=n)
+
+
+def sphere_and_clusters(n, seed=11):
+    """The C3 workload's shape: half uniform on the sphere of radius 0.5 about
+    (0.5, 0.5, 0.5), half in 8 Gaussian clusters (sigma 0.03, centres U[0.1, 0.9]^3);
+    complex N(0,1) charges. Deep and adaptive: at n = 8000 with leaf 16 the tree
+    build must double its box buffer (6096 -> 12192)."""
+    rng = np.random.default_rng(seed + n)
+    ns = n // 2
+    d = rng.normal(size=(ns, 3))
+    sph = 0.5 + 0.5 * d / np.linalg.norm(d, axis=1, keepdims=True)
+    c = rng.uniform(0.1, 0.9, (8, 3))
+    cl = c[rng.integers(0, 8, n - ns)] + 0.03 * rng.normal(size=(n - ns, 3))
+    pos = np.concatenate([sph, cl])
+    q = rng.normal(size=n) + 1j * rng.normal(size=n)
+    return pos, q
+

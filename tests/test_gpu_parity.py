@@ -12,7 +12,8 @@ import numpy as np
 import pytest
 
 import oracle as O
-from cases import uniform, clustered, plane, with_duplicates, complex_uniform, sphere_clusters
+from cases import (uniform, clustered, plane, with_duplicates, complex_uniform, sphere_clusters,
+                   sphere_and_clusters)
 
 pytestmark = pytest.mark.gpu
 TOL = 1e-12
@@ -81,12 +82,22 @@ LIVE = [
     ("depth5", uniform, 3000, 4.0, 4, 8, 5),
     ("clustered_d3", clustered, 2500, 6.0, 5, 32, 3),
     ("sphere", sphere_clusters, 4000, 10.0, 4, 24, None),
+    # the C3 shape: deep, adaptive, and the tree buffer doubles once (6096 -> 12192)
+    ("c3_shape", sphere_and_clusters, 8000, 20.0, 4, 16, None),
 ]
+# Tolerance per case: 1e-12, except where the FP64 method's own rounding floor is
+# higher. On the C3 shape (depth 6, k = 20) the oracle's two summation orders (one
+# decode per site or one fused decode per box) already differ by 2.3e-12 on the real
+# charges: the damped sin-component decodes (eps_rel 1e-12) amplify summation-order
+# differences. The bar there is 1e-11, about four times that floor (which the test
+# re-measures); the CUDA path measured 3.7e-12.
+CASE_TOL = {"c3_shape": 1e-11}
 
 
 @pytest.mark.parametrize("name,fn,n,k,p,nmax,md", LIVE, ids=[c[0] for c in LIVE])
 def test_live_oracle(name, fn, n, k, p, nmax, md):
     import hfmm_b200
+    tol = CASE_TOL.get(name, TOL)
     pos, q = fn(n)
     ref = O.setup(pos, k, p=p, N_max=nmax, max_depth=md)
     st = _setup(pos, k, p, nmax, md)
@@ -103,11 +114,16 @@ def test_live_oracle(name, fn, n, k, p, nmax, md):
         assert np.all(phi == 0) and np.all(E == 0)
         return
     phi_r = hfmm_b200.evaluate(st, qc.real)
-    assert O.relative_error(phi_r, O.evaluate(ref, qc.real)) < TOL
+    ref_r = O.evaluate(ref, qc.real)
+    if tol > TOL:   # the floor that justifies the wider bar is still there, and below it
+        fused = O.evaluate_complex(ref, qc.real, fused_decode=True)
+        floor = O.relative_error(fused, ref_r)
+        assert 1e-13 < floor < tol / 2, floor
+    assert O.relative_error(phi_r, ref_r) < tol
     phi, E = hfmm_b200.evaluate_field(st, qc)
     rphi, rE = O.evaluate_complex(ref, qc, field=True)
-    assert O.relative_error(phi, rphi) < TOL
-    assert O.relative_error(E, rE) < TOL
+    assert O.relative_error(phi, rphi) < tol
+    assert O.relative_error(E, rE) < tol
 
 
 def test_c1_shape_against_oracle():

@@ -12,7 +12,7 @@ import pytest
 
 import oracle as O
 from oracle.hfmm import HelmholtzComponent
-from cases import uniform, clustered, sphere_clusters, with_duplicates, plane
+from cases import uniform, clustered, sphere_clusters, with_duplicates, plane, sphere_and_clusters
 
 
 def _leaves_under(s):
@@ -115,3 +115,17 @@ def test_oracle_rounding_floor():
     a = O.evaluate_complex(st, q, field=False, fused_decode=False)
     b = O.evaluate_complex(st, q, field=False, fused_decode=True)
     assert O.relative_error(b, a) < 1e-13
+
+
+def test_tree_build_retries_when_the_buffer_overflows():
+    """A deep adaptive cloud whose box ids outgrow the first buffer: the reference
+    discards that pass and doubles the buffer (cubic.py:586-595); the restatement
+    must do the same instead of indexing past its arrays."""
+    from oracle.tree import build_fmm_tree_auto, initial_max_boxes
+    pos, _ = sphere_and_clusters(8000)
+    t, mb, md, maxleaf = build_fmm_tree_auto(pos, N_max=16)
+    assert mb == 2 * initial_max_boxes(len(pos), 16) and md == 6
+    leaf = t["is_leaf"] & (t["lvls"] > 0)
+    assert int(t["counts"][leaf].sum()) == len(pos)
+    assert not t["max_boxes_exceeded"]
+
