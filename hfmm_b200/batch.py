@@ -185,7 +185,7 @@ class AutoBatch:
                  device=None, margin=0.5, wisdom=None):
         from . import setup, _device
         from .learned import (OrderNet, features_for, conservative_p, precision_for,
-                              compress_for, FEATURE_LEAF, TOL_LEARNED)
+                              compress_for, network_applies, FEATURE_LEAF, TOL_LEARNED)
         self.tol = float(tol)
         self.device = _device(device)
         self.problems = problems
@@ -195,7 +195,9 @@ class AutoBatch:
             net = OrderNet.load(device=self.device) if net is None else net
             feats = np.stack([features_for(x, k, self.tol, self.device) for x, k in problems])
             Y = net.predict(feats)
-            choice = [net.choose_from(y, margin) for y in Y]
+            plain = (conservative_p(self.tol), FEATURE_LEAF)
+            choice = [net.choose_from(y, margin) if network_applies(f, self.tol) else plain
+                      for f, y in zip(feats, Y)]
         self.choice = choice
         self.precisions = [precision_for(self.tol, p) for p, _ in choice]
         self.states = [setup(x, k, p=p, N_max=leaf, device=self.device, stream_tables=True,

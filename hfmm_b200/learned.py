@@ -41,6 +41,8 @@ LEAVES = (16, 32, 64, 128)
 FEATURE_LEAF = 64          # the tree the features are read from
 TOL_MIXED = 1e-6           # the mixed-precision path is used at tolerances >= this
 TOL_LEARNED = 3e-7         # below this the network is not consulted (outside its training range)
+KD_TRAINED = 24.0          # largest k x domain extent of the committed training sweep
+KD_TRUSTED = 1.5 * KD_TRAINED   # beyond this the network is not consulted either
 DEFAULT_WEIGHTS = os.path.join(os.path.dirname(__file__), "data", "order_net.npz")
 
 
@@ -48,6 +50,15 @@ def conservative_p(tol):
     """The plain order: two surface points per edge for each decade of tolerance,
     clamped to [4, 16] (1e-6 -> 12, the order of the plain path's 1M-point config)."""
     return int(min(P_MAX, max(P_MIN, math.ceil(-2.0 * math.log10(tol)))))
+
+
+def network_applies(feats, tol):
+    """Whether the network's order may be used for these features: the tolerance is
+    in its training range and k x extent at most 1.5 times the largest one it saw
+    (24 in the sweep). Measured: at k x extent up to 30 (the batched workload) its
+    orders certified 62 of 64 problems; at 44 (8M clustered points, k = 40) p = 9
+    missed 1e-6 and every step fell back to the plain FP64 rerun."""
+    return tol >= TOL_LEARNED and float(feats[1]) <= KD_TRUSTED
 
 
 def precision_for(tol, p):
@@ -254,12 +265,14 @@ class AutoPlan:
         self.device = _device(device)
         self.positions = positions
         self.p_plain = conservative_p(self.tol)
-        if net is False or self.tol < TOL_LEARNED:
-            self.p, self.leaf, self.feats = self.p_plain, FEATURE_LEAF, None
-        else:
-            net = OrderNet.load(device=self.device) if net is None else net
+        self.p, self.leaf, self.feats = self.p_plain, FEATURE_LEAF, None
+        self.network_used = False
+        if net is not False and self.tol >= TOL_LEARNED:
             self.feats = features_for(positions, k, tol, self.device)
-            self.p, self.leaf = net.choose(self.feats, margin)
+            if network_applies(self.feats, self.tol):
+                net = OrderNet.load(device=self.device) if net is None else net
+                self.p, self.leaf = net.choose(self.feats, margin)
+                self.network_used = True
         self.precision = precision_for(self.tol, self.p)
         self.m2l_compress = compress_for(self.tol, self.precision)
         self.state = setup(positions, k, p=self.p, N_max=self.leaf, device=self.device,
@@ -348,7 +361,7 @@ class AutoPlan:
             check_errors(self.state)
             err = self._error(phi, E, ref)
             rep = dict(p=self.p, leaf=self.leaf, precision=int(self.precision), error=err,
-                       fallback=False, p_final=self.p)
+                       fallback=False, p_final=self.p, network=self.network_used)
             p = self.p_plain
             while err > self.tol and p <= P_MAX:
                 st = self._plain_state(p)

@@ -100,6 +100,20 @@ def test_auto_plan_below_the_learned_range_uses_the_conservative_order():
     ap.close()
 
 
+def test_auto_plan_beyond_the_trained_wavenumbers_starts_conservative():
+    """k x extent 40 lies beyond 1.5 x the training sweep's 24: the plan starts at the
+    conservative order (12 at 1e-6), still in mixed precision, and certifies."""
+    from hfmm_b200.learned import AutoPlan
+    import hfmm_b200 as hf
+    x, q = _problem(20000, seed=5)
+    ap = AutoPlan(x, 40.0, tol=1e-6)
+    assert ap.feats is not None and ap.feats[1] > 36 and not ap.network_used
+    assert ap.p == 12 and ap.precision == hf.PREC_MIXED
+    ap.evaluate(q)
+    assert ap.report["certified"] and not ap.report["network"]
+    ap.close()
+
+
 def test_auto_plan_conservative_certifies():
     from hfmm_b200.learned import AutoPlan
     x, q = _problem()

@@ -121,3 +121,17 @@ def test_choose_keeps_the_leaf_at_64_or_128():
     assert OrderNet.choose_from([7.4, 7.6]) == (8, 128)
     assert OrderNet.choose_from([2.0, 9.0]) == (4, 128)     # p clamped to [4, 16]
     assert OrderNet.choose_from([30.0, 6.4]) == (16, 64)
+
+
+def test_network_is_consulted_only_in_its_range():
+    from hfmm_b200.learned import network_applies, TOL_LEARNED, KD_TRUSTED
+    f = np.zeros(24, np.float32)
+    f[1] = 30.0                                   # the batched workload's largest k x extent
+    assert network_applies(f, 1e-6)
+    f[1] = 44.0                                   # 8M clustered points at k = 40
+    assert not network_applies(f, 1e-6)
+    f[1] = KD_TRUSTED
+    assert network_applies(f, 1e-6)
+    f[1] = 10.0
+    assert not network_applies(f, TOL_LEARNED / 2)
+
