@@ -6,12 +6,14 @@ check the CUDA product: only ``tests/``, ``__graft_entry__.smoke()`` and the
 CPU-baseline leg of ``bench.py`` may import it, and never as the thing that is
 measured or shipped.
 
-Pinning: the reference ships no golden vectors. The oracle is pinned against
-the reference's own known-answer checks (test.py:63-72: direct-sum error
-thresholds, linearity, exact-zero imaginary part at k=0, monotone improvement
-in p) on the reference's default test grid, and against an O(N^2) direct sum.
-Bit-exact parity of the oracle with the reference's JAX arrays is unpinned:
-JAX is not installed here, so the reference cannot be run.
+Pinning: the reference ships no golden vectors and JAX is not installed here,
+so the reference's own Python code was run on a NumPy stand-in for the JAX calls
+it makes (tests/golden/jax_on_numpy.py, tests/golden/make_golden.py) and its
+outputs committed as fixtures (tests/golden/*.npz, tests/golden/edge/*.npz).
+The oracle matches them bit for bit on every integer array (tree, sort order,
+particles-in-leaf, U/V/W/X/near lists, buffer sizes) and to the rounding floor
+on potentials and fields (tests/test_golden.py). It also passes the reference's
+known-answer checks (test.py:63-72) and an O(N^2) direct sum.
 """
 
 from .surfaces import n_surf, surface_pts, R_EQUIV, R_CHECK

@@ -322,9 +322,14 @@ def eval_direct(s, kern, ppts, pchg, rev, field, batch=512):
     return flat[rev] / (4 * np.pi)
 
 
-def evaluate_setup(s, charges, field=False, fused_decode=False):
+def evaluate_setup(s, charges, field=False, fused_decode=False, trace=None):
     """Potential (N, R) or field (N, R, 3) of the real KIFMM for charge columns
-    (kifmm/setup.py:229-261 -> core.evaluate, core.py:274-335)."""
+    (kifmm/setup.py:229-261 -> core.evaluate, core.py:274-335).
+
+    ``trace``: a dict that receives each phase's output, keyed by the phase
+    (``s2m``, ``m2m``, ``m2l``, ``p2l``, ``l2l``, ``l2p``, ``p2p``, ``m2p``), at the
+    points where core.evaluate hands it to the next phase (core.py:297-335)."""
+    rec = (lambda key, val: trace.__setitem__(key, val)) if trace is not None else (lambda *_: None)
     kern = s["kernel"]
     Q = np.asarray(charges, dtype=np.float64)
     squeeze = Q.ndim == 1
@@ -339,11 +344,13 @@ def evaluate_setup(s, charges, field=False, fused_decode=False):
 
     # upward pass: P2M + decode, then M2M level by level (phases.py:118-125, 163-173)
     equiv = _decode_leveled(p2m(s, kern, ppts, pchg, centres, h), ops["F_up_lv"], lvls, md)
+    rec("s2m", equiv)
     for cl in range(md, 1, -1):
         chk = m2m_check(s, equiv, cl)
         pl = cl - 1
         solved = _decode(chk, tuple(f[pl] for f in ops["F_up_lv"]))
         equiv = equiv + np.where((lvls == pl)[:, None, None], solved, 0.0)
+    rec("m2m", equiv)
 
     # downward pass
     m2l_c = m2l_check(s, equiv)
@@ -361,17 +368,25 @@ def evaluate_setup(s, charges, field=False, fused_decode=False):
                 loc[rows] = _decode(chk[rows], tuple(f[cl] for f in ops["F_dn_lv"]))
     else:
         loc = _decode_leveled(m2l_c, ops["F_dn_lv"], lvls, md)        # phases.py:237
+        rec("m2l", loc.copy())
         for t, c in p2l_pairs:                                         # phases.py:1766-1770
             loc[t] += _decode(c[None], tuple(f[lvls[t]] for f in ops["F_dn_lv"]))[0]
+        if p2l_pairs:
+            rec("p2l", loc.copy())
         for cl in range(2, md + 1):                                    # phases.py:273-280
             add = _decode(l2l_check(s, loc, cl), tuple(f[cl] for f in ops["F_dn_lv"]))
             loc = loc + np.where((lvls == cl)[:, None, None], add, 0.0)
+    rec("l2l", loc)
 
     far = l2p(s, kern, loc, ppts, rev, centres, h, field)
     near = eval_direct(s, kern, ppts, pchg, rev, field)
+    rec("l2p", far)
+    rec("p2p", near)
     pot = far + near
     if s["W"] is not None:
-        pot = pot + m2p(s, kern, equiv, positions, centres, h, field)
+        mp = m2p(s, kern, equiv, positions, centres, h, field)
+        rec("m2p", mp)
+        pot = pot + mp
     return pot[:, 0] if squeeze else pot
 
 

@@ -1,24 +1,45 @@
-"""Generate the golden fixtures under tests/golden/ from the oracle.
+"""Generate the golden fixtures under tests/golden/ by running the reference itself.
 
-The reference (JAX) cannot run in this environment, so the fixtures record the
-oracle's outputs -- pinned against the reference's own known-answer checks in
-tests/test_oracle_known_answers.py -- for small seeded cases: the tree arrays
-(build_fmm_tree outputs for the active boxes), the particles-in-leaf table,
-the V/U/W/X/near lists and the evaluate outputs. Run from the repo root:
+JAX is not installed here and there is no network, so the reference's own
+Python code (`HFMM.py` and the `jaxfmm` package) runs on `jax_on_numpy`, a NumPy
+stand-in for the part of JAX it calls (eager, host only; see that module for the
+JAX semantics it reproduces). Every array in a fixture comes from the
+reference's functions, not from this repository's oracle:
 
-    python tests/golden/make_golden.py
+* tree: `build_fmm_tree_auto` (trees/cubic.py:530-600) as `core.setup_geometry`
+  calls it (m_id, p_id, lvls, counts, is_leaf, sort_idx, max_boxes, depth);
+* U list: `build_ulist_eager` (trees/lists.py:857-889), recorded on its way
+  into `setup_geometry`;
+* particles-in-leaf table, V / W / X lists, near list (`dir_cnct`), maxleaf,
+  domain extent: the state that `HFMM.setup` (HFMM.py:55-80) returns;
+* potentials: `HFMM.evaluate` (HFMM.py:83-91); complex charges by linearity,
+  `evaluate(re) + 1j * evaluate(im)`, since the reference takes real charges only;
+* fields (-grad phi): `kifmm.evaluate_setup(state, q, field=True)`
+  (kifmm/setup.py:229-261) of each component and each charge column, combined
+  as F(re) + 1j * F(im) with F(q) = F_cos(q) + 1j * F_sin(q).
+
+Needs the reference source tree (default /root/reference, or argument
+`--reference DIR`); run from the repo root:
+
+    python tests/golden/make_golden.py [--reference DIR] [--edge] [case ...]
+    python tests/golden/make_golden.py [--reference DIR] --grid
+    python tests/golden/make_golden.py [--reference DIR] --phases
+
+The inputs are the seeded clouds of tests/cases.py.
 """
+import argparse
 import os
 import sys
+import time
 
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+sys.path.insert(0, HERE)
 sys.path.insert(0, os.path.dirname(HERE))
 
-import oracle as O  # noqa: E402
-from cases import uniform, clustered, sphere_clusters, with_duplicates, complex_uniform  # noqa: E402
+from cases import (uniform, clustered, sphere_clusters, with_duplicates, complex_uniform,  # noqa: E402
+                   plane, sphere_and_clusters)
 
 CASES = {
     # name: (cloud, n, k, p, N_max, max_depth, complex charges + field)
@@ -30,34 +51,216 @@ CASES = {
     "cplx2000_k8_p6_d4": (complex_uniform, 2000, 8.0, 6, 32, 4, True),
 }
 
+# Edge cases (tests/golden/edge/): a single point, two points, one box over its
+# leaf size, a plane (depth refinement), many duplicates, explicit depths, and the
+# C3 shape, where the box buffer overflows once and the build retries doubled.
+EDGE = {
+    "tiny1": (uniform, 1, 1.0, 3, 16, None, False),
+    "tiny2": (uniform, 2, 1.0, 3, 16, None, False),
+    "tiny17": (uniform, 17, 1.0, 3, 16, None, False),
+    "plane3000_k3_p4": (plane, 3000, 3.0, 4, 16, None, False),
+    "dups1200_k2_p4": (with_duplicates, 1200, 2.0, 4, 16, None, False),
+    "depth5_3000_k4_p4": (uniform, 3000, 4.0, 4, 8, 5, False),
+    "clustered2500_k6_p5_d3": (clustered, 2500, 6.0, 5, 32, 3, False),
+    "c3shape8000_k20_p4": (sphere_and_clusters, 8000, 20.0, 4, 16, None, True),
+}
 
-def make(name):
-    fn, n, k, p, nmax, md, cplx = CASES[name]
+
+def load_reference(path):
+    """Import `HFMM` from the reference tree on the NumPy stand-in, with recorders
+    on the two builder functions whose outputs `HFMM.setup` does not keep."""
+    import jax_on_numpy
+    jax_on_numpy.install()
+    sys.path.insert(0, path)
+    import HFMM
+    import jaxfmm.trees as trees
+
+    seen = {}
+    tree_auto, ulist = trees.build_fmm_tree_auto, trees.build_ulist_eager
+
+    def record_tree(*a, **k):
+        out = tree_auto(*a, **k)
+        seen["tree"] = out
+        return out
+
+    def record_u(*a, **k):
+        u = ulist(*a, **k)
+        seen["U"] = np.asarray(u)
+        return u
+
+    trees.build_fmm_tree_auto, trees.build_ulist_eager = record_tree, record_u
+    return HFMM, seen
+
+
+def _pairs(x):
+    return np.empty((0, 2), np.int32) if x is None else np.asarray(x).astype(np.int32)
+
+
+def make(HFMM, seen, name, table=CASES, folder=HERE):
+    from jaxfmm import kifmm
+    fn, n, k, p, nmax, md, cplx = table[name]
     pos, q = fn(n)
     if cplx and not np.iscomplexobj(q):
         q = q + 1j * np.random.default_rng(n).normal(size=n)
-    st = O.setup(pos, k, p=p, N_max=nmax, max_depth=md)
-    s = st[0]
-    nb = int((s["lvls"] > 0).sum())
+    seen.clear()
+    state = HFMM.setup(pos, k, p=p, N_max=nmax, max_depth=md)
+    s = state[0]
+    (tree, mb, depth, maxleaf) = seen["tree"]
+    m_id, p_id, lvls, counts, is_leaf, sort_idx = (np.asarray(a) for a in tree[:6])
+    nb = int((lvls > 0).sum())
+    assert not (lvls[nb:] > 0).any()
     out = dict(positions=pos, charges=q, k=k, p=p, N_max=nmax,
-               max_depth=-1 if md is None else md, realised_depth=s["max_depth"],
-               maxleaf=s["maxleaf"], max_boxes=s["max_boxes"], domain_extent=s["domain_extent"],
-               m_id=s["m_id"][:nb], p_id=s["p_id"][:nb], lvls=s["lvls"][:nb],
-               counts=s["counts"][:nb], is_leaf=s["is_leaf"][:nb], sort_idx=s["sort_idx"],
-               pil=s["pil"][:nb], V=s["V"], U=s["U"], near=s["dir_cnct"],
-               W=s["W"] if s["W"] is not None else np.empty((0, 2), np.int32),
-               X=s["X"] if s["X"] is not None else np.empty((0, 2), np.int32))
-    if cplx:
-        phi, E = O.evaluate_complex(st, q, field=True)
-        out.update(phi=phi, E=E)
+               max_depth=-1 if md is None else md, realised_depth=int(s["max_depth"]),
+               maxleaf=int(s["maxleaf"]), max_boxes=int(mb),
+               domain_extent=float(s["domain_extent"]),
+               m_id=m_id[:nb], p_id=p_id[:nb], lvls=lvls[:nb], counts=counts[:nb],
+               is_leaf=is_leaf[:nb], sort_idx=sort_idx.astype(np.int32),
+               pil=np.asarray(s["pil"])[:nb], V=_pairs(s["V"]), U=_pairs(seen["U"]),
+               near=_pairs(s["dir_cnct"]), W=_pairs(s["W"]), X=_pairs(s["X"]))
+    assert int(depth) == out["realised_depth"] and int(maxleaf) == out["maxleaf"]
+    for key in ("m_id", "p_id", "lvls", "is_leaf"):
+        assert np.array_equal(np.asarray(s[key])[:nb], out[key]), key
+
+    def potential(qr):
+        return np.asarray(HFMM.evaluate(state, qr))
+
+    def field(qr):
+        fc = np.asarray(kifmm.evaluate_setup(state[0], qr, field=True))
+        fs = (np.asarray(kifmm.evaluate_setup(state[1], qr, field=True)) if state[1] is not None
+              else np.zeros_like(fc))
+        return fc + 1j * fs
+
+    if np.iscomplexobj(q):
+        out["phi"] = potential(q.real) + 1j * potential(q.imag)
     else:
-        out.update(phi=O.evaluate(st, q))
-    np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+        out["phi"] = potential(q)
+    if cplx:
+        out["E"] = field(q.real) + 1j * field(q.imag)
+    os.makedirs(folder, exist_ok=True)
+    np.savez_compressed(os.path.join(folder, name + ".npz"), **out)
     return out
 
 
+def run_test_py_grid(HFMM, folder):
+    """The reference's own check script (test.py:24-77) on its default grid,
+    uniform and clustered: n in (256, 640), k in (0, 1, 3), p in (3, 5), leaf
+    size 16, seed 42 + n. Records the reference's potentials for each case, and
+    asserts test.py's checks on them (the error bounds against the direct sum,
+    linearity at 1e-10, an exactly-zero imaginary part at k = 0, improvement
+    with p)."""
+    out = {}
+    for clustered_cloud in (False, True):
+        for n in (256, 640):
+            rng = np.random.default_rng(42 + n)
+            positions = rng.uniform(0., 1., (n, 3))
+            if clustered_cloud:
+                positions[:n // 2] = rng.uniform(.1, .25, (n // 2, 3))
+            charges = rng.normal(size=n)
+            tag = f"{'clustered' if clustered_cloud else 'uniform'}{n}"
+            out[f"{tag}_positions"] = positions
+            out[f"{tag}_charges"] = charges
+            for k in (0.0, 1.0, 3.0):
+                d = positions[:, None, :] - positions[None, :, :]
+                r = np.linalg.norm(d, axis=-1)
+                direct = np.where(r > 0, np.exp(1j * k * r) / np.where(r > 0, r, 1.), 0.) @ charges
+                base = None
+                for p in (3, 5):
+                    t = time.time()
+                    state = HFMM.setup(positions, k, p=p, N_max=16)
+                    phi = np.asarray(HFMM.evaluate(state, charges))
+                    half = np.asarray(HFMM.evaluate(state, -.5 * charges))
+                    errs = np.array([np.linalg.norm(a - b) / (np.linalg.norm(b) or 1.0) for a, b in
+                                     ((phi, direct), (phi.real, direct.real), (phi.imag, direct.imag))])
+                    assert errs.max() < (5e-2 if p <= 3 else 5e-3), errs
+                    np.testing.assert_allclose(half, -.5 * phi, rtol=1e-10, atol=1e-10)
+                    if k == 0:
+                        assert np.count_nonzero(phi.imag) == 0
+                    if base is not None:
+                        assert np.all(errs < np.maximum(.8 * base, 2e-6)), errs
+                    base = errs if base is None else base
+                    key = f"{tag}_k{k:g}_p{p}"
+                    out[key + "_phi"] = phi
+                    out[key + "_errors"] = errs
+                    print(key, "errors", errs, f"{time.time() - t:.0f} s", flush=True)
+    os.makedirs(folder, exist_ok=True)
+    np.savez_compressed(os.path.join(folder, "test_py_grid.npz"), **out)
+
+
+# Per-phase outputs (tests/golden/phases/): an adaptive cloud with V, U, W and X
+# lists all non-empty, real charges, both kernel components.
+PHASE_CASE = (clustered, 600, 2.0, 4, 16)
+PHASE_FNS = {"p2m_padded_leveled": "s2m", "m2m_factored_leveled": "m2m", "m2l_leveled": "m2l",
+             "p2l_leveled": "p2l", "l2l_factored_leveled": "l2l", "l2p_padded": "l2p",
+             "m2p": "m2p"}
+
+
+def run_phases(HFMM, folder):
+    """Record what each phase hands to the next inside the reference's evaluate
+    (core.py:297-335): the closures of kifmm/assemble.py:15-89 look their phase
+    functions up in that module at call time, and core.evaluate calls
+    `eval_direct` from its own namespace, so recorders placed there see every
+    phase. Box arrays keep the active boxes' rows (the rest are asserted zero)."""
+    import jaxfmm.core as core
+    import jaxfmm.kifmm.assemble as assemble
+    from jaxfmm import kifmm
+    rec = {}
+
+    def recorder(fn, key):
+        def wrapped(*a, **k):
+            out = fn(*a, **k)
+            rec[key] = np.asarray(out)
+            return out
+        return wrapped
+
+    for name, key in PHASE_FNS.items():
+        setattr(assemble, name, recorder(getattr(assemble, name), key))
+    core.eval_direct = recorder(core.eval_direct, "p2p")
+
+    fn, n, k, p, nmax = PHASE_CASE
+    pos, q = fn(n)
+    state = HFMM.setup(pos, k, p=p, N_max=nmax)
+    s = state[0]
+    assert s["W"] is not None and s["X"] is not None and len(s["V"])
+    nb = int((np.asarray(s["lvls"]) > 0).sum())
+    out = dict(positions=pos, charges=q, k=k, p=p, N_max=nmax, n_boxes=nb)
+    for comp, st in (("cos", state[0]), ("sin", state[1])):
+        rec.clear()
+        pot = np.asarray(kifmm.evaluate_setup(st, q))
+        assert set(rec) == set(PHASE_FNS.values()) | {"p2p"}, sorted(rec)
+        for key, val in rec.items():
+            if val.shape[0] == np.asarray(s["lvls"]).shape[0]:
+                assert not np.any(val[nb:]), key
+                val = val[:nb]
+            out[f"{comp}_{key}"] = val
+        out[f"{comp}_potential"] = pot
+        print(comp, {key: v.shape for key, v in rec.items()}, flush=True)
+    os.makedirs(folder, exist_ok=True)
+    np.savez_compressed(os.path.join(folder, "clustered600_k2_p4.npz"), **out)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--edge", action="store_true", help="the edge cases, into edge/")
+    ap.add_argument("--grid", action="store_true",
+                    help="the reference's test.py grid, into grid/test_py_grid.npz")
+    ap.add_argument("--phases", action="store_true",
+                    help="per-phase outputs of one adaptive case, into phases/")
+    ap.add_argument("cases", nargs="*")
+    a = ap.parse_args()
+    HFMM, seen = load_reference(a.reference)
+    if a.phases:
+        return run_phases(HFMM, os.path.join(HERE, "phases"))
+    if a.grid:
+        return run_test_py_grid(HFMM, os.path.join(HERE, "grid"))
+    table, folder = (EDGE, os.path.join(HERE, "edge")) if a.edge else (CASES, HERE)
+    for name in (a.cases or table):
+        t = time.time()
+        o = make(HFMM, seen, name, table, folder)
+        print(name, "boxes", len(o["m_id"]), "V", len(o["V"]), "U", len(o["U"]),
+              "near", len(o["near"]), "W", len(o["W"]), "X", len(o["X"]),
+              f"{time.time() - t:.0f} s", flush=True)
+
+
 if __name__ == "__main__":
-    for name in (sys.argv[1:] or CASES):
-        o = make(name)
-        print(name, "boxes", len(o["m_id"]), "V", len(o["V"]), "near", len(o["near"]),
-              "W", len(o["W"]), "X", len(o["X"]))
+    main()

@@ -1,10 +1,13 @@
-"""Parity of the CUDA path with the oracle.
+"""Parity of the CUDA path with the reference and the oracle.
 
 Integer work (tree arrays, particle slots, interaction lists) must match bit
 for bit; potentials and fields must match to a relative L2 of 1e-12 (float64
-everywhere; the bar of the plain path). Cases: the committed golden fixtures
-and live oracle runs on further clouds (plane / depth refinement, tiny N,
-duplicates, explicit max_depth)."""
+everywhere; the bar of the plain path). Cases: the committed golden fixtures,
+which are the reference's own outputs (tests/golden/make_golden.py runs its
+code on a NumPy stand-in for JAX), and live oracle runs on further clouds
+(plane / depth refinement, tiny N, duplicates, explicit max_depth, the C3
+shape), whose inputs tests/golden/edge/ pins the oracle on against the
+reference in the same way."""
 import glob
 import os
 

@@ -1,7 +1,9 @@
 """The reference's own known-answer checks (test.py:24-77) run against the oracle.
 
-These pin the oracle: the reference ships no golden vectors, so its test.py
-assertions are the known answers available: complex128 finite output, relative
+The reference ships no golden vectors; its test.py assertions are its known
+answers, and on its default grid the oracle's potentials also equal the
+reference's own (tests/golden/grid/, made by running the reference's code, see
+tests/golden/make_golden.py): complex128 finite output, relative
 L2 error vs the O(N^2) direct sum below 5e-2 (p <= 3) or 5e-3 (p > 3) for the
 total, real and imaginary parts, linearity at 1e-10, an exactly-zero imaginary
 part at k = 0, and errors that improve with p against the smallest p.
@@ -9,14 +11,24 @@ part at k = 0, and errors that improve with p against the smallest p.
 import numpy as np
 import pytest
 
+import os
+
 import oracle as O
 from cases import uniform, clustered
+
+# The reference's own potentials on this grid: tests/golden/make_golden.py --grid ran
+# its test.py checks on them (they pass) and stored them.
+GRID = os.path.join(os.path.dirname(__file__), "golden", "grid", "test_py_grid.npz")
 
 
 @pytest.mark.parametrize("n", [256, 640])
 @pytest.mark.parametrize("clust", [False, True])
 def test_reference_grid(n, clust):
     pos, q = (clustered if clust else uniform)(n)
+    with np.load(GRID) as z:
+        tag = f"{'clustered' if clust else 'uniform'}{n}"
+        grid = {key: z[key] for key in z.files if key.startswith(tag + "_")}
+    assert np.array_equal(grid[tag + "_positions"], pos) and np.array_equal(grid[tag + "_charges"], q)
     for k in (0.0, 1.0, 3.0):
         ref = O.direct(pos, q, k)
         baseline = None
@@ -24,8 +36,13 @@ def test_reference_grid(n, clust):
             st = O.setup(pos, k, p=p, N_max=16)
             act = O.evaluate(st, q)
             assert act.dtype == np.complex128 and np.isfinite(act).all()
+            # the reference's own output on the same case, to its rounding floor
+            assert O.relative_error(act, grid[f"{tag}_k{k:g}_p{p}_phi"]) < 1e-12
             errs = np.array([O.relative_error(a, b) for a, b in
                              ((act, ref), (act.real, ref.real), (act.imag, ref.imag))])
+            # the same errors; an error near 1e-11 (the sin part at k = 1) moves by the
+            # rounding floor of the potential, so the bar has an absolute part
+            np.testing.assert_allclose(errs, grid[f"{tag}_k{k:g}_p{p}_errors"], rtol=1e-6, atol=1e-12)
             assert max(errs) < (5e-2 if p <= 3 else 5e-3), errs
             np.testing.assert_allclose(O.evaluate(st, -0.5 * q), -0.5 * act, rtol=1e-10, atol=1e-10)
             if k == 0:
