@@ -24,6 +24,7 @@ Needs the reference source tree (default /root/reference, or argument
     python tests/golden/make_golden.py [--reference DIR] [--edge] [case ...]
     python tests/golden/make_golden.py [--reference DIR] --grid
     python tests/golden/make_golden.py [--reference DIR] --phases
+    python tests/golden/make_golden.py [--reference DIR] --c1
 
 The inputs are the seeded clouds of tests/cases.py.
 """
@@ -238,6 +239,51 @@ def run_phases(HFMM, folder):
     np.savez_compressed(os.path.join(folder, "clustered600_k2_p4.npz"), **out)
 
 
+def c1_problem():
+    """The reference's CPU-runnable configuration: 20 000 points uniform in the unit
+    cube, complex N(0, 1) charges, seeded default_rng(42 + N) (test.py:40
+    convention: positions, then real and imaginary charge parts), k = 2 pi, p = 8,
+    leaf size 64 (auto depth 3), potential and field, checked on 1024 targets
+    drawn by default_rng(42 + N + 1)."""
+    n = 20_000
+    rng = np.random.default_rng(42 + n)
+    pos = rng.uniform(0.0, 1.0, (n, 3))
+    q = rng.normal(size=n) + 1j * rng.normal(size=n)
+    sample = np.sort(np.random.default_rng(42 + n + 1).choice(n, 1024, replace=False))
+    return pos, q, 2 * np.pi, 8, 64, sample
+
+
+def run_c1(HFMM, seen, folder):
+    from jaxfmm import kifmm
+    pos, q, k, p, nmax, sample = c1_problem()
+    t = time.time()
+    seen.clear()
+    state = HFMM.setup(pos, k, p=p, N_max=nmax)
+    s = state[0]
+    (tree, mb, depth, maxleaf) = seen["tree"]
+    m_id, p_id, lvls, counts, is_leaf, sort_idx = (np.asarray(a) for a in tree[:6])
+    nb = int((lvls > 0).sum())
+    print("setup", f"{time.time() - t:.0f} s", flush=True)
+
+    def both(qr, field):
+        a = np.asarray(kifmm.evaluate_setup(state[0], qr, field=field))
+        b = np.asarray(kifmm.evaluate_setup(state[1], qr, field=field))
+        return a + 1j * b
+
+    phi = both(q.real, False) + 1j * both(q.imag, False)
+    E = both(q.real, True) + 1j * both(q.imag, True)
+    print("evaluate", f"{time.time() - t:.0f} s", flush=True)
+    out = dict(positions_sum=np.float64(pos.sum()), charges_sum=q.sum(), k=k, p=p, N_max=nmax,
+               sample=sample, realised_depth=int(s["max_depth"]), maxleaf=int(s["maxleaf"]),
+               max_boxes=int(mb), domain_extent=float(s["domain_extent"]),
+               m_id=m_id[:nb], p_id=p_id[:nb], lvls=lvls[:nb], counts=counts[:nb],
+               is_leaf=is_leaf[:nb], sort_idx=sort_idx.astype(np.int32),
+               V=_pairs(s["V"]), U=_pairs(seen["U"]), near=_pairs(s["dir_cnct"]),
+               phi=phi[sample], E=E[sample])
+    os.makedirs(folder, exist_ok=True)
+    np.savez_compressed(os.path.join(folder, "c1_n20000_k2pi_p8.npz"), **out)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
@@ -246,9 +292,13 @@ def main():
                     help="the reference's test.py grid, into grid/test_py_grid.npz")
     ap.add_argument("--phases", action="store_true",
                     help="per-phase outputs of one adaptive case, into phases/")
+    ap.add_argument("--c1", action="store_true",
+                    help="the 2e4-point CPU-runnable configuration, into c1/")
     ap.add_argument("cases", nargs="*")
     a = ap.parse_args()
     HFMM, seen = load_reference(a.reference)
+    if a.c1:
+        return run_c1(HFMM, seen, os.path.join(HERE, "c1"))
     if a.phases:
         return run_phases(HFMM, os.path.join(HERE, "phases"))
     if a.grid:

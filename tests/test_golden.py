@@ -130,3 +130,33 @@ def test_oracle_phases_match_the_reference():
             err = O.relative_error(tr[key][:, 0], g[f"{comp}_{key}"])
             assert err < 1e-12, (comp, key, err)
         assert O.relative_error(pot, g[f"{comp}_potential"]) < 1e-12
+
+
+C1 = os.path.join(os.path.dirname(__file__), "golden", "c1", "c1_n20000_k2pi_p8.npz")
+
+
+def test_oracle_matches_the_reference_at_the_cpu_runnable_configuration():
+    """20 000 uniform points, complex N(0, 1) charges, k = 2 pi, p = 8, leaf size 64
+    (depth 3), potential and field: the oracle's tree and lists equal the
+    reference's, and its outputs on the 1024 sampled targets match the reference's
+    own to 1e-12 (tests/golden/make_golden.py --c1 made the fixture)."""
+    g = load(C1)
+    n = 20_000
+    rng = np.random.default_rng(42 + n)
+    pos = rng.uniform(0.0, 1.0, (n, 3))
+    q = rng.normal(size=n) + 1j * rng.normal(size=n)
+    assert pos.sum() == g["positions_sum"] and q.sum() == g["charges_sum"]
+    st = O.setup(pos, float(g["k"]), p=int(g["p"]), N_max=int(g["N_max"]))
+    s = st[0]
+    nb = len(g["m_id"])
+    assert s["max_boxes"] == int(g["max_boxes"]) and s["max_depth"] == int(g["realised_depth"])
+    assert s["maxleaf"] == int(g["maxleaf"]) and s["domain_extent"] == float(g["domain_extent"])
+    for key in ("m_id", "p_id", "lvls", "counts", "is_leaf"):
+        assert np.array_equal(s[key][:nb], g[key]), key
+    assert np.array_equal(s["sort_idx"], g["sort_idx"])
+    for key, sk in (("V", "V"), ("U", "U"), ("near", "dir_cnct")):
+        assert np.array_equal(s[sk], g[key]), key
+    phi, E = O.evaluate_complex(st, q, field=True)
+    sample = g["sample"]
+    assert O.relative_error(phi[sample], g["phi"]) < TOL
+    assert O.relative_error(E[sample], g["E"]) < TOL
