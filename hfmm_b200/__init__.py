@@ -224,13 +224,43 @@ def _load_compressed(state, eps):
                 del U, C
 
 
+def _need_tensors(state, specs):
+    """The kernels take raw pointers and trust the sizes of the plan, so a buffer of
+    the wrong size, type, layout or device is refused before any pointer is passed.
+    ``specs``: (tensor, name, dtype, shape) per buffer; sizes are checked for all
+    of them first, then devices."""
+    for t, name, dtype, shape in specs:
+        if not isinstance(t, torch.Tensor):
+            raise ValueError(f"{name} must be a torch tensor")
+        if t.dtype != dtype or tuple(t.shape) != shape:
+            raise ValueError(f"{name} must be {dtype} of shape {shape}, "
+                             f"got {t.dtype} {tuple(t.shape)}")
+        if not t.is_contiguous():
+            raise ValueError(f"{name} must be contiguous")
+    for t, name, _, _ in specs:
+        if not t.is_cuda or (state.device.index is not None
+                             and t.device.index != state.device.index):
+            raise ValueError(f"{name} must be on the plan's device {state.device}, got {t.device}")
+
+
 def evaluate_into(state, q_re, q_im, phi_out, field_out=None, precision=PREC_FP64, stream=None):
     """Allocation-free evaluate on device tensors (float64 charges, complex128 outputs).
 
     ``q_im`` may be None (real charges). ``stream`` is a torch.cuda.Stream or
     None (the current stream). Asynchronous; call ``check_errors`` to read the
-    device error flag.
+    device error flag. Raises ValueError, before launching anything, for a buffer
+    that is not a contiguous tensor of the plan's size and type on its device:
+    charges float64 (N,), ``phi_out`` complex128 (N,), ``field_out`` complex128 (N, 3).
     """
+    n = state.n
+    specs = [(q_re, "q_re", torch.float64, (n,)), (phi_out, "phi_out", torch.complex128, (n,))]
+    if q_im is not None:
+        specs.append((q_im, "q_im", torch.float64, (n,)))
+    if field_out is not None:
+        specs.append((field_out, "field_out", torch.complex128, (n, 3)))
+    _need_tensors(state, specs)
+    if int(precision) not in (PREC_FP64, PREC_MIXED):
+        raise ValueError("precision must be PREC_FP64 or PREC_MIXED")
     s = stream if stream is not None else torch.cuda.current_stream(state.device)
     _check(_lib.lib.hfmm_evaluate(
         state.handle, q_re.data_ptr(), None if q_im is None else q_im.data_ptr(),
@@ -319,7 +349,15 @@ def evaluate_field(state, charges, precision=PREC_FP64):
 def direct_at(state, q_re, q_im, targets, field=False, stream=None):
     """Device form of ``direct``: float64 charge tensors (``q_im`` may be None) and
     int32 target indices, all on the plan's device; returns device tensors
-    (phi (T,), E (T, 3) or None)."""
+    (phi (T,), E (T, 3) or None). The indices must lie in [0, N): they are read
+    on the device without a check (``direct`` checks them on the host)."""
+    if not isinstance(targets, torch.Tensor) or targets.ndim != 1:
+        raise ValueError("targets must be a 1-D torch tensor")
+    specs = [(q_re, "q_re", torch.float64, (state.n,)),
+             (targets, "targets", torch.int32, (targets.shape[0],))]
+    if q_im is not None:
+        specs.append((q_im, "q_im", torch.float64, (state.n,)))
+    _need_tensors(state, specs)
     m = targets.shape[0]
     dev = state.device
     phi = torch.empty(m, dtype=torch.complex128, device=dev)
@@ -335,13 +373,20 @@ def direct_at(state, q_re, q_im, targets, field=False, stream=None):
 def direct(state, charges, targets, field=False):
     """GPU direct sum sum_{s: r>0} q_s e^{ikr}/r (and -grad) at ``targets`` (indices),
     the referee of test.py:11-18. Returns NumPy complex arrays."""
+    tg_h = np.asarray(targets)
+    if tg_h.ndim != 1 or not (np.issubdtype(tg_h.dtype, np.integer) or tg_h.size == 0):
+        raise ValueError("targets must be a 1-D array of point indices")
+    if tg_h.size and (tg_h.min() < 0 or tg_h.max() >= state.n):
+        raise ValueError(f"targets must lie in [0, {state.n})")
+    if tuple(np.shape(charges)) != (state.n,):
+        raise ValueError(f"charges must have shape ({state.n},)")
     dev = state.device
     with torch.cuda.device(dev):
         q = torch.as_tensor(np.asarray(charges)).to(dev) if not isinstance(charges, torch.Tensor) \
             else charges.to(dev)
         q_re = q.real.to(torch.float64).contiguous() if q.is_complex() else q.to(torch.float64).contiguous()
         q_im = q.imag.to(torch.float64).contiguous() if q.is_complex() else None
-        tg = torch.as_tensor(np.asarray(targets, dtype=np.int32)).to(dev)
+        tg = torch.as_tensor(tg_h.astype(np.int32)).to(dev)
         phi = torch.empty(tg.shape[0], dtype=torch.complex128, device=dev)
         E = torch.empty((tg.shape[0], 3), dtype=torch.complex128, device=dev) if field else None
         s = torch.cuda.current_stream(dev)

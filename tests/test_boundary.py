@@ -78,3 +78,51 @@ def test_no_gpu_means_loud_failure():
         pytest.skip("a GPU is present")
     with pytest.raises(RuntimeError, match="CUDA"):
         hfmm_b200.setup(np.random.default_rng(0).uniform(size=(32, 3)), 1.0, p=3)
+
+
+def _fake_plan(n=4):
+    """Enough of a plan for the host-side checks, which run before any launch."""
+    import types
+    import torch
+    return types.SimpleNamespace(n=n, device=torch.device("cuda", 0), handle=None)
+
+
+@pytest.mark.parametrize("which,bad,msg", [
+    ("q_re", "float32", "float64"), ("q_re", "short", "shape"), ("q_im", "short", "shape"),
+    ("phi_out", "float64", "complex128"), ("field_out", "flat", "shape"),
+    ("phi_out", "strided", "contiguous"), ("q_re", "host", "device")])
+def test_evaluate_into_refuses_buffers_that_do_not_fit_the_plan(which, bad, msg):
+    """The kernels take raw pointers and trust the plan's sizes: a buffer of the
+    wrong type, size, layout or device is refused before any pointer is passed."""
+    import torch
+    import hfmm_b200
+    n = 4
+    bufs = dict(q_re=torch.zeros(n, dtype=torch.float64), q_im=torch.zeros(n, dtype=torch.float64),
+                phi_out=torch.zeros(n, dtype=torch.complex128),
+                field_out=torch.zeros((n, 3), dtype=torch.complex128))
+    if bad == "float32":
+        bufs[which] = torch.zeros(n, dtype=torch.float32)
+    elif bad == "short":
+        bufs[which] = torch.zeros(n - 1, dtype=torch.float64)
+    elif bad == "float64":
+        bufs[which] = torch.zeros(n, dtype=torch.float64)
+    elif bad == "flat":
+        bufs[which] = torch.zeros(3 * n, dtype=torch.complex128)
+    elif bad == "strided":
+        bufs[which] = torch.zeros(2 * n, dtype=torch.complex128)[::2]
+    with pytest.raises(ValueError, match=msg):
+        hfmm_b200.evaluate_into(_fake_plan(n), bufs["q_re"], bufs["q_im"], bufs["phi_out"],
+                                bufs["field_out"])
+
+
+@pytest.mark.parametrize("targets", [[0, 4], [-1], [[0, 1]], [0.5]])
+def test_direct_refuses_targets_outside_the_points(targets):
+    import hfmm_b200
+    with pytest.raises(ValueError, match="targets"):
+        hfmm_b200.direct(_fake_plan(4), np.zeros(4), np.asarray(targets))
+
+
+def test_direct_refuses_charges_of_another_size():
+    import hfmm_b200
+    with pytest.raises(ValueError, match="charges"):
+        hfmm_b200.direct(_fake_plan(4), np.zeros(5), np.array([0, 1]))
