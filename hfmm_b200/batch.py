@@ -63,6 +63,7 @@ class Batch:
         for i, (st, q) in enumerate(zip(self.states, charges)):
             if tuple(q.shape) != (st.n,):
                 raise ValueError(f"charges of problem {i} must have shape ({st.n},)")
+            q = q.to(st.device)                 # the graph reads them through device pointers
             if q.is_complex():
                 q_re, q_im = q.real.double().contiguous(), q.imag.double().contiguous()
             else:
@@ -80,6 +81,8 @@ class Batch:
             self.check_sums = torch.zeros((len(self.states), 4), dtype=torch.float64, device=dev)
             for i, (st, tg) in enumerate(zip(self.states, checks)):
                 tg = tg.to(device=dev, dtype=torch.int32).contiguous()
+                if tg.ndim != 1 or (tg.numel() and (int(tg.min()) < 0 or int(tg.max()) >= st.n)):
+                    raise ValueError(f"check targets of problem {i} must be indices in [0, {st.n})")
                 self._keep.append((tg,))
                 _check(_lib.lib.hfmm_batch_set_check(
                     self._h, i, st.positions.data_ptr(), tg.data_ptr(), tg.shape[0],

@@ -348,6 +348,8 @@ class AutoPlan:
                     raise ValueError(f"charges must have shape ({self.state.n},)")
                 q = _stage_charges(self, qn, np.iscomplexobj(qn), dev)
             else:
+                if tuple(charges.shape) != (self.state.n,):
+                    raise ValueError(f"charges must have shape ({self.state.n},)")
                 q = charges.to(dev)
             if q.is_complex():
                 q_re, q_im = q.real.double().contiguous(), q.imag.double().contiguous()
