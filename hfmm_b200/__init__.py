@@ -108,6 +108,17 @@ class HFMMState:
         _check(_lib.lib.hfmm_export_pil(self.handle, out.ctypes.data))
         return out
 
+    def densities(self, which, columns=1):
+        """Upward equivalent ("up", after P2M and M2M) or downward local ("down", after
+        M2L, P2L and L2L) densities of the last FP64 evaluate, which had ``columns``
+        charge columns: (n_families, n_boxes, columns, n_s) float64, the boxes of
+        levels 2..max_depth filled (hfmm_export_densities)."""
+        nf, nb, ns = self.n_families, self.info["n_boxes"], self.info["n_s"]
+        out = np.empty((nf, nb, int(columns), ns), np.float64)
+        _check(_lib.lib.hfmm_export_densities(self.handle, {"up": 0, "down": 1}[which],
+                                              int(columns), out.ctypes.data, out.size))
+        return out
+
     def pairs(self, which):
         """Interaction list as (len, 2) int32: 'V', 'U', 'W', 'X' or 'near'."""
         idx = {"V": 0, "U": 1, "W": 2, "X": 3, "near": 4}[which]

@@ -60,6 +60,7 @@ SIGNATURES = [
     ("hfmm_export_tree", _c_i32, [_c_vp] * 7),
     ("hfmm_export_pil", _c_i32, [_c_vp, _c_vp]),
     ("hfmm_export_list", _c_i32, [_c_vp, _c_i32, _c_vp, _c_i64]),
+    ("hfmm_export_densities", _c_i32, [_c_vp, _c_i32, _c_i32, _c_vp, _c_i64]),
     ("hfmm_direct", _c_i32, [_c_vp, _c_vp, _c_vp, _c_i64, _c_vp, _c_i64, _c_dbl, _c_vp, _c_vp,
                              _c_vp]),
     ("hfmm_direct_scratch_bytes", _c_i64, [_c_i64, _c_i64]),

@@ -1038,6 +1038,28 @@ int hfmm_export_list(const hfmm_plan* P, int32_t which, int32_t* pairs, int64_t 
     API_END
 }
 
+int hfmm_export_densities(const hfmm_plan* P, int32_t which, int32_t columns, double* out,
+                          int64_t cap) {
+    if (!P || !out) return fail(HFMM_ERR_ARG, "NULL argument");
+    if (!P->finalized) return fail(HFMM_ERR_STATE, "plan not finalized");
+    if (which != 0 && which != 1) return fail(HFMM_ERR_ARG, "which must be 0 (up) or 1 (down)");
+    if (columns != 1 && columns != 2) return fail(HFMM_ERR_ARG, "columns must be 1 or 2");
+    // [family][box][column][ld], the family stride being n_boxes x columns x ld (evaluate
+    // lays the arrays out for its own column count; finalize sized them for two columns)
+    const int64_t rows = (int64_t)P->n_fam * P->nb * columns;
+    if (cap < rows * P->n_s) return fail(HFMM_ERR_CAPACITY, "densities buffer too small");
+    API_BEGIN
+    HFMM_CUDA(cudaDeviceSynchronize());
+    std::vector<double> h((size_t)(rows * P->ld));
+    const DevBuf<double>& b = which == 0 ? P->equiv : P->loc;
+    if (rows)
+        HFMM_CUDA(cudaMemcpy(h.data(), b.p, h.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    for (int64_t r = 0; r < rows; ++r)
+        std::copy(h.data() + r * P->ld, h.data() + r * P->ld + P->n_s, out + r * P->n_s);
+    return HFMM_OK;
+    API_END
+}
+
 int64_t hfmm_direct_scratch_bytes(int64_t n, int64_t n_t) {
     if (n <= 0 || n_t < 0) return fail(HFMM_ERR_ARG, "invalid direct-sum sizes");
     return (int64_t)direct_splits(n, n_t) * std::max<int64_t>(n_t, 1) * 8 * (int64_t)sizeof(double);

@@ -143,6 +143,15 @@ int hfmm_export_tree(const hfmm_plan* plan, uint64_t* m_id, int32_t* p_id, int32
 int hfmm_export_pil(const hfmm_plan* plan, int32_t* pil);
 /* List `which` (0 = V, 1 = U, 2 = W, 3 = X, 4 = near pairs) as (len x 2) int32, host. */
 int hfmm_export_list(const hfmm_plan* plan, int32_t which, int32_t* pairs, int64_t cap);
+/* Densities left by the last HFMM_PREC_FP64 evaluate, for per-phase checks: which = 0
+ * the upward equivalent densities after P2M and M2M (phases.py:79-173), 1 the downward
+ * local densities after M2L, P2L and L2L (phases.py:176-280, 1709-1770), both for the
+ * boxes of levels 2..max_depth (other rows are 0). `columns` is that evaluate's charge
+ * columns (1 real, 2 complex). Host buffer of n_families x n_boxes x columns x n_s
+ * doubles, `cap` its capacity in doubles. Synchronises the device. The mixed path with a
+ * compressed M2L keeps scaled SVD coordinates in these arrays instead. */
+int hfmm_export_densities(const hfmm_plan* plan, int32_t which, int32_t columns, double* out,
+                          int64_t cap);
 
 /* ---- referee ---- */
 /* Direct sum phi_t = sum_{s: r>0} q_s e^{ikr}/r (test.py:11-18) at n_t targets

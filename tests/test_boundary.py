@@ -40,6 +40,7 @@ def test_null_arguments_rejected():
     h = ctypes.c_void_p()
     assert _lib.lib.hfmm_tree_build(None, 10, 16, 0, ctypes.byref(h)) == -1
     assert _lib.lib.hfmm_evaluate(None, None, None, None, None, 0, None) == -1
+    assert _lib.lib.hfmm_export_densities(None, 0, 1, None, 0) == -1
     assert b"NULL" in _lib.lib.hfmm_last_error() or _lib.lib.hfmm_last_error()
 
 
