@@ -356,6 +356,12 @@ def _lax_map(f, xs, batch_size=None):
 
 def _scan(f, init, xs=None, length=None, reverse=False, **_):
     n = length if xs is None else _lead_len(xs)
+    if n == 0:   # the stacked outputs' shapes come from one call, as tracing gives them
+        dummy = None if xs is None else tree_map(
+            lambda a: _wrap(np.zeros(np.asarray(a).shape[1:], np.asarray(a).dtype)), xs)
+        _, y = f(init, dummy)
+        return init, (None if y is None else tree_map(
+            lambda o: _wrap(np.empty((0,) + np.asarray(o).shape, np.asarray(o).dtype)), y))
     carry, ys = init, []
     order = range(n - 1, -1, -1) if reverse else range(n)
     for i in order:

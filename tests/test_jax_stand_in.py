@@ -87,3 +87,8 @@ def test_control_flow_stacks_like_jax():
 def test_map_over_nothing_keeps_the_element_shape():
     out = J._lax_map(lambda t: (t[0] * 2.0, t[1][:2]), (np.zeros((0, 3)), np.zeros((0, 4), np.int32)))
     assert out[0].shape == (0, 3) and out[1].shape == (0, 2) and out[1].dtype == np.int32
+
+
+def test_scan_over_nothing_returns_the_carry_and_empty_outputs():
+    carry, ys = J._scan(lambda c, x: (c + x.sum(), x * 2.0), 1.0, np.zeros((0, 3)))
+    assert carry == 1.0 and ys.shape == (0, 3)
