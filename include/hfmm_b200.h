@@ -69,6 +69,8 @@ typedef struct hfmm_info {
 int hfmm_tree_build(const double* pos_dev, int64_t n, int32_t n_max, int32_t max_depth,
                     hfmm_plan** out);
 
+/* The sizes the reference's setup dict carries (max_depth, maxleaf, max_boxes,
+ * domain_extent, pmin, list lengths: kifmm/setup.py:220-226, core.py:156-160). */
 int hfmm_plan_info(const hfmm_plan* plan, hfmm_info* out);
 
 /* Kernel: wavenumber k, p points per cube edge, n_families = 2 (cos and sin
@@ -129,9 +131,12 @@ int hfmm_evaluate(hfmm_plan* plan, const double* q_re_dev, const double* q_im_de
                   double* phi_out_dev, double* field_out_dev, int32_t precision,
                   void* stream);
 
-/* Read and clear the plan's device error flag (synchronises the stream). */
+/* Read and clear the plan's device error flag (synchronises the stream). No
+ * counterpart: the reference's XLA programs have no device error path. */
 int hfmm_plan_check(hfmm_plan* plan, void* stream);
 
+/* Free the plan and everything it owns (the reference's state dict is freed by
+ * Python's garbage collector, kifmm/setup.py:220-226). */
 void hfmm_plan_destroy(hfmm_plan* plan);
 
 /* ---- inspection (tests compare these with the oracle bit for bit) ---- */
