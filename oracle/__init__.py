@@ -9,11 +9,15 @@ measured or shipped.
 Pinning: the reference ships no golden vectors and JAX is not installed here,
 so the reference's own Python code was run on a NumPy stand-in for the JAX calls
 it makes (tests/golden/jax_on_numpy.py, tests/golden/make_golden.py) and its
-outputs committed as fixtures (tests/golden/*.npz, tests/golden/edge/*.npz).
-The oracle matches them bit for bit on every integer array (tree, sort order,
-particles-in-leaf, U/V/W/X/near lists, buffer sizes) and to the rounding floor
-on potentials and fields (tests/test_golden.py). It also passes the reference's
-known-answer checks (test.py:63-72) and an O(N^2) direct sum.
+outputs committed as fixtures: standard and edge cases (tests/golden/*.npz,
+tests/golden/edge/), the 2e4-point CPU-runnable configuration (tests/golden/c1/),
+the reference's test.py grid (tests/golden/grid/) and per-phase outputs
+(tests/golden/phases/). The oracle matches them bit for bit on every integer
+array (tree, sort order, particles-in-leaf, U/V/W/X/near lists, buffer sizes),
+phase by phase through the potential each density makes on its check surface,
+and to the rounding floor on potentials and fields (tests/test_golden.py,
+tests/test_oracle_known_answers.py). It also passes the reference's known-answer
+checks (test.py:63-72) and an O(N^2) direct sum.
 """
 
 from .surfaces import n_surf, surface_pts, R_EQUIV, R_CHECK
