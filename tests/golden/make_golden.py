@@ -25,6 +25,7 @@ Needs the reference source tree (default /root/reference, or argument
     python tests/golden/make_golden.py [--reference DIR] --grid
     python tests/golden/make_golden.py [--reference DIR] --phases
     python tests/golden/make_golden.py [--reference DIR] --c1
+    python tests/golden/make_golden.py [--reference DIR] --errors
 
 The inputs are the seeded clouds of tests/cases.py.
 """
@@ -284,6 +285,51 @@ def run_c1(HFMM, seen, folder):
     np.savez_compressed(os.path.join(folder, "c1_n20000_k2pi_p8.npz"), **out)
 
 
+# Invalid inputs of HFMM.setup / HFMM.evaluate (HFMM.py:14-16, 57-64, 86-87).
+def _error_cases():
+    good = np.random.default_rng(0).uniform(size=(64, 3))
+    bad_pos = {"empty": np.zeros((0, 3)), "two_columns": np.zeros((4, 2)),
+               "nan": np.array([[0.0, 0.0, np.nan]]), "inf": np.array([[0.0, np.inf, 0.0]]),
+               "one_dim": np.zeros(3)}
+    cases = {f"positions_{n}": dict(positions=x) for n, x in bad_pos.items()}
+    for name, kw in (("p_1", dict(p=1)), ("p_2.5", dict(p=2.5)), ("p_0", dict(p=0)),
+                     ("N_max_0", dict(N_max=0)), ("N_max_2.5", dict(N_max=2.5)),
+                     ("max_depth_0", dict(max_depth=0)), ("max_depth_1.5", dict(max_depth=1.5)),
+                     ("max_depth_-1", dict(max_depth=-1)),
+                     ("k_nan", dict(k=np.nan)), ("k_inf", dict(k=np.inf)),
+                     ("k_-inf", dict(k=-np.inf))):
+        cases[name] = kw
+    return good, cases
+
+
+def run_errors(HFMM, folder):
+    """Which exception the reference raises for each invalid input (none of them
+    reaches the tree build), and for invalid charges on a small valid state."""
+    import json
+    good, cases = _error_cases()
+    out = {}
+    for name, kw in cases.items():
+        args = dict(positions=good, k=1.0, p=3, N_max=16, max_depth=None)
+        args.update(kw)
+        try:
+            HFMM.setup(args.pop("positions"), args.pop("k"), **args)
+            out[name] = None
+        except Exception as e:          # the type is the record
+            out[name] = type(e).__name__
+    state = HFMM.setup(good, 1.0, p=2, N_max=16)
+    for name, q in (("charges_complex", np.ones(64) + 1j), ("charges_short", np.ones(63)),
+                    ("charges_two_columns", np.ones((64, 2)))):
+        try:
+            HFMM.evaluate(state, q)
+            out[name] = None
+        except Exception as e:
+            out[name] = type(e).__name__
+    os.makedirs(folder, exist_ok=True)
+    with open(os.path.join(folder, "reference_errors.json"), "w") as f:
+        json.dump(out, f, indent=1, sort_keys=True)
+    print(out)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
@@ -294,9 +340,13 @@ def main():
                     help="per-phase outputs of one adaptive case, into phases/")
     ap.add_argument("--c1", action="store_true",
                     help="the 2e4-point CPU-runnable configuration, into c1/")
+    ap.add_argument("--errors", action="store_true",
+                    help="the exceptions of invalid inputs, into errors/")
     ap.add_argument("cases", nargs="*")
     a = ap.parse_args()
     HFMM, seen = load_reference(a.reference)
+    if a.errors:
+        return run_errors(HFMM, os.path.join(HERE, "errors"))
     if a.c1:
         return run_c1(HFMM, seen, os.path.join(HERE, "c1"))
     if a.phases:

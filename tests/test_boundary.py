@@ -127,3 +127,40 @@ def test_direct_refuses_charges_of_another_size():
     import hfmm_b200
     with pytest.raises(ValueError, match="charges"):
         hfmm_b200.direct(_fake_plan(4), np.zeros(5), np.array([0, 1]))
+
+
+def _golden_module():
+    import importlib.util
+    path = os.path.join(ROOT, "tests", "golden", "make_golden.py")
+    spec = importlib.util.spec_from_file_location("make_golden", path)
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def test_invalid_inputs_raise_what_the_reference_raises():
+    """Each invalid input of tests/golden/make_golden.py's error cases raises, from
+    setup / evaluate here, the exception the reference's own HFMM.setup /
+    HFMM.evaluate raised for it (tests/golden/errors/reference_errors.json,
+    recorded by running the reference's code), before any device is touched."""
+    import json
+    import hfmm_b200
+    with open(os.path.join(ROOT, "tests", "golden", "errors", "reference_errors.json")) as f:
+        ref = json.load(f)
+    good, cases = _golden_module()._error_cases()
+    assert set(cases) | {"charges_complex", "charges_short", "charges_two_columns"} == set(ref)
+    for name, kw in cases.items():
+        args = dict(positions=good, k=1.0, p=3, N_max=16, max_depth=None)
+        args.update(kw)
+        with pytest.raises(Exception) as e:
+            hfmm_b200.setup(**args)
+        assert type(e.value).__name__ == ref[name], name
+
+    class Plan:                     # the charge checks run before any device work
+        n = 64
+        device = None
+    for name, q in (("charges_complex", np.ones(64) + 1j), ("charges_short", np.ones(63)),
+                    ("charges_two_columns", np.ones((64, 2)))):
+        with pytest.raises(Exception) as e:
+            hfmm_b200.evaluate(Plan(), q)
+        assert type(e.value).__name__ == ref[name], name
