@@ -39,6 +39,7 @@ def load(path):
 
 
 @pytest.mark.parametrize("path", GOLD + EDGE, ids=[os.path.basename(p)[:-4] for p in GOLD + EDGE])
+@pytest.mark.filterwarnings("ignore:invalid value encountered in divide:RuntimeWarning")  # tiny1
 def test_oracle_reproduces_golden(path):
     g = load(path)
     md = int(g["max_depth"])
