@@ -58,3 +58,37 @@ def test_cuda_path_matches_the_reference(path):
         assert O.relative_error(phi, g["phi"]) < tol
     finally:
         st.close()
+
+
+C1 = os.path.join(os.path.dirname(__file__), "golden", "c1", "c1_n20000_k2pi_p8.npz")
+
+
+def test_cuda_path_matches_the_reference_at_the_cpu_runnable_configuration():
+    """20 000 uniform points, complex N(0, 1) charges (seeded 42 + N), k = 2 pi, p = 8,
+    leaf size 64: tree and lists equal to the reference's; potential and field on
+    its 1024 sampled targets to 1e-12 (the oracle is within 2.5e-13 of it)."""
+    import hfmm_b200
+    with np.load(C1) as z:
+        g = {k: z[k] for k in z.files}
+    n = 20_000
+    rng = np.random.default_rng(42 + n)
+    pos = rng.uniform(0.0, 1.0, (n, 3))
+    q = rng.normal(size=n) + 1j * rng.normal(size=n)
+    assert pos.sum() == g["positions_sum"] and q.sum() == g["charges_sum"]
+    st = hfmm_b200.setup(pos, float(g["k"]), p=int(g["p"]), N_max=int(g["N_max"]))
+    try:
+        assert st.info["max_depth"] == int(g["realised_depth"])
+        assert st.info["max_boxes"] == int(g["max_boxes"])
+        assert st.info["maxleaf"] == int(g["maxleaf"])
+        t = st.tree()
+        for key in ("m_id", "p_id", "lvls", "counts", "is_leaf"):
+            assert np.array_equal(t[key], g[key]), key
+        assert np.array_equal(t["sort_idx"], g["sort_idx"])
+        for key in ("V", "U", "near"):
+            assert np.array_equal(st.pairs(key), g[key]), key
+        phi, E = hfmm_b200.evaluate_field(st, q)
+        s = g["sample"]
+        assert O.relative_error(phi[s], g["phi"]) < 1e-12
+        assert O.relative_error(E[s], g["E"]) < 1e-12
+    finally:
+        st.close()
