@@ -26,10 +26,12 @@ Needs the reference source tree (default /root/reference, or argument
     python tests/golden/make_golden.py [--reference DIR] --phases
     python tests/golden/make_golden.py [--reference DIR] --c1
     python tests/golden/make_golden.py [--reference DIR] --errors
+    python tests/golden/make_golden.py [--reference DIR] --tables
 
 The inputs are the seeded clouds of tests/cases.py.
 """
 import argparse
+import hashlib
 import os
 import sys
 import time
@@ -330,6 +332,63 @@ def run_errors(HFMM, folder):
     print(out)
 
 
+# Operator tables (kifmm/operators.py:572-641): (p, max_depth, domain extent, k).
+TABLE_CASES = ((3, 3, 0.97, 2.0), (5, 2, 1.3, 7.5))
+TABLE_KEYS = ("equiv_pts", "check_pts", "M2M_K_lv", "L2L_K_lv", "M2L_K_lv")
+
+
+def table_digest(a):
+    a = np.ascontiguousarray(np.asarray(a))
+    return f"{a.dtype.str} {a.shape} " + hashlib.sha256(a.tobytes()).hexdigest()
+
+
+def table_arrays(t):
+    """name -> array of one leveled table set (the reference's dict or the oracle's)."""
+    arrs = {key: np.asarray(t[key]) for key in TABLE_KEYS}
+    for key in ("F_up_lv", "F_dn_lv"):
+        for i, part in enumerate(("U", "d", "Vt")):
+            arrs[f"{key}.{part}"] = np.asarray(t[key][i])
+    return arrs
+
+
+def table_summary(a, n_samples=64):
+    """Digest, Frobenius norm and seeded sample entries of one table."""
+    flat = np.ascontiguousarray(a).ravel()
+    idx = np.random.default_rng(flat.size).choice(flat.size, min(n_samples, flat.size),
+                                                  replace=False)
+    return dict(digest=table_digest(a), norm=float(np.linalg.norm(flat)),
+                idx=idx.tolist(), values=flat[idx].tolist())
+
+
+def run_tables(HFMM, folder):
+    """Every per-level table the reference's build_operators_leveled makes
+    (surfaces, damped-SVD factors U, d, Vt up and down, M2M, L2L and M2L kernel
+    matrices) for both kernel components (eps_rel 1e-7 and 1e-12, HFMM.py:65-77):
+    digest, norm and sample entries, and whether the oracle's tables were
+    bit-identical on the machine that ran this (the SVD and libm bits may differ
+    on another CPU, so the tests compare samples and norms)."""
+    import json
+    from jaxfmm.kifmm.operators import build_operators_leveled
+    sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+    import oracle as O
+    out = {}
+    for (p, md, ext, k) in TABLE_CASES:
+        for imaginary, eps in ((False, 1e-7), (True, 1e-12)):
+            t = table_arrays(build_operators_leveled(
+                p, md, ext, HFMM.helmholtz_component(k, imaginary), eps_rel=eps))
+            mine = table_arrays(O.build_operators_leveled(
+                p, md, ext, O.helmholtz_G_np(k, imaginary), eps_rel=eps))
+            d = {name: table_summary(a) for name, a in t.items()}
+            d["oracle_bit_identical_when_made"] = all(
+                mine[name].shape == a.shape and np.array_equal(mine[name], a)
+                for name, a in t.items())
+            out[f"p{p}_md{md}_ext{ext}_k{k}_{'sin' if imaginary else 'cos'}"] = d
+    os.makedirs(folder, exist_ok=True)
+    with open(os.path.join(folder, "reference_table_digests.json"), "w") as f:
+        json.dump(out, f, indent=1, sort_keys=True)
+    print(len(out), "table sets")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
@@ -342,9 +401,13 @@ def main():
                     help="the 2e4-point CPU-runnable configuration, into c1/")
     ap.add_argument("--errors", action="store_true",
                     help="the exceptions of invalid inputs, into errors/")
+    ap.add_argument("--tables", action="store_true",
+                    help="digests of the operator tables, into tables/")
     ap.add_argument("cases", nargs="*")
     a = ap.parse_args()
     HFMM, seen = load_reference(a.reference)
+    if a.tables:
+        return run_tables(HFMM, os.path.join(HERE, "tables"))
     if a.errors:
         return run_errors(HFMM, os.path.join(HERE, "errors"))
     if a.c1:

@@ -161,3 +161,51 @@ def test_oracle_matches_the_reference_at_the_cpu_runnable_configuration():
     sample = g["sample"]
     assert O.relative_error(phi[sample], g["phi"]) < TOL
     assert O.relative_error(E[sample], g["E"]) < TOL
+
+
+TABLES = os.path.join(os.path.dirname(__file__), "golden", "tables", "reference_table_digests.json")
+
+
+def test_oracle_tables_match_the_reference():
+    """The per-level operator tables (kifmm/operators.py:572-641) of the oracle against
+    the reference's own build_operators_leveled, two configurations, both kernel
+    components. Where the fixture was made all of them were bit-identical (recorded
+    in it). Here, where LAPACK and libm may be other builds, the check is: surfaces
+    bit for bit (pure arithmetic); kernel matrices on seeded samples to 1e-14 of the
+    largest; the damped singular values to 1e-12 of the largest; the singular
+    vectors by shape and norm (they are arbitrary within degenerate subspaces)."""
+    import json
+    with open(TABLES) as f:
+        ref = json.load(f)
+    mg = _golden_module()
+    assert len(ref) == 2 * len(mg.TABLE_CASES)
+    for (p, md, ext, k) in mg.TABLE_CASES:
+        for imaginary, eps in ((False, 1e-7), (True, 1e-12)):
+            r = ref[f"p{p}_md{md}_ext{ext}_k{k}_{'sin' if imaginary else 'cos'}"]
+            assert r["oracle_bit_identical_when_made"]
+            mine = mg.table_arrays(O.build_operators_leveled(p, md, ext, O.helmholtz_G_np(k, imaginary),
+                                                             eps_rel=eps))
+            for name, a in mine.items():
+                want = r[name]
+                dtype, shape = want["digest"].split(" ", 1)[0], want["digest"].split(" ", 1)[1].rsplit(" ", 1)[0]
+                assert a.dtype.str == dtype and str(a.shape) == shape, name
+                got = np.ascontiguousarray(a).ravel()[want["idx"]]
+                vals = np.asarray(want["values"])
+                if name in ("equiv_pts", "check_pts"):
+                    assert mg.table_digest(a) == want["digest"], name
+                elif name.endswith(".U") or name.endswith(".Vt"):
+                    assert abs(np.linalg.norm(a) - want["norm"]) <= 1e-12 * want["norm"], name
+                elif name.endswith(".d"):
+                    assert np.abs(got - vals).max() <= 1e-12 * np.abs(vals).max(), name
+                else:
+                    assert np.abs(got - vals).max() <= 1e-14 * np.abs(vals).max(), name
+                    assert abs(np.linalg.norm(a) - want["norm"]) <= 1e-13 * want["norm"], name
+
+
+def _golden_module():
+    import importlib.util
+    path = os.path.join(os.path.dirname(__file__), "golden", "make_golden.py")
+    spec = importlib.util.spec_from_file_location("make_golden", path)
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
