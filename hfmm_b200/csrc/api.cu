@@ -921,7 +921,7 @@ int hfmm_plan_check(hfmm_plan* P, void* stream) {
         HFMM_CUDA(cudaMemsetAsync(P->d_err.p, 0, sizeof(int), (cudaStream_t)stream));
         HFMM_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
         return fail(HFMM_ERR_DEVICE, "device error flag " + std::to_string(v) +
-                                         " (1 = index out of bounds, 2 = capacity)");
+                                         " (1 = index out of bounds, 2 = capacity, 4 = a bounded wait timed out)");
     }
     return HFMM_OK;
     API_END

@@ -30,8 +30,14 @@
 // 512 columns. The FP64 sums are stored as the check potentials. (Folding every
 // 4 k-chunks instead was 22 % faster but doubled the M2L error: 8.3e-7 against
 // 4.6e-7 for the potential at p = 8.)
-// Every mbarrier wait is bounded (2 s of %globaltimer); a timeout sets the
-// device error flag and every role drains and exits, TMEM is freed.
+// Every mbarrier wait is bounded (2 s of %globaltimer by default); a timeout sets
+// the CTA's abort flag and the device error flag, and every role stops issuing.
+// Before TMEM is freed and the CTA exits, nothing it issued may still be in flight:
+// the TMA thread waits for the bytes of every stage it loaded (their own tx-only
+// barriers, so the wait does not depend on the other roles), the MMA thread commits
+// its issued MMAs to a drain barrier and waits for it, and the gather threads wait
+// for their own copies. These drain waits ignore the abort flag and are bounded by
+// time only.
 #include "hfmm_internal.cuh"
 #include "mixed.cuh"
 
@@ -101,18 +107,28 @@ __device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
         : "memory");
     return ok != 0;
 }
-// Bounded wait: false on timeout or when another role has aborted.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int* abort_flag) {
+// Bounded wait: false on timeout (which sets the abort flag) or when another role
+// has aborted.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int* abort_flag,
+                                          uint64_t limit_ns) {
     if (mbar_try(bar, parity)) return true;
     const uint64_t t0 = gtimer();
     while (true) {
         if (mbar_try(bar, parity)) return true;
         if (*abort_flag) return false;
-        if (gtimer() - t0 > WAIT_NS) {
+        if (gtimer() - t0 > limit_ns) {
             *abort_flag = 1;
             return false;
         }
     }
+}
+// Drain wait: for work this thread has already issued, so it ignores the abort flag;
+// bounded by time only.
+__device__ __forceinline__ bool mbar_drain(uint32_t bar, uint32_t parity, uint64_t limit_ns) {
+    const uint64_t t0 = gtimer();
+    while (!mbar_try(bar, parity))
+        if (gtimer() - t0 > limit_ns) return false;
+    return true;
 }
 __device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, bool valid) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(dst), "l"(src),
@@ -212,7 +228,8 @@ constexpr uint32_t IDESC = idesc_m(BM);
 constexpr uint32_t IDESC64 = idesc_m(64);
 
 struct __align__(8) Ctl {
-    uint64_t full[STAGES];
+    uint64_t full[STAGES];   // the gather threads' copies of a stage have landed
+    uint64_t tfull[STAGES];  // the stage's TMA bytes have landed (tx-only)
     uint64_t empty[STAGES];
     uint64_t acc_full[2];    // a unit's FP32 sum is complete in buffer b (MMA commit)
     uint64_t acc_empty[2];   // buffer b has been folded into the FP64 sum (one per fold warp)
@@ -237,6 +254,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_m2l_tf32x3(const __grid_constant
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int tile = blockIdx.x, m0 = blockIdx.y * BM, fam = blockIdx.z;
     volatile int* abort_flag = &ctl.abort_flag;
+    const uint64_t wait_ns = c.wait_ns ? c.wait_ns : WAIT_NS;
     const bool half = (c.m_valid > 0 ? c.m_valid : c.ldm) - m0 <= 64;
     const uint32_t idesc = half ? IDESC64 : IDESC;
 
@@ -256,8 +274,9 @@ __global__ void __launch_bounds__(THREADS, 1) k_m2l_tf32x3(const __grid_constant
     if (tid == 0) {
         ctl.abort_flag = 0;
         for (int s = 0; s < STAGES; ++s) {
-            mbar_init(smem_u32(&ctl.full[s]), 1 + 128);   // TMA arrive + each gather thread's copies
-            mbar_init(smem_u32(&ctl.empty[s]), 1);       // MMA commit
+            mbar_init(smem_u32(&ctl.full[s]), 128);   // each gather thread's copies
+            mbar_init(smem_u32(&ctl.tfull[s]), 1);    // the TMA thread's arrive + its bytes
+            mbar_init(smem_u32(&ctl.empty[s]), 1);    // MMA commit
         }
         for (int b = 0; b < 2; ++b) {
             mbar_init(smem_u32(&ctl.acc_full[b]), 1);
@@ -372,7 +391,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_m2l_tf32x3(const __grid_constant
                 }
                 if (ai + 1 < n_act) load_sources(ai + 1);
             }
-            if (!mbar_wait(smem_u32(&ctl.empty[st]), ((q / STAGES) & 1) ^ 1, abort_flag)) break;
+            if (!mbar_wait(smem_u32(&ctl.empty[st]), ((q / STAGES) & 1) ^ 1, abort_flag, wait_ns)) break;
             const int k0 = (q % kch) * BK;
             const uint32_t sbh = smem_u32(sm + st * STAGE_BYTES + 2 * TILE_BYTES);
             const uint32_t sbl = sbh + TILE_BYTES;
@@ -385,11 +404,15 @@ __global__ void __launch_bounds__(THREADS, 1) k_m2l_tf32x3(const __grid_constant
             }
             // the stage's barrier counts this thread's arrival when its copies have
             // landed: no thread waits for its own copies, so every stage can be in flight
-            asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(
-                             smem_u32(&ctl.full[st]))
-                         : "memory");
+            // (c.starve: a test leaves stage 0 without its arrivals, so the MMA thread's
+            // bounded wait runs out)
+            if (!(c.starve && q == 0))
+                asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(
+                                 smem_u32(&ctl.full[st]))
+                             : "memory");
         }
-        asm volatile("cp.async.wait_all;\n" ::);
+        // drain: this thread's copies (and the arrivals they trigger) complete
+        asm volatile("cp.async.wait_all;\n" ::: "memory");
     } else if (warp >= 6) {
         // ---------------- fold entries into the FP64 sums; store at the end
         // Warp w may touch TMEM lanes 32 (w % 4) .. + 31 only: the NFW fold warps
@@ -406,7 +429,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_m2l_tf32x3(const __grid_constant
         for (int i = 0; i < n_units && ok; ++i) {
             const int b = i & 1;
             // the TMEM loads below are warp-collective: agree on the wait's outcome
-            const bool got = mbar_wait(smem_u32(&ctl.acc_full[b]), (i >> 1) & 1, abort_flag);
+            const bool got = mbar_wait(smem_u32(&ctl.acc_full[b]), (i >> 1) & 1, abort_flag, wait_ns);
             if (!__all_sync(0xffffffffu, got)) {
                 ok = false;
                 break;
@@ -463,13 +486,16 @@ __global__ void __launch_bounds__(THREADS, 1) k_m2l_tf32x3(const __grid_constant
             const CUtensorMap* ml = &maps.a_lo[fam];
             const CUtensorMap* lh = &maps.l_hi[fam];
             const CUtensorMap* ll = &maps.l_lo[fam];
+            int last_q[STAGES];   // the last q loaded into each stage (-1: none)
+#pragma unroll
+            for (int st = 0; st < STAGES; ++st) last_q[st] = -1;
             for (int q = 0; q < nq; ++q) {
                 const int st = q % STAGES;
-                if (!mbar_wait(smem_u32(&ctl.empty[st]), ((q / STAGES) & 1) ^ 1, abort_flag)) break;
+                if (!mbar_wait(smem_u32(&ctl.empty[st]), ((q / STAGES) & 1) ^ 1, abort_flag, wait_ns)) break;
                 const int e = ctl.act[q / kch];
                 const int z = ctl.zidx[q / kch];
                 const int k0 = (q % kch) * BK;
-                const uint32_t fb = smem_u32(&ctl.full[st]);
+                const uint32_t fb = smem_u32(&ctl.tfull[st]);
                 const uint32_t sa = smem_u32(sm + st * STAGE_BYTES);
                 mbar_arrive_tx(fb, 2 * TILE_BYTES);
                 if (e < N_DISP) {
@@ -479,24 +505,36 @@ __global__ void __launch_bounds__(THREADS, 1) k_m2l_tf32x3(const __grid_constant
                     tma_load_3d(sa, lh, k0, m0, z, fb);
                     tma_load_3d(sa + TILE_BYTES, ll, k0, m0, z, fb);
                 }
+#pragma unroll
+                for (int j = 0; j < STAGES; ++j)
+                    if (j == st) last_q[j] = q;
             }
+            // drain: every stage's last load has landed (earlier loads of a stage were
+            // consumed by the MMA thread before the stage was loaded again)
+            bool drained = true;
+#pragma unroll
+            for (int j = 0; j < STAGES; ++j)
+                if (last_q[j] >= 0)
+                    drained &= mbar_drain(smem_u32(&ctl.tfull[j]), (last_q[j] / STAGES) & 1, wait_ns);
+            if (!drained) atomicOr(c.err, ERRF_TIMEOUT);
         }
     } else {
         // ---------------- MMA issue (warp 5, one lane)
         if (lane == 0) {
-            bool ok = true;
+            bool ok = true, issued = false;
             for (int q = 0; q < nq && ok; ++q) {
                 const int st = q % STAGES;
                 const int unit = q / FOLD, uq = q % FOLD;
                 const int b = unit & 1;
                 if (uq == 0 && unit >= 2) {   // buffer b must have been folded (unit - 2)
-                    if (!mbar_wait(smem_u32(&ctl.acc_empty[b]), ((unit >> 1) & 1) ^ 1, abort_flag)) {
+                    if (!mbar_wait(smem_u32(&ctl.acc_empty[b]), ((unit >> 1) & 1) ^ 1, abort_flag, wait_ns)) {
                         ok = false;
                         break;
                     }
                     asm volatile("tcgen05.fence::after_thread_sync;");
                 }
-                if (!mbar_wait(smem_u32(&ctl.full[st]), (q / STAGES) & 1, abort_flag)) {
+                if (!mbar_wait(smem_u32(&ctl.full[st]), (q / STAGES) & 1, abort_flag, wait_ns) ||
+                    !mbar_wait(smem_u32(&ctl.tfull[st]), (q / STAGES) & 1, abort_flag, wait_ns)) {
                     ok = false;
                     break;
                 }
@@ -516,14 +554,18 @@ __global__ void __launch_bounds__(THREADS, 1) k_m2l_tf32x3(const __grid_constant
                     umma_tf32(dt, ah + d, bl + d, idesc, 1u);
                     umma_tf32(dt, al + d, bh + d, idesc, 1u);
                 }
+                issued = true;
                 umma_commit(smem_u32(&ctl.empty[st]));
                 if (uq == FOLD - 1 || q == nq - 1) umma_commit(smem_u32(&ctl.acc_full[b]));
             }
-            if (ok && nq > 0) umma_commit(smem_u32(&ctl.done));
+            // drain, on every exit path: the commit tracks every MMA this thread issued
+            if (issued) {
+                umma_commit(smem_u32(&ctl.done));
+                if (!mbar_drain(smem_u32(&ctl.done), 0, wait_ns)) atomicOr(c.err, ERRF_TIMEOUT);
+            }
         }
     }
-    // drain: nothing may be in flight into shared or tensor memory when the CTA exits
-    if (warp == 5 && lane == 0 && nq > 0 && *abort_flag) mbar_wait(smem_u32(&ctl.done), 0, abort_flag);
+    // nothing this CTA issued is in flight into shared or tensor memory from here on
     asm volatile("tcgen05.fence::before_thread_sync;");
     __syncthreads();
     if (warp == 5) {
@@ -620,11 +662,16 @@ void split_transpose_tables(const double* at, float* hi, float* lo, int ld, int 
     HFMM_LAUNCH(k_split_transpose, grid, dim3(32, 8), 0, 0, at, hi, lo, ld);
 }
 
+uint64_t g_m2l_wait_ns = 0;
+int g_m2l_starve = 0;
+
 size_t m2l_tf32x3_smem() { return (size_t)STAGES * STAGE_BYTES + sizeof(Ctl) + 1024; }
 
 void m2l_tf32x3(const MixedMaps& maps, const MixedCall& call, cudaStream_t s) {
     if (call.ntiles == 0) return;
     MixedCall c = call;
+    c.wait_ns = g_m2l_wait_ns;
+    c.starve = g_m2l_starve;
     if (!c.ldk) c.ldk = c.ld;
     if (!c.ldm) c.ldm = c.ld;
     if (c.ldk % BK || c.ldm % BK)
@@ -641,3 +688,9 @@ void m2l_tf32x3(const MixedMaps& maps, const MixedCall& call, cudaStream_t s) {
 }
 
 }  // namespace hfmm
+
+extern "C" int hfmm_debug_m2l_wait(uint64_t wait_ns, int starve) {
+    hfmm::g_m2l_wait_ns = wait_ns;
+    hfmm::g_m2l_starve = starve ? 1 : 0;
+    return HFMM_OK;
+}

@@ -30,7 +30,14 @@ struct MixedCall {
     int64_t fam_stride, out_fam_stride, nb;
     int64_t src_lo, src_hi;        // valid source boxes [src_lo, src_hi) (0, nb when unset)
     int* err;
+    uint64_t wait_ns;              // limit of each bounded wait (0: 2 s); set by m2l_tf32x3
+    int starve;                    // test only: leave stage 0 without its gather arrivals
 };
+
+// Wait limit and starvation switch of the next M2L launches (hfmm_debug_m2l_wait):
+// a test makes a bounded wait run out on purpose and checks the error status.
+extern uint64_t g_m2l_wait_ns;
+extern int g_m2l_starve;
 
 void make_table_map(CUtensorMap* map, const float* base, int ld, int count, int ldm = 0);
 void split_tf32(const double* src, float* hi, float* lo, int64_t n, cudaStream_t s);

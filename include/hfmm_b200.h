@@ -139,6 +139,15 @@ int hfmm_plan_check(hfmm_plan* plan, void* stream);
  * Python's garbage collector, kifmm/setup.py:220-226). */
 void hfmm_plan_destroy(hfmm_plan* plan);
 
+/* Failure-path test hook of the mixed M2L kernel (process-wide; applies to the
+ * launches that follow). wait_ns: the limit of each of its bounded mbarrier
+ * waits (0 restores the default, 2 s). starve != 0 leaves the first operand
+ * stage of every CTA without its gather arrivals, so a wait runs out: the kernel
+ * then drains what it issued, frees its tensor memory, sets the timeout flag (4)
+ * that hfmm_plan_check reports as HFMM_ERR_DEVICE, and returns. No counterpart
+ * in the reference (XLA programs have no device error path). */
+int hfmm_debug_m2l_wait(uint64_t wait_ns, int starve);
+
 /* ---- inspection (tests compare these with the oracle bit for bit) ---- */
 /* Tree arrays of the active boxes: m_id (uint64), p_id, lvls, counts (int32),
  * is_leaf (uint8), each of length n_boxes; sort_idx (int32, n). Host buffers. */
@@ -178,12 +187,15 @@ int hfmm_direct_async(const double* pos_dev, const double* q_re_dev, const doubl
                       int64_t scratch_bytes, int* err_dev, void* stream);
 
 /* Same result as hfmm_direct without allocating anything, for callers that
- * cannot allocate device memory (a JAX/XLA process that owns the GPU memory, a
- * stream under CUDA-graph capture). No counterpart in the reference. The partial
+ * cannot allocate device memory (a JAX/XLA process whose allocator owns the GPU
+ * memory and runs foreign code inside that budget). No counterpart in the
+ * reference. The partial
  * sums live in a fixed 8 MiB device array inside this library, so n_t is limited
  * to 131072 targets (HFMM_ERR_CAPACITY above that). The first call on a device
- * looks up that array's address; make it before any stream capture. All calls
- * share the array: calls that overlap on the GPU race. Synchronises `stream`. */
+ * looks up that array's address (a one-time set-up on that device). All calls
+ * share the array: calls that overlap on the GPU race. An out-of-range target
+ * index gives HFMM_ERR_ARG; the error word is cleared at the start of every
+ * call. Synchronises `stream`. */
 int hfmm_direct_noalloc(const double* pos_dev, const double* q_re_dev, const double* q_im_dev,
                         int64_t n, const int32_t* targets_dev, int64_t n_t, double k,
                         double* phi_out_dev, double* field_out_dev, void* stream);
