@@ -2,17 +2,18 @@
 //
 // Some callers cannot allocate device memory while they run: a JAX/XLA program
 // (the reference's own runtime) preallocates most of the GPU for its allocator
-// and calls foreign code inside that budget, and a stream that is being captured
-// into a CUDA graph must not see cudaMalloc/cudaFree. hfmm_direct allocates its
-// partial-sum scratch per call, so this variant keeps the scratch in a fixed
-// file-scope device array instead.
+// and calls foreign code inside that budget, where a cudaMalloc can fail or
+// fragment memory the host framework owns. hfmm_direct allocates its partial-sum
+// scratch per call, so this variant keeps the scratch in a fixed file-scope
+// device array instead.
 //
 // The array is NOALLOC_SCRATCH_DOUBLES doubles (8 MiB). It is part of this
 // library's device image, so every GPU that loads the library holds it until the
 // process exits. Every call shares it and it keeps the last call's contents:
 // calls that overlap on the GPU (two streams, two threads) race on it. The
 // partial sums are fully written before they are read, so only the error word is
-// cleared per call.
+// cleared per call. The call waits for its stream to finish (it reads the error
+// word back), like hfmm_direct.
 #include "hfmm_internal.cuh"
 
 #include <algorithm>
@@ -24,7 +25,7 @@ constexpr size_t NOALLOC_SCRATCH_DOUBLES = (size_t)1 << 20;   // 8 MiB
 constexpr int MAX_DEVICES = 64;
 
 __device__ __align__(256) double g_noalloc_scratch[NOALLOC_SCRATCH_DOUBLES];
-__device__ __align__(256) int g_noalloc_err[64];
+__device__ __align__(256) int g_noalloc_err;
 
 // Device addresses of the two arrays, looked up once per device with that device
 // current. In host code the symbols are host-side stand-ins, never valid device

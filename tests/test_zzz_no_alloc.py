@@ -1,8 +1,8 @@
 """The allocation-free direct-sum entry point, hfmm_direct_noalloc.
 
-It serves callers that cannot allocate device memory mid-run (a JAX/XLA process
-whose allocator owns the GPU, a stream under CUDA-graph capture): its scratch is
-a fixed device array inside the library. Through the C ABI it must give the same
+It serves callers that cannot allocate device memory mid-run (code running
+inside a JAX/XLA process, whose allocator owns the GPU memory): its scratch is a
+fixed device array inside the library. Through the C ABI it must give the same
 result as the allocating hfmm_direct, on two calls in a row (the array is reused
 and keeps the previous call's contents), and refuse sizes beyond its limit.
 This file is collected last so that a failure here leaves every other test run.
@@ -71,3 +71,25 @@ def test_noalloc_rejects_sizes_beyond_its_scratch():
                                  phi.data_ptr(), None, torch.cuda.current_stream().cuda_stream)
     assert rc == -4
     assert b"131072" in lib.hfmm_last_error()
+
+
+def test_noalloc_out_of_range_target_then_good_call():
+    """A target index equal to n is skipped by the kernel's bounds check and the
+    call returns HFMM_ERR_ARG; the shared error word is cleared per call, so the
+    next good call returns 0 with the allocating entry point's result."""
+    import torch
+    from hfmm_b200 import _lib
+    lib = _lib.load()
+    n = 2000
+    pos, q_re, q_im, tg = _inputs(n, 64, 13)
+    bad = tg.clone()
+    bad[5] = n
+    phi = torch.empty(64, dtype=torch.complex128, device="cuda")
+    s = torch.cuda.current_stream().cuda_stream
+    rc = lib.hfmm_direct_noalloc(pos.data_ptr(), q_re.data_ptr(), q_im.data_ptr(), n,
+                                 bad.data_ptr(), 64, 3.0, phi.data_ptr(), None, s)
+    assert rc == -1
+    assert b"out of range" in lib.hfmm_last_error()
+    ref = _call(lib.hfmm_direct, pos, q_re, q_im, tg, 3.0)
+    got = _call(lib.hfmm_direct_noalloc, pos, q_re, q_im, tg, 3.0)
+    assert _rel(got[0], ref[0]) < TOL and _rel(got[1], ref[1]) < TOL
