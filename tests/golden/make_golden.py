@@ -18,15 +18,16 @@ reference's functions, not from this repository's oracle:
   (kifmm/setup.py:229-261) of each component and each charge column, combined
   as F(re) + 1j * F(im) with F(q) = F_cos(q) + 1j * F_sin(q).
 
-Needs the reference source tree (default /root/reference, or argument
-`--reference DIR`); run from the repo root:
+Needs the reference source tree, given as `--reference DIR` or in the
+environment variable HFMM0_REFERENCE; run from the repo root:
 
-    python tests/golden/make_golden.py [--reference DIR] [--edge] [case ...]
-    python tests/golden/make_golden.py [--reference DIR] --grid
-    python tests/golden/make_golden.py [--reference DIR] --phases
-    python tests/golden/make_golden.py [--reference DIR] --c1
-    python tests/golden/make_golden.py [--reference DIR] --errors
-    python tests/golden/make_golden.py [--reference DIR] --tables
+    python tests/golden/make_golden.py --reference DIR [--edge] [case ...]
+    python tests/golden/make_golden.py --reference DIR --p12
+    python tests/golden/make_golden.py --reference DIR --grid
+    python tests/golden/make_golden.py --reference DIR --phases
+    python tests/golden/make_golden.py --reference DIR --c1
+    python tests/golden/make_golden.py --reference DIR --errors
+    python tests/golden/make_golden.py --reference DIR --tables
 
 The inputs are the seeded clouds of tests/cases.py.
 """
@@ -53,6 +54,14 @@ CASES = {
     "uniform256_k0_p3": (uniform, 256, 0.0, 3, 16, None, False),
     "dup500_k1_p3": (with_duplicates, 500, 1.0, 3, 16, None, False),
     "cplx2000_k8_p6_d4": (complex_uniform, 2000, 8.0, 6, 32, 4, True),
+}
+
+# Expansion order 12 (tests/golden/p12/), the plain path's order at the 1e6-point
+# workload (n_s = 728 surface points, not a multiple of the GEMM tiles): a uniform
+# depth-2 cloud and an adaptive depth-4 cloud with W and X lists, k = 10.
+P12 = {
+    "cplx3000_k10_p12": (complex_uniform, 3000, 10.0, 12, 64, None, True),
+    "sphere2000_k10_p12_d4": (sphere_clusters, 2000, 10.0, 12, 32, 4, True),
 }
 
 # Edge cases (tests/golden/edge/): a single point, two points, one box over its
@@ -391,7 +400,9 @@ def run_tables(HFMM, folder):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=os.environ.get("HFMM0_REFERENCE"),
+                    help="the reference source tree (or set HFMM0_REFERENCE)")
+    ap.add_argument("--p12", action="store_true", help="the expansion-order-12 cases, into p12/")
     ap.add_argument("--edge", action="store_true", help="the edge cases, into edge/")
     ap.add_argument("--grid", action="store_true",
                     help="the reference's test.py grid, into grid/test_py_grid.npz")
@@ -405,6 +416,8 @@ def main():
                     help="digests of the operator tables, into tables/")
     ap.add_argument("cases", nargs="*")
     a = ap.parse_args()
+    if not a.reference:
+        ap.error("give the reference source tree: --reference DIR or HFMM0_REFERENCE")
     HFMM, seen = load_reference(a.reference)
     if a.tables:
         return run_tables(HFMM, os.path.join(HERE, "tables"))
@@ -417,6 +430,8 @@ def main():
     if a.grid:
         return run_test_py_grid(HFMM, os.path.join(HERE, "grid"))
     table, folder = (EDGE, os.path.join(HERE, "edge")) if a.edge else (CASES, HERE)
+    if a.p12:
+        table, folder = P12, os.path.join(HERE, "p12")
     for name in (a.cases or table):
         t = time.time()
         o = make(HFMM, seen, name, table, folder)
