@@ -31,6 +31,10 @@ TOL = 1e-12
 CASE_TOL = {"c3shape8000_k20_p4": 1e-11}
 GOLD = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "*.npz")))
 EDGE = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "edge", "*.npz")))
+# expansion order 12 (n_s = 728): the reference's own outputs; the p12/oracle_* files
+# are the oracle's, at sizes the reference cannot reach on the stand-in
+P12 = sorted(p for p in glob.glob(os.path.join(os.path.dirname(__file__), "golden", "p12", "*.npz"))
+             if not os.path.basename(p).startswith("oracle_"))
 
 
 def load(path):
@@ -38,7 +42,8 @@ def load(path):
         return {k: z[k] for k in z.files}
 
 
-@pytest.mark.parametrize("path", GOLD + EDGE, ids=[os.path.basename(p)[:-4] for p in GOLD + EDGE])
+@pytest.mark.parametrize("path", GOLD + EDGE + P12,
+                         ids=[os.path.basename(p)[:-4] for p in GOLD + EDGE + P12])
 @pytest.mark.filterwarnings("ignore:invalid value encountered in divide:RuntimeWarning")  # tiny1
 def test_oracle_reproduces_golden(path):
     g = load(path)
@@ -73,7 +78,7 @@ def test_oracle_reproduces_golden(path):
 
 
 def test_fixtures_present():
-    assert len(GOLD) >= 6 and len(EDGE) >= 8
+    assert len(GOLD) >= 6 and len(EDGE) >= 8 and len(P12) >= 2
 
 
 

@@ -28,7 +28,7 @@ def test_m2l_wait_runs_out_drains_and_reports():
             hfmm_b200.evaluate_field(st, qt, precision=hfmm_b200.PREC_MIXED)
     finally:
         lib.hfmm_debug_m2l_wait(0, 0)
-    assert ei.value.args[0] == -5
+    assert ei.value.code == -5
     assert "device error flag 4" in str(ei.value)
     after = hfmm_b200.evaluate_field(st, qt, precision=hfmm_b200.PREC_MIXED)
     assert torch.equal(before[0], after[0]) and torch.equal(before[1], after[1])

@@ -1,0 +1,97 @@
+"""Parity of the CUDA path at expansion order 12, the plain path's order at the
+1e6-point workload: n_s = 728 surface points per box, so the padded leading
+dimension (736) is not a multiple of the 64-wide GEMM tiles, and the mixed path's
+tcgen05 M2L runs six 128-row blocks with a partial last one.
+
+Fixtures (tests/golden/p12/):
+* the reference's own outputs (make_golden.py --p12, run on the NumPy stand-in for
+  JAX) on a uniform depth-2 cloud and an adaptive depth-4 cloud with W and X lists;
+  the CUDA path must match them with device and with host tables;
+* the oracle's outputs (make_p12_oracle.py) at 20 000 uniform points (leaf 64,
+  auto depth 3) and on a 6 000-point adaptive cloud at max_depth 4, where the
+  reference takes hours on the stand-in; tests/test_golden.py pins the oracle to
+  the reference's order-12 fixtures above.
+
+Bars: integer arrays bit for bit; potentials and fields to a relative L2 of 1e-12
+(the plain path's parity bar); the mixed evaluate against the FP64 one on the same
+plan at the bar of tests/test_gpu_mixed.py (2e-6)."""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+import oracle as O
+from cases import complex_uniform, sphere_clusters
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-12
+TOL_VS_FP64 = 2e-6
+HERE = os.path.join(os.path.dirname(__file__), "golden", "p12")
+REF = sorted(p for p in glob.glob(os.path.join(HERE, "*.npz"))
+             if not os.path.basename(p).startswith("oracle_"))
+
+
+def load(path):
+    with np.load(path) as z:
+        return {k: z[k] for k in z.files}
+
+
+def _lists_equal(st, g):
+    for key in ("V", "U", "near", "W", "X"):
+        got = st.pairs(key)
+        assert got.shape == g[key].shape and np.array_equal(got, g[key]), key
+
+
+# host tables (NumPy, bit-identical to the oracle's) on the one-level case only: at
+# order 12 the host builds 343 x 728^2 kernel entries per level and family
+REF_CASES = [(p, "device") for p in REF] + [(p, "host") for p in REF if "cplx3000" in p]
+
+
+@pytest.mark.parametrize("path,tables", REF_CASES,
+                         ids=[f"{os.path.basename(p)[:-4]}-{t}" for p, t in REF_CASES])
+def test_reference_p12(path, tables):
+    import hfmm_b200
+    g = load(path)
+    md = int(g["max_depth"])
+    st = hfmm_b200.setup(g["positions"], float(g["k"]), p=int(g["p"]), N_max=int(g["N_max"]),
+                         max_depth=None if md < 0 else md, tables=tables)
+    assert st.info["n_s"] == 728 and st.info["max_depth"] == int(g["realised_depth"])
+    t = st.tree()
+    for key in ("m_id", "p_id", "lvls", "counts", "is_leaf"):
+        assert np.array_equal(t[key], g[key]), key
+    assert np.array_equal(st.pil(), g["pil"])
+    _lists_equal(st, g)
+    phi, E = hfmm_b200.evaluate_field(st, g["charges"])
+    assert O.relative_error(phi, g["phi"]) < TOL
+    assert O.relative_error(E, g["E"]) < TOL
+    st.close()
+
+
+ORACLE = {
+    "oracle_uniform20000_k10_p12": (complex_uniform, 20000, None),
+    "oracle_sphere6000_k10_p12_d4": (sphere_clusters, 6000, 4),
+}
+
+
+@pytest.mark.parametrize("name", sorted(ORACLE))
+def test_oracle_p12_fp64_and_mixed(name):
+    import torch
+    import hfmm_b200
+    g = load(os.path.join(HERE, name + ".npz"))
+    fn, n, md = ORACLE[name]
+    pos, q = fn(n)
+    assert np.float64(pos.sum()) == g["positions_sum"] and q.sum() == g["charges_sum"]
+    st = hfmm_b200.setup(pos, float(g["k"]), p=12, N_max=int(g["N_max"]), max_depth=md)
+    assert st.info["n_s"] == 728 and st.info["max_depth"] == int(g["realised_depth"])
+    assert st.info["n_v"] == int(g["n_v"]) and st.info["n_w"] == int(g["n_w"])
+    qt = torch.as_tensor(q, device="cuda")
+    phi, E = (x.cpu().numpy() for x in hfmm_b200.evaluate_field(st, qt))
+    assert O.relative_error(phi, g["phi"]) < TOL
+    assert O.relative_error(E, g["E"]) < TOL
+    m_phi, m_E = (x.cpu().numpy() for x in
+                  hfmm_b200.evaluate_field(st, qt, precision=hfmm_b200.PREC_MIXED))
+    assert np.isfinite(m_phi).all() and np.isfinite(m_E).all()
+    assert O.relative_error(m_phi, phi) < TOL_VS_FP64
+    assert O.relative_error(m_E, E) < TOL_VS_FP64
+    st.close()
