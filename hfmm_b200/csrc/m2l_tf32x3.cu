@@ -21,15 +21,16 @@
 // Accumulation precision: the error of an FP32 accumulator grows with the
 // length of its chain of MMAs (measured: about linearly), and the damped decode
 // amplifies it. So every FOLD k-chunks (24 MMAs) accumulate into a fresh FP32
-// buffer in TMEM (two buffers alternate), and the fold warps (16: four per TMEM lane
-// quadrant, each taking a quarter of the columns; on the 1M-point p = 8 M2L, 8 fold
-// warps were 14 % faster than 4 and 16 another 3 %, all with the same bits) fold each
-// finished buffer into an FP64
-// running sum kept in TMEM (two 32-bit columns per double) while the tensor core
-// fills the other buffer. TMEM: 2 x 128 FP32 columns + 256 for the FP64 sums =
-// 512 columns. The FP64 sums are stored as the check potentials. (Folding every
-// 4 k-chunks instead was 22 % faster but doubled the M2L error: 8.3e-7 against
-// 4.6e-7 for the potential at p = 8.)
+// buffer in TMEM (four buffers in turn, 4 x 128 columns = all 512), and the fold
+// warps (16: four per TMEM lane quadrant, each taking 32 of the 128 columns) add each
+// finished buffer into FP64 running sums held in their own registers, 32 doubles a
+// thread, while the tensor core fills the next buffers. The FP64 sums are stored as
+// the check potentials. (Folding every 4 k-chunks instead was 22 % faster but
+// doubled the M2L error: 8.3e-7 against 4.6e-7 for the potential at p = 8.)
+// Registers: the block launches with 768 threads; setmaxnreg moves registers from
+// the gather and control warpgroups (warps 0-7) to the four fold warpgroups (8-23),
+// and the host checks that the split fits the launch's register file before the
+// first launch.
 // Every mbarrier wait is bounded (2 s of %globaltimer by default); a timeout sets
 // the CTA's abort flag and the device error flag, and every role stops issuing.
 // Before TMEM is freed and the CTA exits, nothing it issued may still be in flight:
@@ -67,15 +68,16 @@ constexpr int CPR = ROW_BYTES / 16;         // 16-byte chunks per row
 constexpr int TILE_BYTES = BM * ROW_BYTES;  // one operand half
 constexpr int STAGE_BYTES = 4 * TILE_BYTES;
 constexpr int STAGES = (3 * 64 * 1024) / STAGE_BYTES;
-#ifndef HFMM_MX_FOLD_WARPS
-#define HFMM_MX_FOLD_WARPS 16
-#endif
-constexpr int N_FOLD_WARPS = HFMM_MX_FOLD_WARPS;   // 4, 8 or 16: NFW/4 per TMEM lane quadrant
-constexpr int THREADS = (6 + N_FOLD_WARPS) * 32;  // warps 0-3 gather, 4 TMA, 5 MMA, 6.. fold
-constexpr int COLS_PER_FOLD_WARP = BN * 4 / N_FOLD_WARPS;
-constexpr int SUB = N_FOLD_WARPS >= 16 ? 16 : 32;  // columns per TMEM access of a fold warp
-static_assert(N_FOLD_WARPS == 4 || N_FOLD_WARPS == 8 || N_FOLD_WARPS == 16, "fold warps");
-constexpr int TMEM_COLS = 512;
+constexpr int N_FOLD_WARPS = 16;                  // four per TMEM lane quadrant
+constexpr int FOLD_WARP0 = 8;                     // warps 0-3 gather, 4 TMA, 5 MMA, 6-7 idle
+constexpr int THREADS = (FOLD_WARP0 + N_FOLD_WARPS) * 32;
+constexpr int COLS_PER_FOLD_WARP = BN * 4 / N_FOLD_WARPS;   // 32
+constexpr int NACC = 4;                           // FP32 accumulation buffers in TMEM
+constexpr int TMEM_COLS = NACC * BN;              // 512
+// registers per thread after setmaxnreg: gather warpgroup, control warpgroup, fold
+constexpr int REG_GATHER = 64, REG_CTRL = 32, REG_FOLD = 96;
+static_assert(128 * REG_GATHER + 128 * REG_CTRL + 32 * N_FOLD_WARPS * REG_FOLD <= THREADS * 80,
+              "register split exceeds an 80-register launch");
 constexpr int FOLD = 64 / BK;   // k-chunks per FP32 accumulation unit: 64 K values, 24 MMAs
 constexpr uint64_t WAIT_NS = 2000000000ull;   // bounded waits: 2 s
 
@@ -161,29 +163,6 @@ __device__ __forceinline__ void umma_commit(uint32_t bar) {
                  : "memory");
 }
 
-__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t* v) {
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,"
-        "%14,%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
-        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
-          "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
-          "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]),
-          "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]),
-          "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
-        : "r"(taddr));
-}
-__device__ __forceinline__ void tmem_st32(uint32_t taddr, const uint32_t* v) {
-    asm volatile(
-        "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,"
-        "%13,%14,%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,%32};" ::"r"(taddr),
-        "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7]),
-        "r"(v[8]), "r"(v[9]), "r"(v[10]), "r"(v[11]), "r"(v[12]), "r"(v[13]), "r"(v[14]),
-        "r"(v[15]), "r"(v[16]), "r"(v[17]), "r"(v[18]), "r"(v[19]), "r"(v[20]), "r"(v[21]),
-        "r"(v[22]), "r"(v[23]), "r"(v[24]), "r"(v[25]), "r"(v[26]), "r"(v[27]), "r"(v[28]),
-        "r"(v[29]), "r"(v[30]), "r"(v[31])
-        : "memory");
-}
-
 __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t* v) {
     asm volatile(
         "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,"
@@ -193,27 +172,6 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t* v) {
           "=r"(v[14]), "=r"(v[15])
         : "r"(taddr));
 }
-__device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t* v) {
-    asm volatile(
-        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,"
-        "%13,%14,%15,%16};" ::"r"(taddr),
-        "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7]),
-        "r"(v[8]), "r"(v[9]), "r"(v[10]), "r"(v[11]), "r"(v[12]), "r"(v[13]), "r"(v[14]),
-        "r"(v[15])
-        : "memory");
-}
-// n consecutive 32-bit TMEM columns of this warp's 32 lanes (n = 16 or 32)
-template <int n>
-__device__ __forceinline__ void tmem_ld(uint32_t taddr, uint32_t* v) {
-    if constexpr (n == 32) tmem_ld32(taddr, v);
-    else tmem_ld16(taddr, v);
-}
-template <int n>
-__device__ __forceinline__ void tmem_st(uint32_t taddr, const uint32_t* v) {
-    if constexpr (n == 32) tmem_st32(taddr, v);
-    else tmem_st16(taddr, v);
-}
-
 // Instruction descriptor: D = F32, A = B = TF32, both K-major, M = 128 (or 64), N = BN.
 constexpr uint32_t idesc_m(int m) {
     return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(BN >> 3) << 17) |
@@ -231,8 +189,8 @@ struct __align__(8) Ctl {
     uint64_t full[STAGES];   // the gather threads' copies of a stage have landed
     uint64_t tfull[STAGES];  // the stage's TMA bytes have landed (tx-only)
     uint64_t empty[STAGES];
-    uint64_t acc_full[2];    // a unit's FP32 sum is complete in buffer b (MMA commit)
-    uint64_t acc_empty[2];   // buffer b has been folded into the FP64 sum (one per fold warp)
+    uint64_t acc_full[NACC];    // a unit's FP32 sum is complete in buffer b (MMA commit)
+    uint64_t acc_empty[NACC];   // buffer b has been folded into the FP64 sums (one per fold warp)
     uint64_t done;
     uint32_t tmem;
     int abort_flag;
@@ -278,14 +236,14 @@ __global__ void __launch_bounds__(THREADS, 1) k_m2l_tf32x3(const __grid_constant
             mbar_init(smem_u32(&ctl.tfull[s]), 1);    // the TMA thread's arrive + its bytes
             mbar_init(smem_u32(&ctl.empty[s]), 1);    // MMA commit
         }
-        for (int b = 0; b < 2; ++b) {
+        for (int b = 0; b < NACC; ++b) {
             mbar_init(smem_u32(&ctl.acc_full[b]), 1);
             mbar_init(smem_u32(&ctl.acc_empty[b]), N_FOLD_WARPS);   // one per fold warp
         }
         mbar_init(smem_u32(&ctl.done), 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    if (warp == 5) {   // tensor memory: 2 FP32 entry buffers + the FP64 running sums
+    if (warp == 5) {   // tensor memory: the FP32 accumulation buffers
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                          smem_u32(&ctl.tmem)),
                      "r"(TMEM_COLS));
@@ -338,6 +296,13 @@ __global__ void __launch_bounds__(THREADS, 1) k_m2l_tf32x3(const __grid_constant
     const int nq = n_act * kch;
     const uint32_t tmem = ctl.tmem;
     const int64_t fs = (int64_t)fam * c.fam_stride;
+    // per warpgroup: the fold warps take the registers the other roles do not need
+    if (warp < 4)
+        asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" ::"n"(REG_GATHER));
+    else if (warp < FOLD_WARP0)
+        asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" ::"n"(REG_CTRL));
+    else
+        asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;" ::"n"(REG_FOLD));
 
     if (warp < 4) {
         // ---------------- B gathers (cp.async, manual SWIZZLE_128B placement)
@@ -413,48 +378,39 @@ __global__ void __launch_bounds__(THREADS, 1) k_m2l_tf32x3(const __grid_constant
         }
         // drain: this thread's copies (and the arrivals they trigger) complete
         asm volatile("cp.async.wait_all;\n" ::: "memory");
-    } else if (warp >= 6) {
-        // ---------------- fold entries into the FP64 sums; store at the end
-        // Warp w may touch TMEM lanes 32 (w % 4) .. + 31 only: the NFW fold warps
-        // cover each lane quadrant NFW / 4 times, each folding its share of columns.
+    } else if (warp >= FOLD_WARP0) {
+        // ---------------- fold each finished buffer into FP64 sums in registers
+        // Warp w may touch TMEM lanes 32 (w % 4) .. + 31 only: four fold warps cover
+        // each lane quadrant, each folding 32 of the 128 columns.
         const int quad = warp & 3;                 // TMEM lane quadrant of this warp
-        const int c_lo = ((warp - 6) >> 2) * COLS_PER_FOLD_WARP;
+        const int c_lo = ((warp - FOLD_WARP0) >> 2) * COLS_PER_FOLD_WARP;
         // the row of this lane (M = 64 blocks: lanes 16-31 of a quadrant hold none)
         const int m = half ? m0 + quad * 16 + lane : m0 + quad * 32 + lane;
         const bool row_ok = half ? (lane < 16 && m < c.ldm) : (m0 + quad * 32 < c.ldm);
         const uint32_t lane_base = tmem + ((uint32_t)(quad * 32) << 16);
         double* out = c.out + (int64_t)fam * c.out_fam_stride;
+        double sum[COLS_PER_FOLD_WARP];
+#pragma unroll
+        for (int j = 0; j < COLS_PER_FOLD_WARP; ++j) sum[j] = 0.0;
         bool ok = true;
         const int n_units = (nq + FOLD - 1) / FOLD;
-        for (int i = 0; i < n_units && ok; ++i) {
-            const int b = i & 1;
+        for (int i = 0; i < n_units; ++i) {
+            const int b = i & (NACC - 1);
             // the TMEM loads below are warp-collective: agree on the wait's outcome
-            const bool got = mbar_wait(smem_u32(&ctl.acc_full[b]), (i >> 1) & 1, abort_flag, wait_ns);
+            const bool got = mbar_wait(smem_u32(&ctl.acc_full[b]), (i / NACC) & 1, abort_flag, wait_ns);
             if (!__all_sync(0xffffffffu, got)) {
                 ok = false;
                 break;
             }
             asm volatile("tcgen05.fence::after_thread_sync;");
-            for (int cb = c_lo; cb < c_lo + COLS_PER_FOLD_WARP; cb += SUB) {
-                uint32_t v[SUB];
-                tmem_ld<SUB>(lane_base + b * BN + cb, v);
-                uint32_t w[2 * SUB];
-                if (i > 0) {
-                    tmem_ld<SUB>(lane_base + 2 * BN + 2 * cb, w);
-                    tmem_ld<SUB>(lane_base + 2 * BN + 2 * cb + SUB, w + SUB);
-                }
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                uint32_t v[16];
+                tmem_ld16(lane_base + b * BN + c_lo + 16 * h, v);
                 asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-                for (int j = 0; j < SUB; ++j) {
-                    double acc = (double)__uint_as_float(v[j]);
-                    if (i > 0) acc += __hiloint2double((int)w[2 * j + 1], (int)w[2 * j]);
-                    w[2 * j] = (uint32_t)__double2loint(acc);
-                    w[2 * j + 1] = (uint32_t)__double2hiint(acc);
-                }
-                tmem_st<SUB>(lane_base + 2 * BN + 2 * cb, w);
-                tmem_st<SUB>(lane_base + 2 * BN + 2 * cb + SUB, w + SUB);
+                for (int j = 0; j < 16; ++j) sum[16 * h + j] += (double)__uint_as_float(v[j]);
             }
-            asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
             asm volatile("tcgen05.fence::before_thread_sync;");
             __syncwarp();   // one arrive per fold warp
             if (lane == 0) mbar_arrive(smem_u32(&ctl.acc_empty[b]));
@@ -462,21 +418,12 @@ __global__ void __launch_bounds__(THREADS, 1) k_m2l_tf32x3(const __grid_constant
         const bool aborted = !__all_sync(0xffffffffu, ok && !*abort_flag);
         if (aborted) {
             if (lane == 0) atomicOr(c.err, ERRF_TIMEOUT);
-        } else if (__any_sync(0xffffffffu, row_ok)) {   // the TMEM loads are warp-collective
-            for (int cb = c_lo; cb < c_lo + COLS_PER_FOLD_WARP; cb += SUB) {
-                uint32_t w[2 * SUB];
-                if (nq > 0) {
-                    tmem_ld<SUB>(lane_base + 2 * BN + 2 * cb, w);
-                    tmem_ld<SUB>(lane_base + 2 * BN + 2 * cb + SUB, w + SUB);
-                    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-                }
+        } else if (row_ok) {
 #pragma unroll
-                for (int j = 0; j < SUB; ++j) {
-                    const int n = cb + j;
-                    const int t = ctl.tgt[n / R];
-                    const double val = nq > 0 ? __hiloint2double((int)w[2 * j + 1], (int)w[2 * j]) : 0.0;
-                    if (t >= 0 && row_ok) out[((int64_t)t * R + (n % R)) * c.ldm + m] = val;
-                }
+            for (int j = 0; j < COLS_PER_FOLD_WARP; ++j) {
+                const int n = c_lo + j;
+                const int t = ctl.tgt[n / R];
+                if (t >= 0) out[((int64_t)t * R + (n % R)) * c.ldm + m] = sum[j];
             }
         }
     } else if (warp == 4) {
@@ -518,16 +465,16 @@ __global__ void __launch_bounds__(THREADS, 1) k_m2l_tf32x3(const __grid_constant
                     drained &= mbar_drain(smem_u32(&ctl.tfull[j]), (last_q[j] / STAGES) & 1, wait_ns);
             if (!drained) atomicOr(c.err, ERRF_TIMEOUT);
         }
-    } else {
-        // ---------------- MMA issue (warp 5, one lane)
+    } else if (warp == 5) {
+        // ---------------- MMA issue (warp 5, one lane; warps 6 and 7 have no role)
         if (lane == 0) {
             bool ok = true, issued = false;
             for (int q = 0; q < nq && ok; ++q) {
                 const int st = q % STAGES;
                 const int unit = q / FOLD, uq = q % FOLD;
-                const int b = unit & 1;
-                if (uq == 0 && unit >= 2) {   // buffer b must have been folded (unit - 2)
-                    if (!mbar_wait(smem_u32(&ctl.acc_empty[b]), ((unit >> 1) & 1) ^ 1, abort_flag, wait_ns)) {
+                const int b = unit & (NACC - 1);
+                if (uq == 0 && unit >= NACC) {   // buffer b must have been folded (unit - NACC)
+                    if (!mbar_wait(smem_u32(&ctl.acc_empty[b]), ((unit / NACC) & 1) ^ 1, abort_flag, wait_ns)) {
                         ok = false;
                         break;
                     }
@@ -662,6 +609,27 @@ void split_transpose_tables(const double* at, float* hi, float* lo, int ld, int 
     HFMM_LAUNCH(k_split_transpose, grid, dim3(32, 8), 0, 0, at, hi, lo, ld);
 }
 
+// setmaxnreg.inc draws on the registers the block was launched with: the split of the
+// three warp roles must fit THREADS x (registers per thread at launch), or the fold
+// warps' increase would wait forever. Checked once, before the first launch.
+void check_register_split() {
+    static int verdict = 0;   // 0 unknown, 1 fits, -1 does not
+    static std::mutex mu;
+    std::lock_guard<std::mutex> g(mu);
+    if (verdict == 0) {
+        int fits = 1;
+        for (int r = 0; r < 2; ++r) {
+            cudaFuncAttributes a{};
+            HFMM_CUDA(cudaFuncGetAttributes(&a, r ? (const void*)k_m2l_tf32x3<2> : (const void*)k_m2l_tf32x3<1>));
+            const long need = 128L * REG_GATHER + 128L * REG_CTRL + 32L * N_FOLD_WARPS * REG_FOLD;
+            if ((long)a.numRegs * THREADS < need || a.maxThreadsPerBlock < THREADS) fits = 0;
+        }
+        verdict = fits ? 1 : -1;
+    }
+    if (verdict < 0)
+        throw Error{HFMM_ERR_STATE, "m2l_tf32x3: the warp roles' register split exceeds the launch's registers"};
+}
+
 uint64_t g_m2l_wait_ns = 0;
 int g_m2l_starve = 0;
 
@@ -678,6 +646,7 @@ void m2l_tf32x3(const MixedMaps& maps, const MixedCall& call, cudaStream_t s) {
         throw Error{HFMM_ERR_STATE, "m2l_tf32x3: ld must be a multiple of 32"};
     const size_t smem = m2l_tf32x3_smem();
     dim3 grid(c.ntiles, (c.ldm + BM - 1) / BM, c.n_fam);
+    check_register_split();
     if (c.R == 1) {
         HFMM_CUDA(cudaFuncSetAttribute(k_m2l_tf32x3<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         HFMM_LAUNCH(k_m2l_tf32x3<1>, grid, THREADS, smem, s, maps, c);
