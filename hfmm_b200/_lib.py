@@ -58,6 +58,7 @@ SIGNATURES = [
     ("hfmm_plan_check", _c_i32, [_c_vp, _c_vp]),
     ("hfmm_plan_destroy", None, [_c_vp]),
     ("hfmm_debug_m2l_wait", _c_i32, [ctypes.c_uint64, _c_i32]),
+    ("hfmm_debug_m2l_grid", _c_i32, [_c_i32]),
     ("hfmm_export_tree", _c_i32, [_c_vp] * 7),
     ("hfmm_export_pil", _c_i32, [_c_vp, _c_vp]),
     ("hfmm_export_list", _c_i32, [_c_vp, _c_i32, _c_vp, _c_i64]),

@@ -456,8 +456,12 @@ void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double*
                 LevelTables& T = P->tables[f][l];
                 gemm_1(K_CMP, l, f, P->equiv.p + f * fs, P->ld, level_base(T.xc.p, l, T.ckld), T.ckld,
                        s);
-                const int64_t cnt = (int64_t)(P->level_hi[l] - P->level_lo[l]) * R * T.ckld;
-                split_tf32(T.xc.p, T.xc_hi.p, T.xc_lo.p, cnt, s);
+                const int64_t nbl = P->level_hi[l] - P->level_lo[l];
+                if (R == 2 && T.grid && g_m2l_grid)   // complete level: into the dense grid
+                    split_tf32_grid(T.xc.p, P->m_id.p + P->level_lo[l], nbl, T.grid, T.ckld,
+                                    T.xg_hi.p, T.xg_lo.p, s);
+                else
+                    split_tf32(T.xc.p, T.xc_hi.p, T.xc_lo.p, nbl * R * T.ckld, s);
             }
     } else if (use_mx) {   // TF32 hi/lo halves of every equivalent density (B operand of the M2L)
         PhaseTimer pt(X, s, 11);
@@ -501,6 +505,12 @@ void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double*
             mc.out_fam_stride = 0;
             mc.nb = P->nb;
             mc.err = P->d_err.p;
+            if (R == 2 && T.grid && g_m2l_grid) {   // sources from the dense grid by TMA
+                mc.grid = 1;
+                mc.tile_tgt = P->gx_tiles[l].tgt.p;
+                mc.ntiles = P->gx_tiles[l].ntiles;
+                mc.tile_org = P->gx_org[l].p;
+            }
             m2l_tf32x3(static_cast<MixedMaps*>(P->cx_maps)[f * MAX_LEVELS + l], mc, ss);
             // expand into the level's downward coordinates: y_dn = d_dn .* (y' U_c^T U_dn)
             // (overwrites; the L2L and X list add to it on the main stream)

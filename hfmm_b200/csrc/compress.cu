@@ -143,6 +143,21 @@ void compressed_prepare(hfmm_plan* P) {
             T.xc_lo.zero();
             make_table_map(&maps[f * MAX_LEVELS + l].a_hi[0], T.c_hi.p, T.ckld, N_M2L, T.cmld);
             make_table_map(&maps[f * MAX_LEVELS + l].a_lo[0], T.c_lo.p, T.ckld, N_M2L, T.cmld);
+            // complete level: the complex-charge M2L reads its densities from a dense grid
+            T.grid = 0;
+            T.xg_hi.release();
+            T.xg_lo.release();
+            if (P->gx_tiles[l].ntiles > 0) {
+                const int G = 1 << l;
+                const size_t cells = (size_t)G * G * G * 2 * T.ckld;
+                T.xg_hi.alloc(cells);
+                T.xg_lo.alloc(cells);
+                T.xg_hi.zero();
+                T.xg_lo.zero();
+                make_grid_map(&maps[f * MAX_LEVELS + l].b_hi[0], T.xg_hi.p, T.ckld, G);
+                make_grid_map(&maps[f * MAX_LEVELS + l].b_lo[0], T.xg_lo.p, T.ckld, G);
+                T.grid = G;
+            }
         }
     {
         DevBuf<double> tmp;

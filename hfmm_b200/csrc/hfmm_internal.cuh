@@ -74,6 +74,7 @@ struct DevBuf {
 constexpr int MAX_LEVELS = 16;
 constexpr int N_DISP = 343;        // (dx, dy, dz) in [-3, 3]^3
 constexpr int M2L_ENTRIES = N_DISP + 8;   // 343 displacement slots + 8 L2L octant slots
+constexpr int GRID_MAX_LEVEL = 5;  // densest level kept as a dense box grid (32^3 boxes)
 
 // Per-level, per-family operator tables in the GEMM layout (A^T, k-major,
 // leading dimension ld, zero padded): out_col = A @ in_col.
@@ -92,6 +93,10 @@ struct LevelTables {
     DevBuf<float> c_hi, c_lo;      // C_d halves as A [316][cmld][ckld]
     DevBuf<double> xc, yc;         // the level's compressed densities [.][R][ckld] and
     DevBuf<float> xc_hi, xc_lo;    // check potentials [.][R][cmld] (box - level_lo first)
+    // a complete level's split densities as a dense box grid [x][y][z][2][ckld] (complex
+    // charges): a target tile's sources at one displacement are then one strided TMA box
+    int grid = 0;                  // grid side 2^level when the grid is in use, else 0
+    DevBuf<float> xg_hi, xg_lo;
     // the low-rank plan's folded tables (row-major right multipliers, zero padded):
     // the decodes' Vt and U taken into the operators next to them, so a box keeps its
     // densities as scaled SVD coordinates (d .* (U^T x)) through both passes
@@ -107,6 +112,8 @@ struct LevelTables {
         cr = ckld = cmld = 0;
         c_cmp.release(); c_exp.release(); c_hi.release(); c_lo.release();
         xc.release(); yc.release(); xc_hi.release(); xc_lo.release();
+        grid = 0;
+        xg_hi.release(); xg_lo.release();
         m2m_f.release(); l2l_f.release(); cmp_f.release(); exp_f.release();
         set = false;
     }
@@ -174,6 +181,10 @@ struct hfmm_plan {
     Tiles dec_tiles[hfmm::MAX_LEVELS][2];
     Tiles leaf_tiles[hfmm::MAX_LEVELS][2];  // the level's leaves only
     Tiles mx_tiles[hfmm::MAX_LEVELS][2];    // mixed M2L tiles: 128 / R targets, by octant
+    // complete levels, complex charges: tiles of one octant of a 4 x 4 x 4 block of
+    // parents (target j = (x * 4 + y) * 4 + z at grid org + 2 (x, y, z)), origins per tile
+    Tiles gx_tiles[hfmm::MAX_LEVELS];
+    hfmm::DevBuf<int32_t> gx_org[hfmm::MAX_LEVELS];
     hfmm::DevBuf<int32_t> disp_compact;     // 343 -> M2L table index or -1
     hfmm::DevBuf<float> e_hi, e_lo, l_hi, l_lo;   // split densities [fam][box][R][ld]
     void* mx_maps = nullptr;                // MixedMaps per level (host array)

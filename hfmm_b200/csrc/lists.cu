@@ -492,6 +492,44 @@ void schedules_build(hfmm_plan* P) {
             P->mx_tiles[l][r].ntiles = (int)(mx.size() / TTM);
             upload(P->mx_tiles[l][r].tgt, mx);
         }
+        // grid tiles of a complete level (every one of its 8^l boxes present), for the
+        // mixed M2L with complex charges: 64 targets = one octant o of a 4 x 4 x 4 block
+        // of parents, target j = (x * 4 + y) * 4 + z at grid position
+        // org + 2 (x, y, z), org = 8 (block) + o; the octants' tiles interleaved as above
+        P->gx_tiles[l].ntiles = 0;
+        const int64_t G = (int64_t)1 << l;
+        if (l >= 3 && l <= GRID_MAX_LEVEL && (int64_t)(hi - lo) == G * G * G) {
+            std::vector<int32_t> at((size_t)(G * G * G), -1);   // grid position -> box
+            bool fits = true;
+            for (int b = lo; b < hi && fits; ++b) {
+                int64_t x, y, z;
+                demorton3(P->h_m_id[b], x, y, z);
+                if (x < 0 || y < 0 || z < 0 || x >= G || y >= G || z >= G ||
+                    at[(size_t)((x * G + y) * G + z)] >= 0)
+                    fits = false;   // not one box per grid cell: keep the gather
+                else
+                    at[(size_t)((x * G + y) * G + z)] = b;
+            }
+            if (!fits) continue;
+            const int64_t nc = (G / 2 + 3) / 4;   // parent blocks per axis
+            std::vector<int32_t> tg, org;
+            for (int64_t c = 0; c < nc * nc * nc; ++c)
+                for (int o = 0; o < 8; ++o) {
+                    const int64_t ox = 8 * (c / (nc * nc)) + (o & 1);
+                    const int64_t oy = 8 * ((c / nc) % nc) + ((o >> 1) & 1);
+                    const int64_t oz = 8 * (c % nc) + ((o >> 2) & 1);
+                    org.push_back((int32_t)ox);
+                    org.push_back((int32_t)oy);
+                    org.push_back((int32_t)oz);
+                    for (int j = 0; j < 64; ++j) {
+                        const int64_t x = ox + 2 * (j / 16), y = oy + 2 * ((j / 4) % 4), z = oz + 2 * (j % 4);
+                        tg.push_back(x < G && y < G && z < G ? at[(size_t)((x * G + y) * G + z)] : -1);
+                    }
+                }
+            P->gx_tiles[l].ntiles = (int)(tg.size() / 64);
+            upload(P->gx_tiles[l].tgt, tg);
+            upload(P->gx_org[l], org);
+        }
     }
     HFMM_CUDA(cudaDeviceSynchronize());
 }

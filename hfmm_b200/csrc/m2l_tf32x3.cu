@@ -18,6 +18,12 @@
 //   * warp 5 (one lane) issues 4 k-steps x 3 tcgen05.mma and commits the stage
 //     back to its "empty" mbarrier;
 // three stages in flight.
+// Grid mode (a complete level with complex charges, the uniform workloads): the
+// level's densities sit in a dense box grid and a tile is one octant of a 4 x 4 x 4
+// block of parents, so its 64 targets' sources at one displacement form a stride-2
+// 4 x 4 x 4 box of that grid: warp 4 then loads B hi/lo with two 5-D TMA copies per
+// stage as well (element strides 2, out-of-domain sources read the zero fill), the
+// gather warps idle, and the stage's only barrier is the TMA transaction count.
 // Accumulation precision: the error of an FP32 accumulator grows with the
 // length of its chain of MMAs (measured: about linearly), and the damped decode
 // amplifies it. So every FOLD k-chunks (24 MMAs) accumulate into a fresh FP32
@@ -142,6 +148,14 @@ __device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap* map
         "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
         " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(dst),
         "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(bar)
+        : "memory");
+}
+__device__ __forceinline__ void tma_load_5d(uint32_t dst, const CUtensorMap* map, int c0, int c1,
+                                            int c2, int c3, int c4, uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3, %4, %5, %6}], [%7];" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4), "r"(bar)
         : "memory");
 }
 // UMMA shared-memory descriptor: K-major, swizzled rows of ROW_BYTES (layout type 2 =
@@ -305,79 +319,81 @@ __global__ void __launch_bounds__(THREADS, 1) k_m2l_tf32x3(const __grid_constant
         asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;" ::"n"(REG_FOLD));
 
     if (warp < 4) {
-        // ---------------- B gathers (cp.async, manual SWIZZLE_128B placement)
-        const float* Bh = c.Bhi + fs;
-        const float* Bl = c.Blo + fs;
-        // Each thread always serves chunk ch of the same CPR rows (columns) of the B
-        // tile: rows n_i = tid / CPR + (128 / CPR) i. Their swizzled shared-memory
-        // offsets are fixed (the 16-byte chunk index XORs with the row's bits: all three
-        // for 128-byte rows, the upper two for 64-byte rows, as TMA and the MMA read them);
-        // their global sources change only when the displacement entry changes.
-        constexpr int RSTEP = 128 / CPR;
-        const int ch = tid % CPR;
-        uint32_t soff[CPR];
-        int64_t goff[CPR];
-#pragma unroll
-        for (int i = 0; i < CPR; ++i) {
-            const int n = tid / CPR + RSTEP * i;
-            const int sw = BK == 32 ? (n & 7) : ((n & 7) >> 1);
-            soff[i] = (uint32_t)((n >> 3) * 8 * ROW_BYTES + (n & 7) * ROW_BYTES + ((ch ^ sw) << 4));
-            goff[i] = -1;
-        }
-        // The source boxes of the next entry are loaded while the current one streams,
-        // so the table lookups' latency stays off the copy pipeline.
-        int nsrc[CPR];
-        auto load_sources = [&](int ai) {
-            const int e = ctl.act[ai];
-#pragma unroll
+        if (!c.grid) {   // (grid mode: B comes by TMA, warp 4)
+            // ---------------- B gathers (cp.async, manual SWIZZLE_128B placement)
+            const float* Bh = c.Bhi + fs;
+            const float* Bl = c.Blo + fs;
+            // Each thread always serves chunk ch of the same CPR rows (columns) of the B
+            // tile: rows n_i = tid / CPR + (128 / CPR) i. Their swizzled shared-memory
+            // offsets are fixed (the 16-byte chunk index XORs with the row's bits: all three
+            // for 128-byte rows, the upper two for 64-byte rows, as TMA and the MMA read them);
+            // their global sources change only when the displacement entry changes.
+            constexpr int RSTEP = 128 / CPR;
+            const int ch = tid % CPR;
+            uint32_t soff[CPR];
+            int64_t goff[CPR];
+    #pragma unroll
             for (int i = 0; i < CPR; ++i) {
-                const int t = ctl.tgt[(tid / CPR + RSTEP * i) / R];
-                nsrc[i] = t >= 0 ? c.src_tab[(int64_t)t * M2L_ENTRIES + e] : -1;
+                const int n = tid / CPR + RSTEP * i;
+                const int sw = BK == 32 ? (n & 7) : ((n & 7) >> 1);
+                soff[i] = (uint32_t)((n >> 3) * 8 * ROW_BYTES + (n & 7) * ROW_BYTES + ((ch ^ sw) << 4));
+                goff[i] = -1;
             }
-        };
-        const int64_t src_lo = c.src_hi > 0 ? c.src_lo : 0;
-        const int64_t src_hi = c.src_hi > 0 ? c.src_hi : c.nb;
-        if (nq > 0) load_sources(0);
-        int cur_entry = -1;
-        for (int q = 0; q < nq; ++q) {
-            const int st = q % STAGES;
-            const int ai = q / kch;
-            if (ai != cur_entry) {   // new displacement entry: this thread's 8 sources
-                cur_entry = ai;
-#pragma unroll
+            // The source boxes of the next entry are loaded while the current one streams,
+            // so the table lookups' latency stays off the copy pipeline.
+            int nsrc[CPR];
+            auto load_sources = [&](int ai) {
+                const int e = ctl.act[ai];
+    #pragma unroll
                 for (int i = 0; i < CPR; ++i) {
-                    const int n = tid / CPR + RSTEP * i;
-                    int s_ = nsrc[i];
-                    if (s_ >= 0 && (s_ < src_lo || s_ >= src_hi)) {
-                        atomicOr(c.err, ERRF_BOUNDS);
-                        s_ = -1;
-                    }
-                    goff[i] = s_ >= 0 ? ((int64_t)s_ * R + (n % R)) * c.ldk + ch * 4 : -1;
+                    const int t = ctl.tgt[(tid / CPR + RSTEP * i) / R];
+                    nsrc[i] = t >= 0 ? c.src_tab[(int64_t)t * M2L_ENTRIES + e] : -1;
                 }
-                if (ai + 1 < n_act) load_sources(ai + 1);
+            };
+            const int64_t src_lo = c.src_hi > 0 ? c.src_lo : 0;
+            const int64_t src_hi = c.src_hi > 0 ? c.src_hi : c.nb;
+            if (nq > 0) load_sources(0);
+            int cur_entry = -1;
+            for (int q = 0; q < nq; ++q) {
+                const int st = q % STAGES;
+                const int ai = q / kch;
+                if (ai != cur_entry) {   // new displacement entry: this thread's 8 sources
+                    cur_entry = ai;
+    #pragma unroll
+                    for (int i = 0; i < CPR; ++i) {
+                        const int n = tid / CPR + RSTEP * i;
+                        int s_ = nsrc[i];
+                        if (s_ >= 0 && (s_ < src_lo || s_ >= src_hi)) {
+                            atomicOr(c.err, ERRF_BOUNDS);
+                            s_ = -1;
+                        }
+                        goff[i] = s_ >= 0 ? ((int64_t)s_ * R + (n % R)) * c.ldk + ch * 4 : -1;
+                    }
+                    if (ai + 1 < n_act) load_sources(ai + 1);
+                }
+                if (!mbar_wait(smem_u32(&ctl.empty[st]), ((q / STAGES) & 1) ^ 1, abort_flag, wait_ns)) break;
+                const int k0 = (q % kch) * BK;
+                const uint32_t sbh = smem_u32(sm + st * STAGE_BYTES + 2 * TILE_BYTES);
+                const uint32_t sbl = sbh + TILE_BYTES;
+    #pragma unroll
+                for (int i = 0; i < CPR; ++i) {
+                    const bool ok = goff[i] >= 0;
+                    const int64_t o = ok ? goff[i] + k0 : 0;
+                    cp_async16(sbh + soff[i], Bh + o, ok);
+                    cp_async16(sbl + soff[i], Bl + o, ok);
+                }
+                // the stage's barrier counts this thread's arrival when its copies have
+                // landed: no thread waits for its own copies, so every stage can be in flight
+                // (c.starve: a test leaves stage 0 without its arrivals, so the MMA thread's
+                // bounded wait runs out)
+                if (!(c.starve && q == 0))
+                    asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(
+                                     smem_u32(&ctl.full[st]))
+                                 : "memory");
             }
-            if (!mbar_wait(smem_u32(&ctl.empty[st]), ((q / STAGES) & 1) ^ 1, abort_flag, wait_ns)) break;
-            const int k0 = (q % kch) * BK;
-            const uint32_t sbh = smem_u32(sm + st * STAGE_BYTES + 2 * TILE_BYTES);
-            const uint32_t sbl = sbh + TILE_BYTES;
-#pragma unroll
-            for (int i = 0; i < CPR; ++i) {
-                const bool ok = goff[i] >= 0;
-                const int64_t o = ok ? goff[i] + k0 : 0;
-                cp_async16(sbh + soff[i], Bh + o, ok);
-                cp_async16(sbl + soff[i], Bl + o, ok);
-            }
-            // the stage's barrier counts this thread's arrival when its copies have
-            // landed: no thread waits for its own copies, so every stage can be in flight
-            // (c.starve: a test leaves stage 0 without its arrivals, so the MMA thread's
-            // bounded wait runs out)
-            if (!(c.starve && q == 0))
-                asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(
-                                 smem_u32(&ctl.full[st]))
-                             : "memory");
+            // drain: this thread's copies (and the arrivals they trigger) complete
+            asm volatile("cp.async.wait_all;\n" ::: "memory");
         }
-        // drain: this thread's copies (and the arrivals they trigger) complete
-        asm volatile("cp.async.wait_all;\n" ::: "memory");
     } else if (warp >= FOLD_WARP0) {
         // ---------------- fold each finished buffer into FP64 sums in registers
         // Warp w may touch TMEM lanes 32 (w % 4) .. + 31 only: four fold warps cover
@@ -433,24 +449,38 @@ __global__ void __launch_bounds__(THREADS, 1) k_m2l_tf32x3(const __grid_constant
             const CUtensorMap* ml = &maps.a_lo[fam];
             const CUtensorMap* lh = &maps.l_hi[fam];
             const CUtensorMap* ll = &maps.l_lo[fam];
+            const CUtensorMap* bh = &maps.b_hi[fam];
+            const CUtensorMap* bl = &maps.b_lo[fam];
+            int ox = 0, oy = 0, oz = 0;   // grid mode: the tile's grid origin
+            if (c.grid) {
+                ox = c.tile_org[3 * (int64_t)tile];
+                oy = c.tile_org[3 * (int64_t)tile + 1];
+                oz = c.tile_org[3 * (int64_t)tile + 2];
+            }
             int last_q[STAGES];   // the last q loaded into each stage (-1: none)
 #pragma unroll
             for (int st = 0; st < STAGES; ++st) last_q[st] = -1;
             for (int q = 0; q < nq; ++q) {
                 const int st = q % STAGES;
                 if (!mbar_wait(smem_u32(&ctl.empty[st]), ((q / STAGES) & 1) ^ 1, abort_flag, wait_ns)) break;
+                if (c.grid && c.starve && q == 0) continue;   // test: stage 0 never fills
                 const int e = ctl.act[q / kch];
                 const int z = ctl.zidx[q / kch];
                 const int k0 = (q % kch) * BK;
                 const uint32_t fb = smem_u32(&ctl.tfull[st]);
                 const uint32_t sa = smem_u32(sm + st * STAGE_BYTES);
-                mbar_arrive_tx(fb, 2 * TILE_BYTES);
+                mbar_arrive_tx(fb, (c.grid ? 4 : 2) * TILE_BYTES);
                 if (e < N_DISP) {
                     tma_load_3d(sa, mh, k0, m0, z, fb);
                     tma_load_3d(sa + TILE_BYTES, ml, k0, m0, z, fb);
                 } else {
                     tma_load_3d(sa, lh, k0, m0, z, fb);
                     tma_load_3d(sa + TILE_BYTES, ll, k0, m0, z, fb);
+                }
+                if (c.grid) {   // sources at target - d, d = (e / 49 - 3, (e / 7) % 7 - 3, e % 7 - 3)
+                    const int sx = ox - (e / 49 - 3), sy = oy - ((e / 7) % 7 - 3), sz = oz - (e % 7 - 3);
+                    tma_load_5d(sa + 2 * TILE_BYTES, bh, k0, 0, sz, sy, sx, fb);
+                    tma_load_5d(sa + 3 * TILE_BYTES, bl, k0, 0, sz, sy, sx, fb);
                 }
 #pragma unroll
                 for (int j = 0; j < STAGES; ++j)
@@ -480,14 +510,14 @@ __global__ void __launch_bounds__(THREADS, 1) k_m2l_tf32x3(const __grid_constant
                     }
                     asm volatile("tcgen05.fence::after_thread_sync;");
                 }
-                if (!mbar_wait(smem_u32(&ctl.full[st]), (q / STAGES) & 1, abort_flag, wait_ns) ||
+                if ((!c.grid && !mbar_wait(smem_u32(&ctl.full[st]), (q / STAGES) & 1, abort_flag, wait_ns)) ||
                     !mbar_wait(smem_u32(&ctl.tfull[st]), (q / STAGES) & 1, abort_flag, wait_ns)) {
                     ok = false;
                     break;
                 }
                 // the gathered B halves were written by cp.async (generic proxy): order them
                 // before the tensor core's (async proxy) reads of the stage
-                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                if (!c.grid) asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
                 asm volatile("tcgen05.fence::after_thread_sync;");
                 const uint32_t base = smem_u32(sm + st * STAGE_BYTES);
                 const uint64_t ah = sw_desc(base), al = sw_desc(base + TILE_BYTES);
@@ -541,6 +571,23 @@ __global__ void k_split_tf32(const double* __restrict__ src, float* hi, float* l
     split2(src[i], h, l);
     hi[i] = h;
     lo[i] = l;
+}
+
+// densities [box][2][ckld] of a complete level -> TF32 halves at the box's grid position
+__global__ void k_split_tf32_grid(const double* __restrict__ src, const uint64_t* __restrict__ m_id,
+                                  int64_t n, int G, int ckld, float* hi, float* lo) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int64_t row = 2 * (int64_t)ckld;
+    const int64_t b = i / row, within = i % row;
+    int64_t x, y, z;
+    demorton3(m_id[b], x, y, z);
+    if (x >= G || y >= G || z >= G) return;
+    const int64_t o = ((x * G + y) * G + z) * row + within;
+    float h, l;
+    split2(src[i], h, l);
+    hi[o] = h;
+    lo[o] = l;
 }
 
 // FP64 A^T tables ([k][m], ld x ld) -> TF32 hi/lo A tables ([m][k]), count matrices
@@ -599,6 +646,32 @@ void make_table_map(CUtensorMap* map, const float* base, int ld, int count, int 
     if (r != CUDA_SUCCESS) throw Error{HFMM_ERR_CUDA, "cuTensorMapEncodeTiled failed: " + std::to_string((int)r)};
 }
 
+void make_grid_map(CUtensorMap* map, const float* base, int ckld, int G) {
+    // dense grid [x][y][z][2][ckld] fp32: dims (k, r, z, y, x); a box is one k-chunk of both
+    // charge columns of 4 x 4 x 4 boxes two grid steps apart (element strides 2: a box of
+    // 8 elements loads 4 of them), 128 rows of ROW_BYTES in the tile layout of the A maps
+    if (((uintptr_t)base & 15) || (ckld * 4) % 16 || ckld < BK || G < 1)
+        throw Error{HFMM_ERR_STATE, "grid map: grid not 16-byte aligned or smaller than a box"};
+    cuuint64_t dims[5] = {(cuuint64_t)ckld, 2, (cuuint64_t)G, (cuuint64_t)G, (cuuint64_t)G};
+    cuuint64_t strides[4] = {(cuuint64_t)ckld * 4, (cuuint64_t)ckld * 8, (cuuint64_t)G * ckld * 8,
+                             (cuuint64_t)G * G * ckld * 8};
+    cuuint32_t box[5] = {BK, 2, 8, 8, 8};
+    cuuint32_t estr[5] = {1, 1, 2, 2, 2};
+    CUresult r = encode_fn()(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 5, (void*)base, dims, strides,
+                             box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                             BK == 32 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B,
+                             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS)
+        throw Error{HFMM_ERR_CUDA, "cuTensorMapEncodeTiled (grid) failed: " + std::to_string((int)r)};
+}
+
+void split_tf32_grid(const double* src, const uint64_t* m_id, int64_t n_boxes, int G, int ckld,
+                     float* hi, float* lo, cudaStream_t s) {
+    const int64_t n = n_boxes * 2 * ckld;
+    if (n <= 0) return;
+    HFMM_LAUNCH(k_split_tf32_grid, (unsigned)ceil_div(n, 256), 256, 0, s, src, m_id, n, G, ckld, hi, lo);
+}
+
 void split_tf32(const double* src, float* hi, float* lo, int64_t n, cudaStream_t s) {
     if (n <= 0) return;
     HFMM_LAUNCH(k_split_tf32, (unsigned)ceil_div(n, 256), 256, 0, s, src, hi, lo, n);
@@ -631,6 +704,7 @@ void check_register_split() {
 }
 
 uint64_t g_m2l_wait_ns = 0;
+int g_m2l_grid = 1;
 int g_m2l_starve = 0;
 
 size_t m2l_tf32x3_smem() { return (size_t)STAGES * STAGE_BYTES + sizeof(Ctl) + 1024; }
@@ -657,6 +731,11 @@ void m2l_tf32x3(const MixedMaps& maps, const MixedCall& call, cudaStream_t s) {
 }
 
 }  // namespace hfmm
+
+extern "C" int hfmm_debug_m2l_grid(int on) {
+    hfmm::g_m2l_grid = on ? 1 : 0;
+    return HFMM_OK;
+}
 
 extern "C" int hfmm_debug_m2l_wait(uint64_t wait_ns, int starve) {
     hfmm::g_m2l_wait_ns = wait_ns;

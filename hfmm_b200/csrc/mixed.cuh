@@ -10,6 +10,7 @@ namespace hfmm {
 // M2L (316 non-adjacent displacements) and L2L (8 octants), each [z][m][k] fp32.
 struct MixedMaps {
     CUtensorMap a_hi[2], a_lo[2], l_hi[2], l_lo[2];
+    CUtensorMap b_hi[2], b_lo[2];   // grid mode: the level's dense density grid (5-D)
 };
 
 struct MixedCall {
@@ -32,6 +33,11 @@ struct MixedCall {
     int* err;
     uint64_t wait_ns;              // limit of each bounded wait (0: 2 s); set by m2l_tf32x3
     int starve;                    // test only: leave stage 0 without its gather arrivals
+    // grid mode (complete level, R = 2): B comes from the dense density grid by TMA, one
+    // strided 4 x 4 x 4 box per displacement; tile_tgt then holds grid tiles and
+    // tile_org each tile's grid origin (x, y, z)
+    int grid;
+    const int32_t* tile_org;
 };
 
 // Wait limit and starvation switch of the next M2L launches (hfmm_debug_m2l_wait):
@@ -41,6 +47,13 @@ extern int g_m2l_starve;
 
 void make_table_map(CUtensorMap* map, const float* base, int ld, int count, int ldm = 0);
 void split_tf32(const double* src, float* hi, float* lo, int64_t n, cudaStream_t s);
+// a complete level's densities [box][2][ckld] (boxes in level order from m_id) -> TF32
+// halves in the dense grid [x][y][z][2][ckld] of side G
+void split_tf32_grid(const double* src, const uint64_t* m_id, int64_t n_boxes, int G, int ckld,
+                     float* hi, float* lo, cudaStream_t s);
+void make_grid_map(CUtensorMap* map, const float* base, int ckld, int G);
+// process-wide: 1 (default) lets complete levels use grid mode, 0 forces the gather
+extern int g_m2l_grid;
 void split_transpose_tables(const double* at, float* hi, float* lo, int ld, int count);
 void m2l_tf32x3(const MixedMaps& maps, const MixedCall& c, cudaStream_t s);
 size_t m2l_tf32x3_smem();

@@ -148,6 +148,14 @@ void hfmm_plan_destroy(hfmm_plan* plan);
  * in the reference (XLA programs have no device error path). */
 int hfmm_debug_m2l_wait(uint64_t wait_ns, int starve);
 
+/* Source layout of the mixed M2L on complete tree levels (process-wide; applies to
+ * the evaluates that follow): on != 0 (the default) lets a level whose every box is
+ * present read its compressed densities, with complex charges, from a dense box
+ * grid by strided TMA copies; on == 0 gathers them per target like every other
+ * level. The two agree to the FP32 accumulation order. For tests and timing. No
+ * counterpart in the reference. */
+int hfmm_debug_m2l_grid(int on);
+
 /* ---- inspection (tests compare these with the oracle bit for bit) ---- */
 /* Tree arrays of the active boxes: m_id (uint64), p_id, lvls, counts (int32),
  * is_leaf (uint8), each of length n_boxes; sort_idx (int32, n). Host buffers. */

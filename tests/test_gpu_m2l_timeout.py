@@ -36,3 +36,27 @@ def test_m2l_wait_runs_out_drains_and_reports():
     a = hfmm_b200.evaluate_field(st, qt, precision=hfmm_b200.PREC_FP64)
     assert np.isfinite(a[0].cpu().numpy()).all()
     st.close()
+
+
+def test_m2l_grid_mode_wait_runs_out_drains_and_reports():
+    """The same failure path when the M2L reads its sources from the dense box grid
+    (complete levels, complex charges, low-rank tables): stage 0 is never loaded."""
+    import torch
+    import hfmm_b200
+    from hfmm_b200 import _lib
+    lib = _lib.load()
+    pos, q = complex_uniform(30000)
+    st = hfmm_b200.setup(pos, 6.0, p=8, N_max=32, m2l_compress=1e-7)
+    qt = torch.as_tensor(q, device="cuda")
+    before = hfmm_b200.evaluate_field(st, qt, precision=hfmm_b200.PREC_MIXED)
+    try:
+        assert lib.hfmm_debug_m2l_wait(20_000_000, 1) == 0
+        with pytest.raises(hfmm_b200.HFMMError) as ei:
+            hfmm_b200.evaluate_field(st, qt, precision=hfmm_b200.PREC_MIXED)
+    finally:
+        lib.hfmm_debug_m2l_wait(0, 0)
+    assert ei.value.code == -5
+    assert "device error flag 4" in str(ei.value)
+    after = hfmm_b200.evaluate_field(st, qt, precision=hfmm_b200.PREC_MIXED)
+    assert torch.equal(before[0], after[0]) and torch.equal(before[1], after[1])
+    st.close()

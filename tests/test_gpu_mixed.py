@@ -59,3 +59,34 @@ def test_mixed_is_deterministic():
     r1 = hfmm_b200.evaluate_field(st, qt, precision=hfmm_b200.PREC_MIXED)
     r2 = hfmm_b200.evaluate_field(st, qt, precision=hfmm_b200.PREC_MIXED)
     assert torch.equal(r1[0], r2[0]) and torch.equal(r1[1], r2[1])
+
+
+def test_grid_sources_match_the_gather():
+    """Complete tree levels with complex charges read their compressed densities from
+    a dense box grid by strided TMA copies (the 1e6-point workload's path); the gather
+    of the same sources per target must give the same result to the FP32 accumulation
+    order (the two can split the active displacements into accumulation units
+    differently only on tiles at the domain boundary), both within the mixed path's bar
+    of the FP64 evaluate."""
+    import torch
+    import hfmm_b200
+    from hfmm_b200 import _lib
+    lib = _lib.load()
+    pos, q = complex_uniform(60000)
+    st = hfmm_b200.setup(pos, 8.0, p=8, N_max=32, m2l_compress=1e-7)
+    assert st.max_depth >= 4
+    qt = torch.as_tensor(q, device="cuda")
+    ref = [x.cpu().numpy() for x in hfmm_b200.evaluate_field(st, qt, precision=hfmm_b200.PREC_FP64)]
+    try:
+        lib.hfmm_debug_m2l_grid(1)
+        grid = [x.cpu().numpy() for x in hfmm_b200.evaluate_field(st, qt, precision=hfmm_b200.PREC_MIXED)]
+        lib.hfmm_debug_m2l_grid(0)
+        gath = [x.cpu().numpy() for x in hfmm_b200.evaluate_field(st, qt, precision=hfmm_b200.PREC_MIXED)]
+    finally:
+        lib.hfmm_debug_m2l_grid(1)
+    for g, h, r in zip(grid, gath, ref):
+        assert np.isfinite(g).all()
+        assert O.relative_error(g, h) < 1e-6
+        assert O.relative_error(g, r) < TOL_VS_FP64
+        assert O.relative_error(h, r) < TOL_VS_FP64
+    st.close()
