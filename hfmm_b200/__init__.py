@@ -150,7 +150,7 @@ def _validate_setup(positions, k, p, N_max, max_depth):
 
 
 def setup(positions, k, p=4, N_max=16, max_depth=None, device=None, tables="device",
-          stream_tables=False, m2l_compress=None):
+          stream_tables=False, m2l_compress=None, domain=None):
     """Build the plan for ``positions`` and wavenumber ``k`` (HFMM.setup, HFMM.py:55-80).
 
     ``p`` is the number of surface points per cube edge, ``N_max`` the leaf
@@ -164,19 +164,34 @@ def setup(positions, k, p=4, N_max=16, max_depth=None, device=None, tables="devi
     to the resident "device" tables; memory per plan drops to one level's worth).
     ``m2l_compress``: a relative tolerance (e.g. 1e-8) to give the mixed-precision
     evaluate a low-rank M2L (``hfmm_b200.compress``); the FP64 evaluate is unchanged.
+    ``domain``: ``(pmin (3,), extent)``, a fixed domain cube instead of the points'
+    bounding box (moving geometry, ``hfmm_b200.moving``); needs ``max_depth``. Every
+    point must lie inside it; ``rebuild`` then moves the points within it.
     """
     if tables not in ("device", "host"):
         raise ValueError('tables must be "device" or "host"')
     if stream_tables and tables != "device":
         raise ValueError('stream_tables needs tables="device"')
     x, kf = _validate_setup(positions, k, p, N_max, max_depth)
+    if domain is not None:
+        lo, ext = np.asarray(domain[0], dtype=np.float64).reshape(3), float(domain[1])
+        if max_depth is None:
+            raise ValueError("a fixed domain needs max_depth")
+        if not (np.isfinite(lo).all() and np.isfinite(ext) and ext > 0):
+            raise ValueError("domain must be (finite corner (3,), positive extent)")
     dev = _device(device)
     with torch.cuda.device(dev):
         pos = torch.as_tensor(x, dtype=torch.float64).to(dev).contiguous()
         h = _lib.ctypes.c_void_p()
-        _check(_lib.lib.hfmm_tree_build(pos.data_ptr(), pos.shape[0], int(N_max),
-                                        int(max_depth) if max_depth is not None else 0,
-                                        _lib.ctypes.byref(h)))
+        if domain is None:
+            _check(_lib.lib.hfmm_tree_build(pos.data_ptr(), pos.shape[0], int(N_max),
+                                            int(max_depth) if max_depth is not None else 0,
+                                            _lib.ctypes.byref(h)))
+        else:
+            lo_c = (_lib.ctypes.c_double * 3)(*lo.tolist())
+            _check(_lib.lib.hfmm_tree_build_in_domain(pos.data_ptr(), pos.shape[0], int(N_max),
+                                                      int(max_depth), lo_c, ext,
+                                                      _lib.ctypes.byref(h)))
         state = HFMMState(h.value, pos, kf, p, N_max, dev)
         try:
             _load_tables(state, tables, stream_tables)
@@ -186,6 +201,22 @@ def setup(positions, k, p=4, N_max=16, max_depth=None, device=None, tables="devi
         except Exception:
             state.close()
             raise
+        state._refresh()
+    return state
+
+
+def rebuild(state, positions):
+    """Move a fixed-domain plan's points (hfmm_plan_rebuild): the tree, lists and
+    schedules are rebuilt in place on the device for ``positions`` (same N), the
+    operator tables are kept. A point outside the plan's domain raises HFMMError
+    (HFMM_ERR_CAPACITY, -4) before anything changes."""
+    x, _ = _validate_setup(positions, state.k, state.p, state.N_max, None)
+    if x.shape[0] != state.n:
+        raise ValueError("rebuild keeps the number of points")
+    with torch.cuda.device(state.device):
+        pos = torch.as_tensor(x, dtype=torch.float64).to(state.device).contiguous()
+        _check(_lib.lib.hfmm_plan_rebuild(state.handle, pos.data_ptr()))
+        state.positions = pos
         state._refresh()
     return state
 

@@ -47,6 +47,9 @@ class HfmmInfo(ctypes.Structure):
 SIGNATURES = [
     ("hfmm_tree_build", _c_i32, [_c_vp, _c_i64, _c_i32, _c_i32, ctypes.POINTER(_c_vp)]),
     ("hfmm_plan_info", _c_i32, [_c_vp, ctypes.POINTER(HfmmInfo)]),
+    ("hfmm_tree_build_in_domain", _c_i32, [_c_vp, _c_i64, _c_i32, _c_i32, _c_vp, _c_dbl,
+                                           ctypes.POINTER(_c_vp)]),
+    ("hfmm_plan_rebuild", _c_i32, [_c_vp, _c_vp]),
     ("hfmm_plan_set_kernel", _c_i32, [_c_vp, _c_dbl, _c_i32, _c_i32, _c_vp, _c_vp]),
     ("hfmm_plan_set_level", _c_i32, [_c_vp, _c_i32, _c_i32] + [_c_vp] * 9),
     ("hfmm_plan_set_level_decode", _c_i32, [_c_vp, _c_i32, _c_i32] + [_c_vp] * 6),

@@ -687,6 +687,63 @@ int hfmm_tree_build(const double* pos_dev, int64_t n, int32_t n_max, int32_t max
     }
 }
 
+int hfmm_tree_build_in_domain(const double* pos_dev, int64_t n, int32_t n_max, int32_t max_depth,
+                              const double* pmin, double extent, hfmm_plan** out) {
+    if (!out) return fail(HFMM_ERR_ARG, "out is NULL");
+    *out = nullptr;
+    if (!pos_dev || n <= 0) return fail(HFMM_ERR_ARG, "positions must be a nonempty (N,3) array");
+    if (n_max < 1) return fail(HFMM_ERR_ARG, "N_max must be a positive integer");
+    if (max_depth < 1) return fail(HFMM_ERR_ARG, "a fixed domain needs a fixed max_depth >= 1");
+    if (!pmin || !std::isfinite(pmin[0]) || !std::isfinite(pmin[1]) || !std::isfinite(pmin[2]) ||
+        !std::isfinite(extent) || !(extent > 0))
+        return fail(HFMM_ERR_ARG, "the domain needs a finite corner and a positive extent");
+    if (n > (int64_t)INT32_MAX) return fail(HFMM_ERR_CAPACITY, "more than 2^31-1 points");
+    hfmm_plan* P = new hfmm_plan();
+    API_BEGIN
+    HFMM_CUDA(cudaGetDevice(&P->device));
+    require_device_ptr(pos_dev, "positions");
+    P->n = n;
+    P->n_max = n_max;
+    P->md_given = true;
+    P->md = max_depth;
+    P->domain_fixed = true;
+    P->extent = extent;
+    for (int a = 0; a < 3; ++a) P->pmin[a] = pmin[a];
+    P->d_err.alloc(1);
+    P->d_err.zero();
+    tree_build(P, pos_dev);
+    *out = P;
+    return HFMM_OK;
+    }
+    catch (const hfmm::Error& e) {
+        delete P;
+        return fail(e.code, e.msg);
+    }
+    catch (...) {
+        delete P;
+        return fail(HFMM_ERR_STATE, "tree build failed");
+    }
+}
+
+int hfmm_plan_rebuild(hfmm_plan* P, const double* pos_dev) {
+    if (!P) return fail(HFMM_ERR_ARG, "plan is NULL");
+    if (!P->domain_fixed) return fail(HFMM_ERR_STATE, "rebuild needs a plan built in a fixed domain");
+    if (!P->finalized) return fail(HFMM_ERR_STATE, "finalize the plan first");
+    if (P->batch_owner) return fail(HFMM_ERR_STATE, "the plan belongs to a batch (its graph holds the old tree)");
+    if (!pos_dev) return fail(HFMM_ERR_ARG, "positions are NULL");
+    API_BEGIN
+    require_device_ptr(pos_dev, "positions");
+    HFMM_CUDA(cudaDeviceSynchronize());   // no evaluate of the old tree in flight
+    tree_build(P, pos_dev);               // checks the domain before it changes anything
+    // lists, schedules and every tree-sized buffer follow the new tree; the operator
+    // tables (same depth, same domain, same level scales) are kept
+    P->finalized = false;
+    P->V.release();
+    const int rc = hfmm_plan_finalize(P);
+    return rc;
+    API_END
+}
+
 int hfmm_plan_info(const hfmm_plan* P, hfmm_info* o) {
     if (!P || !o) return fail(HFMM_ERR_ARG, "NULL argument");
     std::memset(o, 0, sizeof(*o));

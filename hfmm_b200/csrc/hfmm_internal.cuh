@@ -129,6 +129,9 @@ struct hfmm_plan {
     int64_t n = 0;
     int n_max = 0, md = 0, maxleaf = 0;
     bool md_given = false;
+    // moving geometry: the domain cube [pmin, pmin + extent]^3 is given, not measured, so
+    // the level scales (and the operator tables) stay valid when the points move
+    bool domain_fixed = false;
     double extent = 0, pmin[3] = {0, 0, 0};
     int64_t ref_max_boxes = 0;     // the reference's buffer size (reporting only)
     int64_t nb = 0;                // active boxes

@@ -466,9 +466,17 @@ void tree_build(hfmm_plan* P, const double* pos_dev) {
     HFMM_CUDA(cudaMemcpy(h_mm, mm.p, sizeof(h_mm), cudaMemcpyDeviceToHost));
     if (scalar_to_host(bad.p)) throw Error{HFMM_ERR_ARG, "positions must be finite"};
     double extent = 0.0;
-    for (int a = 0; a < 3; ++a) extent = std::max(extent, h_mm[3 + a] - h_mm[a]);
-    P->extent = extent;
-    for (int a = 0; a < 3; ++a) P->pmin[a] = h_mm[a];
+    if (P->domain_fixed) {   // every point inside the given cube, before the plan changes
+        extent = P->extent;
+        for (int a = 0; a < 3; ++a)
+            if (!(h_mm[a] >= P->pmin[a] && h_mm[3 + a] <= P->pmin[a] + extent))
+                throw Error{HFMM_ERR_CAPACITY, "points outside the plan's fixed domain"};
+        for (int a = 0; a < 3; ++a) h_mm[a] = P->pmin[a];
+    } else {
+        for (int a = 0; a < 3; ++a) extent = std::max(extent, h_mm[3 + a] - h_mm[a]);
+        P->extent = extent;
+        for (int a = 0; a < 3; ++a) P->pmin[a] = h_mm[a];
+    }
 
     // depth and buffer schedule of build_fmm_tree_auto (cubic.py:577-600)
     int md;

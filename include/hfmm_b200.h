@@ -69,6 +69,21 @@ typedef struct hfmm_info {
 int hfmm_tree_build(const double* pos_dev, int64_t n, int32_t n_max, int32_t max_depth,
                     hfmm_plan** out);
 
+/* Moving geometry (replaces the reference's fully-jit evaluator,
+ * kifmm/fulljit.py:57-328, and its guarded driver, driver.py:556-640, for the
+ * Helmholtz path): hfmm_tree_build with the domain cube [pmin, pmin + extent]^3
+ * and the depth given instead of measured, so the level scales, and with them the
+ * plan's operator tables, do not depend on where the points are. Then, per time
+ * step, hfmm_plan_rebuild(plan, new_positions) rebuilds the tree, the U/V/W/X
+ * lists and the schedules in place on the device and keeps the tables. Its
+ * certificate: a point outside the domain returns HFMM_ERR_CAPACITY before
+ * anything changes (the caller refits the domain and builds a new plan); a plan
+ * in a batch returns HFMM_ERR_STATE. Same n as the plan; synchronises the device.
+ * hfmm_plan_info then reports the realised counts. */
+int hfmm_tree_build_in_domain(const double* pos_dev, int64_t n, int32_t n_max, int32_t max_depth,
+                              const double* pmin, double extent, hfmm_plan** out);
+int hfmm_plan_rebuild(hfmm_plan* plan, const double* pos_dev);
+
 /* The sizes the reference's setup dict carries (max_depth, maxleaf, max_boxes,
  * domain_extent, pmin, list lengths: kifmm/setup.py:220-226, core.py:156-160). */
 int hfmm_plan_info(const hfmm_plan* plan, hfmm_info* out);
