@@ -23,7 +23,7 @@ from ._lib import check as _check, HFMMError, launch_count
 from .operators import level_tables, level_decodes, surface_pts, R_EQUIV, R_CHECK, n_surf
 
 __all__ = ["setup", "evaluate", "evaluate_field", "evaluate_into", "direct", "direct_at",
-           "HFMMState",
+           "HFMMState", "kernel_setup", "kernel_evaluate", "rebuild",
            "HFMMError", "launch_count", "PREC_FP64", "PREC_MIXED"]
 
 PREC_FP64 = _lib.HFMM_PREC_FP64
@@ -46,15 +46,18 @@ class HFMMState:
     (max_depth, maxleaf, max_boxes, domain_extent, list lengths).
     """
 
-    def __init__(self, handle, positions, k, p, N_max, device):
+    def __init__(self, handle, positions, k, p, N_max, device, kernel=None):
+        from .kernels import helmholtz
         self._h = handle
         self.positions = positions          # (N, 3) float64 on the device
         self.n = positions.shape[0]
-        self.k = float(k)
+        self.kernel = kernel if kernel is not None else helmholtz(k)
+        self.kind = self.kernel.kind
+        self.k = float(self.kernel.param)
         self.p = int(p)
         self.N_max = int(N_max)
         self.device = device
-        self.n_families = 1 if self.k == 0 else 2
+        self.n_families = self.kernel.families
         self._pin = {}
         self._refresh()
 
@@ -150,7 +153,7 @@ def _validate_setup(positions, k, p, N_max, max_depth):
 
 
 def setup(positions, k, p=4, N_max=16, max_depth=None, device=None, tables="device",
-          stream_tables=False, m2l_compress=None, domain=None):
+          stream_tables=False, m2l_compress=None, domain=None, kernel=None):
     """Build the plan for ``positions`` and wavenumber ``k`` (HFMM.setup, HFMM.py:55-80).
 
     ``p`` is the number of surface points per cube edge, ``N_max`` the leaf
@@ -167,6 +170,8 @@ def setup(positions, k, p=4, N_max=16, max_depth=None, device=None, tables="devi
     ``domain``: ``(pmin (3,), extent)``, a fixed domain cube instead of the points'
     bounding box (moving geometry, ``hfmm_b200.moving``); needs ``max_depth``. Every
     point must lie inside it; ``rebuild`` then moves the points within it.
+    ``kernel``: a ``hfmm_b200.kernels`` specification in place of the Helmholtz
+    components of ``k`` (``kernel_setup`` is the entry point for it).
     """
     if tables not in ("device", "host"):
         raise ValueError('tables must be "device" or "host"')
@@ -192,7 +197,7 @@ def setup(positions, k, p=4, N_max=16, max_depth=None, device=None, tables="devi
             _check(_lib.lib.hfmm_tree_build_in_domain(pos.data_ptr(), pos.shape[0], int(N_max),
                                                       int(max_depth), lo_c, ext,
                                                       _lib.ctypes.byref(h)))
-        state = HFMMState(h.value, pos, kf, p, N_max, dev)
+        state = HFMMState(h.value, pos, kf, p, N_max, dev, kernel)
         try:
             _load_tables(state, tables, stream_tables)
             if m2l_compress is not None:
@@ -226,22 +231,25 @@ def _load_tables(state, mode="device", streamed=False):
     extent = state.info["domain_extent"]
     eq = np.ascontiguousarray(surface_pts(p, R_EQUIV))
     ch = np.ascontiguousarray(surface_pts(p, R_CHECK))
+    yuk = state.kind == "yukawa"
+    _check(_lib.lib.hfmm_plan_set_kernel_kind(state.handle, 1 if yuk else 0))
     _check(_lib.lib.hfmm_plan_set_kernel(state.handle, state.k, p, state.n_families,
                                          eq.ctypes.data, ch.ctypes.data))
     _check(_lib.lib.hfmm_plan_set_streaming(state.handle, int(bool(streamed))))
     state.streamed = bool(streamed)
     for fam in range(state.n_families):
-        eps_rel = 1e-7 if fam == 0 else 1e-12          # HFMM.py:75-77
+        # HFMM.py:75-77; another kernel: build_operators_leveled's default (operators.py:572)
+        eps_rel = 1e-7 if fam == 0 else 1e-12
         for level in range(2, md + 1):
             if mode == "device":
-                t = level_decodes(p, level, extent, state.k, fam == 1, eps_rel)
+                t = level_decodes(p, level, extent, state.k, fam == 1, eps_rel, state.kind)
                 arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in
                         (t["F_up"][0], t["F_up"][1], t["F_up"][2], t["F_dn"][0], t["F_dn"][1],
                          t["F_dn"][2])]
                 _check(_lib.lib.hfmm_plan_set_level_decode(state.handle, fam, level,
                                                            *[a.ctypes.data for a in arrs]))
                 continue
-            t = level_tables(p, level, md, extent, state.k, fam == 1, eps_rel)
+            t = level_tables(p, level, md, extent, state.k, fam == 1, eps_rel, state.kind)
             arrs = [t["F_up"][0], t["F_up"][1], t["F_up"][2], t["F_dn"][0], t["F_dn"][1],
                     t["F_dn"][2], t["M2M_K"], t["L2L_K"], t["M2L_K"]]
             arrs = [None if a is None else np.ascontiguousarray(a, dtype=np.float64) for a in arrs]
@@ -258,7 +266,8 @@ def _load_compressed(state, eps):
     with torch.cuda.device(state.device):
         for fam in range(state.n_families):
             for level in range(2, state.max_depth + 1):
-                U, C = level_compressed(state.p, level, extent, state.k, fam == 1, eps, state.device)
+                U, C = level_compressed(state.p, level, extent, state.k, fam == 1, eps, state.device,
+                                        state.kind)
                 r = U.shape[1]
                 _check(_lib.lib.hfmm_plan_set_m2l_compressed(state.handle, fam, level, r,
                                                               U.data_ptr(), C.data_ptr()))
@@ -405,11 +414,15 @@ def direct_at(state, q_re, q_im, targets, field=False, stream=None):
     phi = torch.empty(m, dtype=torch.complex128, device=dev)
     E = torch.empty((m, 3), dtype=torch.complex128, device=dev) if field else None
     s = stream if stream is not None else torch.cuda.current_stream(dev)
-    _check(_lib.lib.hfmm_direct(state.positions.data_ptr(), q_re.data_ptr(),
-                                None if q_im is None else q_im.data_ptr(), state.n,
-                                targets.data_ptr(), m, state.k, phi.data_ptr(),
-                                None if E is None else E.data_ptr(), s.cuda_stream))
+    _check(_lib.lib.hfmm_direct_kernel(_kind_code(state), state.positions.data_ptr(),
+                                       q_re.data_ptr(), None if q_im is None else q_im.data_ptr(),
+                                       state.n, targets.data_ptr(), m, state.k, phi.data_ptr(),
+                                       None if E is None else E.data_ptr(), s.cuda_stream))
     return phi, E
+
+
+def _kind_code(state):
+    return 1 if getattr(state, "kind", "helmholtz") == "yukawa" else 0
 
 
 def direct(state, charges, targets, field=False):
@@ -432,10 +445,40 @@ def direct(state, charges, targets, field=False):
         phi = torch.empty(tg.shape[0], dtype=torch.complex128, device=dev)
         E = torch.empty((tg.shape[0], 3), dtype=torch.complex128, device=dev) if field else None
         s = torch.cuda.current_stream(dev)
-        _check(_lib.lib.hfmm_direct(state.positions.data_ptr(), q_re.data_ptr(),
-                                    None if q_im is None else q_im.data_ptr(), state.n,
-                                    tg.data_ptr(), tg.shape[0], state.k, phi.data_ptr(),
-                                    None if E is None else E.data_ptr(), s.cuda_stream))
+        _check(_lib.lib.hfmm_direct_kernel(_kind_code(state), state.positions.data_ptr(),
+                                           q_re.data_ptr(), None if q_im is None else q_im.data_ptr(),
+                                           state.n, tg.data_ptr(), tg.shape[0], state.k,
+                                           phi.data_ptr(), None if E is None else E.data_ptr(),
+                                           s.cuda_stream))
         phi = phi.cpu().numpy()
         E = E.cpu().numpy() if E is not None else None
     return (phi, E) if field else phi
+
+
+def kernel_setup(positions, kernel, p=4, N_max=16, max_depth=None, device=None, tables="device",
+                 m2l_compress=None, domain=None):
+    """The reference's ``kifmm.setup(positions, p, N_max, max_depth, kernel=...)``
+    (kifmm/setup.py:19-226) for a kernel of ``hfmm_b200.kernels`` (``yukawa(kappa)``,
+    ``LAPLACE``, ``helmholtz(k)``): the same plan, with that kernel in every particle
+    kernel, table and referee. Evaluate with ``kernel_evaluate`` (real charges, real
+    result, like ``kifmm.evaluate_setup``) or ``evaluate_field`` (complex charges by
+    linearity)."""
+    from .kernels import KernelSpec
+    if not isinstance(kernel, KernelSpec):
+        raise ValueError("kernel must be a hfmm_b200.kernels specification")
+    return setup(positions, kernel.param, p=p, N_max=N_max, max_depth=max_depth, device=device,
+                 tables=tables, m2l_compress=m2l_compress, domain=domain, kernel=kernel)
+
+
+def kernel_evaluate(state, charges, field=False, precision=PREC_FP64):
+    """kifmm.evaluate_setup(s, charges, field) (kifmm/setup.py:229-261) of a real
+    kernel plan: real charges (N,) -> potential (N,) or field -grad phi (N, 3), float64."""
+    if state.kind != "yukawa":
+        raise ValueError("kernel_evaluate is for the real kernels (yukawa, LAPLACE); "
+                         "use evaluate / evaluate_field for Helmholtz")
+    q = charges if isinstance(charges, torch.Tensor) else np.asarray(charges)
+    if (q.is_complex() if isinstance(q, torch.Tensor) else np.iscomplexobj(q)):
+        raise ValueError("charges must be real")
+    phi, E = _run(state, q, complex_ok=False, field=True, precision=precision)
+    out = E if field else phi
+    return out.real.copy() if isinstance(out, np.ndarray) else out.real.contiguous()

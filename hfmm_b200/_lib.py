@@ -50,6 +50,7 @@ SIGNATURES = [
     ("hfmm_tree_build_in_domain", _c_i32, [_c_vp, _c_i64, _c_i32, _c_i32, _c_vp, _c_dbl,
                                            ctypes.POINTER(_c_vp)]),
     ("hfmm_plan_rebuild", _c_i32, [_c_vp, _c_vp]),
+    ("hfmm_plan_set_kernel_kind", _c_i32, [_c_vp, _c_i32]),
     ("hfmm_plan_set_kernel", _c_i32, [_c_vp, _c_dbl, _c_i32, _c_i32, _c_vp, _c_vp]),
     ("hfmm_plan_set_level", _c_i32, [_c_vp, _c_i32, _c_i32] + [_c_vp] * 9),
     ("hfmm_plan_set_level_decode", _c_i32, [_c_vp, _c_i32, _c_i32] + [_c_vp] * 6),
@@ -68,6 +69,8 @@ SIGNATURES = [
     ("hfmm_export_densities", _c_i32, [_c_vp, _c_i32, _c_i32, _c_vp, _c_i64]),
     ("hfmm_direct", _c_i32, [_c_vp, _c_vp, _c_vp, _c_i64, _c_vp, _c_i64, _c_dbl, _c_vp, _c_vp,
                              _c_vp]),
+    ("hfmm_direct_kernel", _c_i32, [_c_i32, _c_vp, _c_vp, _c_vp, _c_i64, _c_vp, _c_i64, _c_dbl,
+                                    _c_vp, _c_vp, _c_vp]),
     ("hfmm_direct_scratch_bytes", _c_i64, [_c_i64, _c_i64]),
     ("hfmm_direct_async", _c_i32, [_c_vp, _c_vp, _c_vp, _c_i64, _c_vp, _c_i64, _c_dbl, _c_vp, _c_vp,
                                    _c_vp, _c_i64, _c_vp, _c_vp]),

@@ -33,8 +33,9 @@ def nonadjacent_displacements():
     return np.array(out, dtype=np.float64)
 
 
-def level_m2l_matrices(p, level, extent, k, imaginary, device, chunk=64):
-    """K_d = G((equiv + 2 d) s, equiv s), (316, n_s, n_s) float64 on ``device``."""
+def level_m2l_matrices(p, level, extent, k, imaginary, device, chunk=64, kind="helmholtz"):
+    """K_d = G((equiv + 2 d) s, equiv s), (316, n_s, n_s) float64 on ``device``; G a
+    Helmholtz component, or exp(-k r) / (4 pi r) for kind "yukawa"."""
     eq = torch.as_tensor(surface_pts(p, R_EQUIV), dtype=torch.float64, device=device)
     s = level_scale(extent, level)
     disp = torch.as_tensor(2.0 * nonadjacent_displacements(), dtype=torch.float64, device=device)
@@ -44,8 +45,11 @@ def level_m2l_matrices(p, level, extent, k, imaginary, device, chunk=64):
     for c0 in range(0, disp.shape[0], chunk):
         x = (eq[None, :, :] + disp[c0:c0 + chunk, None, :]) * s
         r = torch.linalg.norm(x[:, :, None, :] - y[None, None, :, :], dim=-1)
-        trig = torch.sin if imaginary else torch.cos
-        out[c0:c0 + chunk] = trig(float(k) * r) / r
+        if kind == "yukawa":
+            out[c0:c0 + chunk] = torch.exp(-float(k) * r) / (4.0 * np.pi * r)
+        else:
+            trig = torch.sin if imaginary else torch.cos
+            out[c0:c0 + chunk] = trig(float(k) * r) / r
     return out
 
 
@@ -62,8 +66,8 @@ def compress_level(K, eps):
     return U, C
 
 
-def level_compressed(p, level, extent, k, imaginary, eps, device):
-    K = level_m2l_matrices(p, level, extent, k, imaginary, device)
+def level_compressed(p, level, extent, k, imaginary, eps, device, kind="helmholtz"):
+    K = level_m2l_matrices(p, level, extent, k, imaginary, device, kind=kind)
     U, C = compress_level(K, eps)
     del K
     return U, C

@@ -164,6 +164,7 @@ EvalView view(hfmm_plan* P) {
     v.n_s = P->n_s;
     v.ld = P->ld;
     v.k = P->k;
+    v.yukawa = P->yukawa ? 1 : 0;
     v.pos_s = P->pos_s.p;
     v.pos_f = P->pos_f.p;
     v.q_s = P->q_s.p;
@@ -770,10 +771,22 @@ int hfmm_plan_info(const hfmm_plan* P, hfmm_info* o) {
     return HFMM_OK;
 }
 
+int hfmm_plan_set_kernel_kind(hfmm_plan* P, int32_t kind) {
+    if (!P) return fail(HFMM_ERR_ARG, "plan is NULL");
+    if (kind != HFMM_KERNEL_HELMHOLTZ && kind != HFMM_KERNEL_YUKAWA)
+        return fail(HFMM_ERR_ARG, "kind must be HFMM_KERNEL_HELMHOLTZ or HFMM_KERNEL_YUKAWA");
+    P->yukawa = kind == HFMM_KERNEL_YUKAWA;
+    P->n_s = 0;   // hfmm_plan_set_kernel comes next
+    P->finalized = false;
+    return HFMM_OK;
+}
+
 int hfmm_plan_set_kernel(hfmm_plan* P, double k, int32_t p, int32_t n_families,
                          const double* equiv_pts, const double* check_pts) {
     if (!P) return fail(HFMM_ERR_ARG, "plan is NULL");
     if (!std::isfinite(k)) return fail(HFMM_ERR_ARG, "k must be a finite real number");
+    if (P->yukawa && (n_families != 1 || k < 0))
+        return fail(HFMM_ERR_ARG, "the screened-Coulomb kernel has one family and kappa >= 0");
     if (p < 2) return fail(HFMM_ERR_ARG, "p must be an integer >= 2");
     if (n_families != 1 && n_families != 2) return fail(HFMM_ERR_ARG, "n_families must be 1 or 2");
     if (!equiv_pts || !check_pts) return fail(HFMM_ERR_ARG, "surfaces are NULL");
@@ -1156,9 +1169,22 @@ int hfmm_direct_async(const double* pos, const double* q_re, const double* q_im,
     API_END
 }
 
+int hfmm_direct_kernel(int32_t kind, const double* pos, const double* q_re, const double* q_im,
+                       int64_t n, const int32_t* targets, int64_t n_t, double k, double* phi,
+                       double* fld, void* stream);
+
 int hfmm_direct(const double* pos, const double* q_re, const double* q_im, int64_t n,
                 const int32_t* targets, int64_t n_t, double k, double* phi, double* fld,
                 void* stream) {
+    return hfmm_direct_kernel(HFMM_KERNEL_HELMHOLTZ, pos, q_re, q_im, n, targets, n_t, k, phi, fld,
+                              stream);
+}
+
+int hfmm_direct_kernel(int32_t kind, const double* pos, const double* q_re, const double* q_im,
+                       int64_t n, const int32_t* targets, int64_t n_t, double k, double* phi,
+                       double* fld, void* stream) {
+    if (kind != HFMM_KERNEL_HELMHOLTZ && kind != HFMM_KERNEL_YUKAWA)
+        return fail(HFMM_ERR_ARG, "kind must be HFMM_KERNEL_HELMHOLTZ or HFMM_KERNEL_YUKAWA");
     if (!pos || !q_re || !targets || !phi || n <= 0 || n_t < 0)
         return fail(HFMM_ERR_ARG, "invalid direct-sum arguments");
     if (!std::isfinite(k)) return fail(HFMM_ERR_ARG, "k must be finite");
@@ -1176,7 +1202,7 @@ int hfmm_direct(const double* pos, const double* q_re, const double* q_im, int64
     err.alloc(1);
     err.zero((cudaStream_t)stream);
     direct_sum(pos, q_re, q_im, n, targets, n_t, k, phi, fld, scratch.p, splits,
-               (cudaStream_t)stream, err.p);
+               (cudaStream_t)stream, err.p, kind == HFMM_KERNEL_YUKAWA ? 1 : 0);
     int h = 0;
     HFMM_CUDA(cudaMemcpyAsync(&h, err.p, sizeof(int), cudaMemcpyDeviceToHost, (cudaStream_t)stream));
     HFMM_CUDA(cudaStreamSynchronize((cudaStream_t)stream));

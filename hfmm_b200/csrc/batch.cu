@@ -279,7 +279,7 @@ int hfmm_batch_capture(hfmm_batch* B) {
                         double* rE = io.ref.p + 2 * io.n_t;
                         direct_sum(io.pos, io.q_re, io.q_im, P->n, io.tg, io.n_t, P->k, rphi,
                                    io.E ? rE : nullptr, io.scratch.p, io.n_split, B->streams[s],
-                                   P->d_err.p);
+                                   P->d_err.p, P->yukawa ? 1 : 0);
                         HFMM_LAUNCH(k_check_sums, 1, 256, 0, B->streams[s], io.phi, io.E, io.tg,
                                     io.n_t, P->n, rphi, rE, io.sums, P->d_err.p);
                     }

@@ -1,5 +1,7 @@
 // Direct-sum referee: phi_t = sum_{s: r > 0} q_s e^{ikr} / r at sampled targets
 // (test.py:11-18), and the field -grad phi = sum q_s e^{ikr} (1 - ikr) / r^3 (x_t - x_s).
+// With the screened-Coulomb kernel (yukawa != 0, k = kappa): phi_t = sum q_s G(r),
+// G = exp(-kappa r) / (4 pi r), field sum q_s (1 + kappa r) exp(-kappa r) / (4 pi r^3) d.
 //
 // Sources are split into n_split contiguous chunks; each (target block, chunk)
 // CTA writes its partial sums to scratch, and a second kernel adds the chunks
@@ -61,7 +63,7 @@ __global__ void __launch_bounds__(DT) k_direct_partial(const double* __restrict_
                                                        const double* __restrict__ q_im, int64_t n,
                                                        const int32_t* __restrict__ tg, int64_t n_t,
                                                        double k, int field, int n_split,
-                                                       double* scratch, int* err) {
+                                                       double* scratch, int* err, int yukawa) {
     __shared__ double sx[DSTAGE], sy[DSTAGE], sz[DSTAGE], sqr[DSTAGE], sqi[DSTAGE];
     const int64_t ti = blockIdx.x * (int64_t)DT + threadIdx.x;
     const int split = blockIdx.y;
@@ -102,7 +104,12 @@ __global__ void __launch_bounds__(DT) k_direct_partial(const double* __restrict_
             if (!(r2 > 0.0)) continue;
             double ir = rsqrt(r2), r = r2 * ir;
             double kr = k * r, sn, cs;
-            sincos_reduced(kr, &sn, &cs);
+            if (yukawa) {   // real kernel: w = G, field weight (1 + kr) G / r^2
+                cs = exp(-kr) * 0.07957747154594767;
+                sn = 0.0;
+            } else {
+                sincos_reduced(kr, &sn, &cs);
+            }
             // w = e^{ikr}/r; q w
             double wr = cs * ir, wi = sn * ir;
             acc[0] += sqr[i] * wr - sqi[i] * wi;
@@ -111,6 +118,10 @@ __global__ void __launch_bounds__(DT) k_direct_partial(const double* __restrict_
                 // e^{ikr}(1 - ikr)/r^3 = ((cs + kr sn) + i (sn - kr cs)) / r^3
                 double ir3 = ir * ir * ir;
                 double fr = (cs + kr * sn) * ir3, fi = (sn - kr * cs) * ir3;
+                if (yukawa) {
+                    fr = cs * (1.0 + kr) * ir3;
+                    fi = 0.0;
+                }
                 double gr = sqr[i] * fr - sqi[i] * fi, gi = sqr[i] * fi + sqi[i] * fr;
                 acc[2] += gr * dx;
                 acc[3] += gi * dx;
@@ -152,11 +163,11 @@ int direct_splits(int64_t n, int64_t n_t) {
 
 void direct_sum(const double* pos, const double* q_re, const double* q_im, int64_t n,
                 const int32_t* targets, int64_t n_t, double k, double* phi, double* fld,
-                double* scratch, int n_split, cudaStream_t s, int* err) {
+                double* scratch, int n_split, cudaStream_t s, int* err, int yukawa) {
     if (n_t == 0) return;
     dim3 grid((unsigned)ceil_div(n_t, DT), (unsigned)n_split);
     HFMM_LAUNCH(k_direct_partial, grid, DT, 0, s, pos, q_re, q_im, n, targets, n_t, k,
-                fld ? 1 : 0, n_split, scratch, err);
+                fld ? 1 : 0, n_split, scratch, err, yukawa);
     HFMM_LAUNCH(k_direct_reduce, (unsigned)ceil_div(n_t, 256), 256, 0, s, scratch, n_t, n_split,
                 fld ? 1 : 0, phi, fld);
 }

@@ -132,6 +132,10 @@ struct hfmm_plan {
     // moving geometry: the domain cube [pmin, pmin + extent]^3 is given, not measured, so
     // the level scales (and the operator tables) stay valid when the points move
     bool domain_fixed = false;
+    // the kernel seam: false, the Helmholtz components cos|sin(kr)/r (one or two
+    // families); true, the screened-Coulomb kernel exp(-k r) / (4 pi r), k = kappa >= 0
+    // (one family; kappa = 0: Laplace)
+    bool yukawa = false;
     double extent = 0, pmin[3] = {0, 0, 0};
     int64_t ref_max_boxes = 0;     // the reference's buffer size (reporting only)
     int64_t nb = 0;                // active boxes
@@ -238,7 +242,7 @@ void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double*
                    double* fld, cudaStream_t s, bool mixed = false);
 void direct_sum(const double* pos, const double* q_re, const double* q_im, int64_t n,
                 const int32_t* targets, int64_t n_t, double k, double* phi, double* fld,
-                double* scratch, int n_split, cudaStream_t s, int* err);
+                double* scratch, int n_split, cudaStream_t s, int* err, int yukawa = 0);
 int direct_splits(int64_t n, int64_t n_t);
 
 // ---------------------------------------------------------------- GEMM launcher

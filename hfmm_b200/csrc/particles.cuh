@@ -7,7 +7,8 @@ namespace hfmm {
 struct EvalView {
     int64_t n, nb;
     int n_s, ld;
-    double k;
+    double k;                  // Helmholtz wavenumber, or the screening constant kappa
+    int yukawa;                // 0: Helmholtz (two families); 1: exp(-kappa r) / (4 pi r)
     const double* pos_s;       // 3 x n, leaf-major sorted
     const float* pos_f;        // 6 x n: FP32 hi parts x|y|z, then lo parts (pos = hi + lo)
     const double* q_s;         // R x n, leaf-major sorted
@@ -73,6 +74,24 @@ __device__ __forceinline__ void sincos_phase64(double x, double* s, double* c) {
         *c = fma(-x2, pc, 1.0);                         // 1 - x^2 (1/2! - x^2/4! + ...)
     } else {
         sincos(x, s, c);
+    }
+}
+
+// The kernel seam of the particle kernels. Helmholtz: (sn, cs) = sin, cos of the phase
+// kr, so family 0 is cs / r, family 1 sn / r and their field weights (cs + kr sn) / r^3
+// and (sn - kr cs) / r^3 (HFMM.py:25-40). The screened-Coulomb kernel (one family,
+// jaxfmm/kernels/yukawa/kernel.py:36-75; kappa = 0 is Laplace,
+// kernels/laplace/kernel.py:40-104) puts exp(-kr) / (4 pi) in both slots, so family 0's
+// value cs / r and field weight (cs + kr sn) / r^3 = (1 + kr) exp(-kr) / (4 pi r^3) come
+// out of the same expressions.
+constexpr double INV_4PI = 0.07957747154594767;
+__device__ __forceinline__ void kernel_pair64(int yukawa, double kr, double* sn, double* cs) {
+    if (yukawa) {
+        const double e = exp(-kr) * INV_4PI;
+        *sn = e;
+        *cs = e;
+    } else {
+        sincos_phase64(kr, sn, cs);
     }
 }
 

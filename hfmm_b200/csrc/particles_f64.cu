@@ -69,7 +69,7 @@ __global__ void __launch_bounds__(512) k_surface_from_particles(
                         double ir = rsqrt(r2);
                         double rr = r2 * ir;
                         double sn, cs;
-                        sincos_phase64(v.k * rr, &sn, &cs);
+                        kernel_pair64(v.yukawa, v.k * rr, &sn, &cs);
                         double wc = cs * ir, ws = sn * ir;
 #pragma unroll
                         for (int r = 0; r < R; ++r) {
@@ -145,7 +145,7 @@ __global__ void __launch_bounds__(256) k_particles_from_surface(
                 double rr = r2 * ir;
                 double sn, cs;
                 double kr = v.k * rr;
-                sincos_phase64(kr, &sn, &cs);
+                kernel_pair64(v.yukawa, kr, &sn, &cs);
                 double w[2] = {cs * ir, sn * ir};
                 double wf[2] = {0.0, 0.0};
                 if (FIELD) {
@@ -234,7 +234,11 @@ __global__ void __launch_bounds__(128) k_p2p(EvalView v, const int32_t* __restri
                     double rr = sqrt(d2);
                     double kr = v.k * rr;
                     double sn, cs;
-                    sincos(kr, &sn, &cs);
+                    if (v.yukawa) {
+                        sn = cs = exp(-kr) * INV_4PI;
+                    } else {
+                        sincos(kr, &sn, &cs);
+                    }
                     double ir = 1.0 / rr;
                     double w[2] = {cs * ir, sn * ir};
                     double wf[2] = {0.0, 0.0};

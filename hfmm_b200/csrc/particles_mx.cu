@@ -142,7 +142,10 @@ __global__ void __launch_bounds__(WARPS * 32, 8) k_p2p_mx(EvalView v, const int3
                             const float rr = d2 * ir;
                             const float kr = kf * rr;
                             float sn, cs_;
-                            sincos_phase(kr, &sn, &cs_);
+                            if (v.yukawa)   // the kernel seam (particles.cuh): one family
+                                sn = cs_ = __expf(-kr) * 0.0795774715f;
+                            else
+                                sincos_phase(kr, &sn, &cs_);
                             const float w[2] = {cs_ * ir, sn * ir};
                             float wf[2] = {0.f, 0.f};
                             if (FIELD) {

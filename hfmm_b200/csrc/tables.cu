@@ -46,8 +46,10 @@ __device__ __forceinline__ void disp_of(int c, double& dx, double& dy, double& d
     dz = 2.0 * c_disp.d[c][2];
 }
 
+// fam: 0 cos(kw r) / r, 1 sin(kw r) / r (the Helmholtz components), 2 exp(-kw r) / (4 pi r)
+// (the screened-Coulomb kernel; kw = 0: Laplace)
 __global__ void k_gen(int kind, const double* __restrict__ eq, const double* __restrict__ ck,
-                      int n_s, int ld, double s, double kw, int imag, double* out) {
+                      int n_s, int ld, double s, double kw, int fam, double* out) {
     const int c = blockIdx.z;
     const int m = blockIdx.y * blockDim.y + threadIdx.y;   // row: target point
     const int kk = blockIdx.x * blockDim.x + threadIdx.x;  // column: source point
@@ -85,9 +87,13 @@ __global__ void k_gen(int kind, const double* __restrict__ eq, const double* __r
     }
     const double dx = __dsub_rn(x[0], y[0]), dy = __dsub_rn(x[1], y[1]), dz = __dsub_rn(x[2], y[2]);
     const double r = sqrt(__dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz)));
+    if (fam == 2) {
+        *o = exp(-kw * r) / (4.0 * M_PI * r);
+        return;
+    }
     double sn, cs;
     sincos(kw * r, &sn, &cs);
-    *o = (imag ? sn : cs) / r;
+    *o = (fam == 1 ? sn : cs) / r;
 }
 
 __device__ __forceinline__ float tf32_round(float x) {
@@ -99,7 +105,7 @@ __device__ __forceinline__ float tf32_round(float x) {
 // halves as A [fam][c][m][k] (the tcgen05 path), hi at ws, lo after the hi block.
 // The fastest thread index runs along the contiguous axis of the layout.
 __global__ void k_gen_m2l_stream(const double* __restrict__ eq, int n_s, int ld, double s, double kw,
-                                 int n_fam, int layout, void* ws) {
+                                 int n_fam, int yukawa, int layout, void* ws) {
     const int c = blockIdx.z;
     const int a = blockIdx.x * blockDim.x + threadIdx.x;   // contiguous axis
     const int b = blockIdx.y * blockDim.y + threadIdx.y;
@@ -118,10 +124,14 @@ __global__ void k_gen_m2l_stream(const double* __restrict__ eq, int n_s, int ld,
         const double dz = __dsub_rn(__dmul_rn(__dadd_rn(eq[2 * n_s + m], oz), s),
                                     __dmul_rn(eq[2 * n_s + kk], s));
         const double r = sqrt(__dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz)));
-        double sn, cs;
-        sincos(kw * r, &sn, &cs);
-        v[0] = cs / r;
-        v[1] = sn / r;
+        if (yukawa) {
+            v[0] = exp(-kw * r) / (4.0 * M_PI * r);
+        } else {
+            double sn, cs;
+            sincos(kw * r, &sn, &cs);
+            v[0] = cs / r;
+            v[1] = sn / r;
+        }
     }
     if (layout == 0) {
         double* o = static_cast<double*>(ws);
@@ -148,7 +158,7 @@ void generate_m2l_stream(hfmm_plan* P, int level, bool mixed, void* ws, cudaStre
     dim3 blk(32, 8);
     dim3 grid((unsigned)ceil_div(P->ld, 32), (unsigned)ceil_div(P->ld, 8), 316u);
     HFMM_LAUNCH(k_gen_m2l_stream, grid, blk, 0, st, P->equiv_pts.p, P->n_s, P->ld, s, P->k,
-                P->n_fam, mixed ? 1 : 0, ws);
+                P->n_fam, P->yukawa ? 1 : 0, mixed ? 1 : 0, ws);
 }
 
 void generate_tables(hfmm_plan* P, int fam, int level) {
@@ -157,7 +167,7 @@ void generate_tables(hfmm_plan* P, int fam, int level) {
     const double extent = P->extent;
     const double s = extent * std::ldexp(1.0, -(level + 1));
     const double s_child = extent * std::ldexp(1.0, -(level + 2));
-    const int imag = fam == 1 ? 1 : 0;
+    const int imag = P->yukawa ? 2 : (fam == 1 ? 1 : 0);   // the k_gen family code
     const size_t mat = (size_t)ld * ld;
     dim3 blk(32, 8);
     auto grid = [&](int count) {

@@ -59,6 +59,28 @@ def component_matrix(k, imaginary):
     return G
 
 
+def screened_matrix(kappa):
+    """G(x, y) = exp(-kappa r) / (4 pi r) with the ULP-relative zero, the reference's
+    yukawa G_np (jaxfmm/kernels/yukawa/kernel.py:36-42); kappa = 0 gives its Laplace
+    G_np 1 / (4 pi r) (kernels/laplace/kernel.py:40-43) to the last bit."""
+    kappa = float(kappa)
+
+    def G(x, y):
+        d = x[:, None, :] - y[None, :, :]
+        r = np.sqrt((d ** 2).sum(-1))
+        with np.errstate(divide="ignore", invalid="ignore"):
+            K = np.exp(-kappa * r) / (4.0 * np.pi * r)
+        K[r <= 16 * np.finfo(r.dtype).eps * r.max(initial=0.0)] = 0.0
+        return K
+    return G
+
+
+def family_matrix(k, imaginary, kind="helmholtz"):
+    """The kernel matrix of one family: a Helmholtz component, or the screened-Coulomb
+    kernel (kind "yukawa", k = kappa; one family)."""
+    return screened_matrix(k) if kind == "yukawa" else component_matrix(k, imaginary)
+
+
 def damped_factors(A, eps_rel):
     U, s, Vt = np.linalg.svd(A, full_matrices=False)
     eps = eps_rel * s[0]
@@ -69,10 +91,10 @@ def level_scale(domain_extent, level):
     return float(domain_extent) * 0.5 ** (level + 1)
 
 
-def level_decodes(p, level, domain_extent, k, imaginary, eps_rel):
+def level_decodes(p, level, domain_extent, k, imaginary, eps_rel, kind="helmholtz"):
     """Only the two damped-SVD decodes of one family at one level (the kernel matrices
     are then generated on the device, hfmm_plan_set_level_decode)."""
-    G = component_matrix(k, imaginary)
+    G = family_matrix(k, imaginary, kind)
     equiv = surface_pts(p, R_EQUIV)
     check = surface_pts(p, R_CHECK)
     s = level_scale(domain_extent, level)
@@ -81,9 +103,9 @@ def level_decodes(p, level, domain_extent, k, imaginary, eps_rel):
     return dict(F_up=F_up, F_dn=F_dn)
 
 
-def level_tables(p, level, max_depth, domain_extent, k, imaginary, eps_rel):
+def level_tables(p, level, max_depth, domain_extent, k, imaginary, eps_rel, kind="helmholtz"):
     """Tables of one kernel family at one level, in the layout hfmm_plan_set_level takes."""
-    G = component_matrix(k, imaginary)
+    G = family_matrix(k, imaginary, kind)
     equiv = surface_pts(p, R_EQUIV)
     check = surface_pts(p, R_CHECK)
     n_s = equiv.shape[0]

@@ -34,6 +34,12 @@ extern "C" {
 #define HFMM_ERR_CAPACITY -4  /* a size limit was exceeded                           */
 #define HFMM_ERR_DEVICE -5    /* a kernel raised its device error flag               */
 
+/* Kernel kinds of the kernel seam (hfmm_plan_set_kernel_kind; the reference's
+ * Kernel specification, jaxfmm/kernels/spec.py:10-62). */
+#define HFMM_KERNEL_HELMHOLTZ 0   /* cos(kr)/r and sin(kr)/r, HFMM.py:12-52            */
+#define HFMM_KERNEL_YUKAWA 1      /* exp(-kappa r)/(4 pi r), kernels/yukawa/kernel.py:10-75;
+                                     kappa = 0 is Laplace, kernels/laplace/kernel.py:104  */
+
 #define HFMM_PREC_FP64 0      /* plain path: every phase in float64                  */
 #define HFMM_PREC_MIXED 1     /* M2L as split 3xTF32 on tcgen05 (FP32 accumulation in
                                  short chains, folded into FP64), P2P in FP32 with an
@@ -87,6 +93,14 @@ int hfmm_plan_rebuild(hfmm_plan* plan, const double* pos_dev);
 /* The sizes the reference's setup dict carries (max_depth, maxleaf, max_boxes,
  * domain_extent, pmin, list lengths: kifmm/setup.py:220-226, core.py:156-160). */
 int hfmm_plan_info(const hfmm_plan* plan, hfmm_info* out);
+
+/* Choose the kernel before hfmm_plan_set_kernel (default HFMM_KERNEL_HELMHOLTZ):
+ * HFMM_KERNEL_YUKAWA takes kappa >= 0 as set_kernel's k, one family, and decode
+ * tables of that kernel; every particle kernel, the device table generation, the
+ * mixed near field and the direct-sum referee then evaluate exp(-kappa r)/(4 pi r)
+ * (the reference's kifmm.setup(..., kernel=yukawa(kappa)) or kernel=LAPLACE,
+ * kifmm/setup.py:19-226). */
+int hfmm_plan_set_kernel_kind(hfmm_plan* plan, int32_t kind);
 
 /* Kernel: wavenumber k, p points per cube edge, n_families = 2 (cos and sin
  * components, HFMM.py:65-80) or 1 (k == 0, HFMM.py:71-72). equiv_pts and
@@ -197,6 +211,13 @@ int hfmm_export_densities(const hfmm_plan* plan, int32_t which, int32_t columns,
 int hfmm_direct(const double* pos_dev, const double* q_re_dev, const double* q_im_dev,
                 int64_t n, const int32_t* targets_dev, int64_t n_t, double k,
                 double* phi_out_dev, double* field_out_dev, void* stream);
+/* hfmm_direct for a kernel kind: HFMM_KERNEL_YUKAWA sums q_s exp(-k r)/(4 pi r)
+ * (field: q_s (1 + k r) exp(-k r)/(4 pi r^3) (x_t - x_s)) with complex charges by
+ * linearity. Replaces the reference's own direct checks of its other kernels. */
+int hfmm_direct_kernel(int32_t kind, const double* pos_dev, const double* q_re_dev,
+                       const double* q_im_dev, int64_t n, const int32_t* targets_dev,
+                       int64_t n_t, double k, double* phi_out_dev, double* field_out_dev,
+                       void* stream);
 
 /* hfmm_direct without allocation or synchronisation, for a check that overlaps
  * other work: the caller gives a device scratch of hfmm_direct_scratch_bytes(n,

@@ -27,7 +27,7 @@ from .tree import (morton_encode, morton_decode, build_fmm_tree, build_fmm_tree_
                    assign_particles, box_geometry, NEIGH_OFFSETS, ADJ_CHILD_MASK)
 from .lists import build_v, build_u, build_wx, near_pairs
 from .hfmm import (setup, evaluate, evaluate_setup, evaluate_complex, kifmm_setup,
-                   direct, direct_field, relative_error)
+                   direct, direct_field, relative_error, YukawaKernel, kernel_setup)
 
 __all__ = [
     "n_surf", "surface_pts", "R_EQUIV", "R_CHECK",
@@ -36,5 +36,5 @@ __all__ = [
     "assign_particles", "box_geometry", "NEIGH_OFFSETS", "ADJ_CHILD_MASK",
     "build_v", "build_u", "build_wx", "near_pairs",
     "setup", "evaluate", "evaluate_setup", "evaluate_complex", "kifmm_setup",
-    "direct", "direct_field", "relative_error",
+    "direct", "direct_field", "relative_error", "YukawaKernel", "kernel_setup",
 ]

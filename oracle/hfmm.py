@@ -81,6 +81,60 @@ class HelmholtzComponent:
         return 4 * np.pi * self.field_weight(d2)
 
 
+class YukawaKernel:
+    """The reference's screened-Coulomb kernel G = exp(-kappa r) / (4 pi r)
+    (jaxfmm/kernels/yukawa/kernel.py:10-75); kappa = 0 is its Laplace kernel
+    1 / (4 pi r) (jaxfmm/kernels/laplace/kernel.py:40-104), whose value and field
+    functions are the same expressions with exp(0) = 1."""
+
+    def __init__(self, kappa):
+        kappa = float(kappa)
+        if not (np.isfinite(kappa) and kappa >= 0):
+            raise ValueError("kappa must be finite and >= 0")
+        self.kappa = kappa
+        self.name = "laplace" if kappa == 0 else f"yukawa(kappa={kappa:g})"
+
+        def G_np(x, y):
+            d = x[:, None, :] - y[None, :, :]
+            r = np.sqrt((d ** 2).sum(-1))
+            with np.errstate(divide="ignore", invalid="ignore"):
+                K = np.exp(-kappa * r) / (4.0 * np.pi * r)
+            K[r <= 16 * EPS * r.max(initial=0.0)] = 0.0          # ULP-relative
+            return K
+        self.G_np = G_np
+
+    def g_box(self, r):
+        mx = r.max(axis=tuple(range(1, r.ndim)), keepdims=True)
+        ok = r > 16 * EPS * mx
+        return np.where(ok, 0.25 / np.pi * np.exp(-self.kappa * r) / np.where(ok, r, 1.0), 0.0)
+
+    def field_weight(self, d2):
+        """(1 + kappa r) exp(-kappa r) / r^3 (4 pi-free), 0 at d2 = 0."""
+        safe = np.where(d2 > 0, d2, 1.0)
+        r = np.sqrt(safe)
+        return np.where(d2 > 0, (1 + self.kappa * r) * np.exp(-self.kappa * r) / (safe * r), 0.0)
+
+    def g_grad_box(self, d):
+        d2 = np.sum(d * d, axis=-1)
+        mx = d2.max(axis=tuple(range(1, d2.ndim)), keepdims=True)
+        ok = d2 > (16 * EPS) ** 2 * mx
+        return d * (0.25 / np.pi * self.field_weight(np.where(ok, d2, 0.0)))[..., None]
+
+    def k2(self, d2):
+        r = np.sqrt(np.where(d2 > 0, d2, 1.0))
+        return np.where(d2 > 0, np.exp(-self.kappa * r) / r, 0.0)
+
+    def k2g(self, d2):
+        return self.field_weight(d2)
+
+
+def kernel_setup(positions, kernel, p=4, N_max=16, max_depth=None):
+    """kifmm.setup(positions, p, N_max, max_depth, kernel=...) for a real kernel
+    (kifmm/setup.py:19-226, leveled operators, FP64 near field): the oracle of the
+    other kernels the CUDA path takes through its kernel seam."""
+    return kifmm_setup(positions, int(p), int(N_max), max_depth, kernel)
+
+
 # ---------------------------------------------------------------- setup
 def kifmm_setup(positions, p, N_max, max_depth, kernel, eps_rel=1e-7):
     """Leveled KIFMM setup (kifmm/setup.py:19-226 with HFMM's arguments)."""

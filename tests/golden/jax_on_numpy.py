@@ -549,6 +549,17 @@ def _cumsum(a, axis=None, dtype=None, **_):
 
 
 
+def _bincount(x, weights=None, minlength=0, *, length=None):
+    """jnp.bincount: with ``length`` the output has exactly that many bins and values
+    at or above it are dropped (the jit-static form); without it, NumPy's."""
+    x = np.asarray(x).astype(np.int64)
+    w = None if weights is None else np.asarray(weights)
+    if length is None:
+        return _wrap(np.bincount(x, weights=w, minlength=minlength))
+    keep = (x >= 0) & (x < length)
+    return _wrap(np.bincount(x[keep], weights=None if w is None else w[keep], minlength=length)[:length])
+
+
 def _searchsorted(a, v, side="left", sorter=None, method=None):
     return _wrap(np.searchsorted(np.asarray(a), np.asarray(v), side=side, sorter=sorter))
 
@@ -558,7 +569,7 @@ class _NumpyModule(types.ModuleType):
         "searchsorted": _searchsorted,
         "asarray": _asarray, "array": _asarray, "argsort": _argsort, "sort": _sort,
         "take": _take, "take_along_axis": _take_along_axis, "unique": _unique,
-        "nonzero": _nonzero, "where": _where, "cumsum": _cumsum,
+        "nonzero": _nonzero, "where": _where, "cumsum": _cumsum, "bincount": _bincount,
         "ndarray": np.ndarray,
     }
 

@@ -23,6 +23,7 @@ environment variable HFMM0_REFERENCE; run from the repo root:
 
     python tests/golden/make_golden.py --reference DIR [--edge] [case ...]
     python tests/golden/make_golden.py --reference DIR --p12
+    python tests/golden/make_golden.py --reference DIR --kernels
     python tests/golden/make_golden.py --reference DIR --grid
     python tests/golden/make_golden.py --reference DIR --phases
     python tests/golden/make_golden.py --reference DIR --c1
@@ -63,6 +64,39 @@ P12 = {
     "cplx3000_k10_p12": (complex_uniform, 3000, 10.0, 12, 64, None, True),
     "sphere2000_k10_p12_d4": (sphere_clusters, 2000, 10.0, 12, 32, 4, True),
 }
+
+# Other kernels through the reference's Kernel seam (tests/golden/kernels/):
+# kifmm.setup(positions, p, N_max, kernel=...) with the exact FP64 near field
+# (p2p_mixed=False), potential and field of real charges (kifmm/setup.py:19-261).
+# name: (cloud, n, kernel ("yukawa", kappa) or ("laplace", None), p, N_max)
+KERNEL_CASES = {
+    "yukawa1500_kappa3_p5": (uniform, 1500, ("yukawa", 3.0), 5, 24),
+    "yukawa2000_kappa8_p4_clustered": (clustered, 2000, ("yukawa", 8.0), 4, 16),
+    "laplace1500_p5": (uniform, 1500, ("laplace", None), 5, 24),
+    "laplace2500_p4_sphere": (sphere_clusters, 2500, ("laplace", None), 4, 16),
+}
+
+
+def run_kernels(folder, keep=False):
+    """The reference's kifmm.setup / evaluate_setup with its yukawa and LAPLACE kernels."""
+    from jaxfmm import kifmm
+    from jaxfmm.kernels import LAPLACE, yukawa
+    os.makedirs(folder, exist_ok=True)
+    for name, (fn, n, (kind, kappa), p, nmax) in KERNEL_CASES.items():
+        if keep and os.path.exists(os.path.join(folder, name + ".npz")):
+            continue
+        t = time.time()
+        pos, q = fn(n)
+        q = np.real(q)
+        kern = LAPLACE if kind == "laplace" else yukawa(kappa)
+        s = kifmm.setup(pos, p=p, N_max=nmax, kernel=kern, p2p_mixed=False)
+        pot = np.asarray(kifmm.evaluate_setup(s, q))
+        fld = np.asarray(kifmm.evaluate_setup(s, q, field=True))
+        np.savez_compressed(os.path.join(folder, name + ".npz"), positions=pos, charges=q,
+                            kind=kind, kappa=np.float64(kappa or 0.0), p=p, N_max=nmax,
+                            realised_depth=int(s["max_depth"]), pot=pot, field=fld)
+        print(name, "depth", int(s["max_depth"]), f"{time.time() - t:.0f} s", flush=True)
+
 
 # Edge cases (tests/golden/edge/): a single point, two points, one box over its
 # leaf size, a plane (depth refinement), many duplicates, explicit depths, and the
@@ -403,6 +437,9 @@ def main():
     ap.add_argument("--reference", default=os.environ.get("HFMM0_REFERENCE"),
                     help="the reference source tree (or set HFMM0_REFERENCE)")
     ap.add_argument("--p12", action="store_true", help="the expansion-order-12 cases, into p12/")
+    ap.add_argument("--kernels", action="store_true",
+                    help="the Yukawa and Laplace kernels of kifmm.setup, into kernels/")
+    ap.add_argument("--keep", action="store_true", help="--kernels: skip fixtures already made")
     ap.add_argument("--edge", action="store_true", help="the edge cases, into edge/")
     ap.add_argument("--grid", action="store_true",
                     help="the reference's test.py grid, into grid/test_py_grid.npz")
@@ -421,6 +458,8 @@ def main():
     HFMM, seen = load_reference(a.reference)
     if a.tables:
         return run_tables(HFMM, os.path.join(HERE, "tables"))
+    if a.kernels:
+        return run_kernels(os.path.join(HERE, "kernels"), keep=a.keep)
     if a.errors:
         return run_errors(HFMM, os.path.join(HERE, "errors"))
     if a.c1:

@@ -92,3 +92,13 @@ def test_map_over_nothing_keeps_the_element_shape():
 def test_scan_over_nothing_returns_the_carry_and_empty_outputs():
     carry, ys = J._scan(lambda c, x: (c + x.sum(), x * 2.0), 1.0, np.zeros((0, 3)))
     assert carry == 1.0 and ys.shape == (0, 3)
+
+
+def test_bincount_length_drops_out_of_range_values():
+    """jnp.bincount(x, weights, length=L): exactly L bins, values >= L dropped."""
+    import jax_on_numpy as jn
+    jnp = jn._NumpyModule("jax.numpy")
+    assert np.array_equal(jnp.bincount(np.array([0, 1, 1, 5]), length=3), [1, 2, 0])
+    w = np.array([0.5, 1.0, 2.0, 4.0])
+    assert np.allclose(jnp.bincount(np.array([2, 2, 0, 9]), weights=w, length=4), [2.0, 0, 1.5, 0])
+    assert np.array_equal(jnp.bincount(np.array([3, 1])), [0, 1, 0, 1])
