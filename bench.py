@@ -889,7 +889,8 @@ def run_batch(a, cfg, rank, world, local_rank):
             "dtype": "f32+tf32x3+f64",
             "data": "synthetic (seeded uniform points and N(0,1) complex charges)",
             "config": {"workload": cfg["workload"], "problems": len(probs), "points_total": n_tot,
-                       "n_streams": ab.batch.n_streams, "p_chosen": ps, "tol": a.tol,
+                       "n_streams": ab.batch.n_streams, "queued_m2l": bool(ab.batch.queued),
+                       "autotune_ms": getattr(ab, "tune_ms", None), "p_chosen": ps, "tol": a.tol,
                        "parallelism": f"replicas x{world}",
                        "l2": "inputs larger than L2 (64 problems' expansions and workspaces)"},
             "certification": {"certified": int(sum(r["certified"] for r in rep)),

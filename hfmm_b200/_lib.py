@@ -81,6 +81,9 @@ SIGNATURES = [
     ("hfmm_plan_set_m2l_compressed", _c_i32, [_c_vp, _c_i32, _c_i32, _c_i32, _c_vp, _c_vp]),
     ("hfmm_batch_create", _c_i32, [ctypes.POINTER(_c_vp), _c_i32, _c_i32, ctypes.POINTER(_c_vp)]),
     ("hfmm_batch_stream_of", _c_i32, [_c_vp, _c_i32]),
+    ("hfmm_batch_set_queue", _c_i32, [_c_vp, _c_i32]),
+    ("hfmm_batch_queued", _c_i32, [_c_vp]),
+    ("hfmm_batch_queue_note", ctypes.c_char_p, [_c_vp]),
     ("hfmm_batch_set_problem", _c_i32, [_c_vp, _c_i32, _c_vp, _c_vp, _c_vp, _c_vp, _c_i32]),
     ("hfmm_batch_set_check", _c_i32, [_c_vp, _c_i32, _c_vp, _c_vp, _c_i32, _c_vp]),
     ("hfmm_batch_capture", _c_i32, [_c_vp]),

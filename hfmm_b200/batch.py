@@ -30,7 +30,9 @@ from ._lib import check as _check
 class Batch:
     """Finalized plans evaluated together; ``bind`` sets the inputs and captures."""
 
-    def __init__(self, states, n_streams=4):
+    def __init__(self, states, n_streams=4, queue=True):
+        """``queue``: run the problems' low-rank mixed M2L as one persistent kernel
+        over a queue of all their work (hfmm_batch_set_queue) when they allow it."""
         if not states:
             raise ValueError("a batch needs at least one plan")
         self.states = list(states)
@@ -41,6 +43,7 @@ class Batch:
             _check(_lib.lib.hfmm_batch_create(arr, len(states), self.n_streams,
                                               _lib.ctypes.byref(h)))
         self._h = h.value
+        _check(_lib.lib.hfmm_batch_set_queue(self._h, int(bool(queue))))
         self.outputs = None
 
     def stream_of(self, i):
@@ -91,6 +94,8 @@ class Batch:
             before = _lib.launch_count()
             _check(_lib.lib.hfmm_batch_capture(self._h))
             self.kernels_per_launch = _lib.launch_count() - before   # kernels in the graph
+        self.queued = bool(_lib.lib.hfmm_batch_queued(self._h))
+        self.queue_note = _lib.lib.hfmm_batch_queue_note(self._h).decode(errors="replace")
         return self.outputs
 
     def launch(self, stream=None):
@@ -141,38 +146,46 @@ def signature(states):
 
 
 def autotune(states, charges, candidates=(1, 2, 4, 8), wisdom=None, reps=3, field=True,
-             precision=None, checks=None):
-    """Pick the stream count with the lowest graph time; returns (Batch, timings).
+             precision=None, checks=None, queue_modes=(True, False)):
+    """Pick the launch configuration with the lowest graph time: the stream count and
+    whether the M2L runs as one queued persistent kernel or per plan on the streams.
+    Returns (Batch, timings keyed "S,queue"). (The plans' leaf sizes are the learned
+    order's choice, made per problem before this.)
 
     With ``wisdom`` (a JSON path) a previous result for the same signature is
-    reused without measuring, and new measurements are stored there."""
+    reused without measuring, and new measurements are stored there (the precedent is
+    jaxfmm/tune.py:123-172's wisdom store)."""
     key = signature(states)
     store = {}
     if wisdom and os.path.exists(wisdom):
         with open(wisdom) as f:
             store = json.load(f)
-    if key in store:
-        b = Batch(states, store[key]["n_streams"])
+    if key in store and "queue" in store[key]:
+        b = Batch(states, store[key]["n_streams"], store[key]["queue"])
         b.bind(charges, field, precision, checks)
         return b, store[key]["ms"]
     times = {}
     for S in candidates:                 # a plan belongs to one batch at a time
         if S > len(states) and S != candidates[0]:
             continue
-        b = Batch(states, S)
-        b.bind(charges, field, precision, checks)
-        times[S] = b.time_ms(reps)
-        b.close()
+        for qm in queue_modes:
+            b = Batch(states, S, qm)
+            b.bind(charges, field, precision, checks)
+            k = (S, bool(b.queued))      # the queue may not apply: then both modes are one
+            if k not in times:
+                times[k] = b.time_ms(reps)
+            b.close()
     best = min(times, key=times.get)
     if wisdom:
-        store[key] = {"n_streams": best, "ms": {str(k): v for k, v in times.items()}}
+        store[key] = {"n_streams": best[0], "queue": best[1],
+                      "ms": {f"{k[0]},{int(k[1])}": v for k, v in times.items()}}
         tmp = wisdom + ".tmp"
         with open(tmp, "w") as f:
             json.dump(store, f, indent=1, sort_keys=True)
         os.replace(tmp, wisdom)
-    b = Batch(states, best)
+    b = Batch(states, best[0], best[1])
     b.bind(charges, field, precision, checks)
-    return b, times
+    return b, {f"{k[0]},{int(k[1])}": v for k, v in times.items()}
 
 
 class AutoBatch:

@@ -269,14 +269,52 @@ void stream_maps(hfmm_plan* P) {
         }
 }
 
+// The low-rank mixed M2L of one level and family (R charge columns): the call of
+// m2l_tf32x3 / one entry of the batch's M2L queue.
+MixedCall cx_call(hfmm_plan* P, int l, int f, int R) {
+    LevelTables& T = P->tables[f][l];
+    auto lb = [&](auto* buf, int cld) { return buf - (int64_t)P->level_lo[l] * R * cld; };
+    MixedCall mc{};
+    mc.tile_tgt = P->mx_tiles[l][R - 1].tgt.p;
+    mc.ntiles = P->mx_tiles[l][R - 1].ntiles;
+    mc.src_tab = P->m2l_src.p;
+    mc.disp_compact = P->disp_compact.p;
+    mc.Bhi = lb(T.xc_hi.p, T.ckld);
+    mc.Blo = lb(T.xc_lo.p, T.ckld);
+    mc.Lhi = nullptr;
+    mc.Llo = nullptr;
+    mc.out = lb(T.yc.p, T.cmld);
+    mc.src_lo = P->level_lo[l];   // the level's buffers hold its own boxes only
+    mc.src_hi = P->level_hi[l];
+    mc.R = R;
+    mc.ld = T.cmld;
+    mc.ldk = T.ckld;
+    mc.ldm = T.cmld;
+    mc.m_valid = T.cr;   // rows r..cmld of the C_d tables are zero
+    mc.n_fam = 1;
+    mc.has_l2l = 0;
+    mc.fam_stride = 0;
+    mc.out_fam_stride = 0;
+    mc.nb = P->nb;
+    mc.err = P->d_err.p;
+    if (R == 2 && T.grid && g_m2l_grid) {   // sources from the dense grid by TMA
+        mc.grid = 1;
+        mc.tile_tgt = P->gx_tiles[l].tgt.p;
+        mc.ntiles = P->gx_tiles[l].ntiles;
+        mc.tile_org = P->gx_org[l].p;
+    }
+    return mc;
+}
+
 void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double* phi, double* E,
-                   cudaStream_t s, bool mixed) {
+                   cudaStream_t s, bool mixed, int phase) {
+    const bool up = phase & EVAL_UP, down = phase & EVAL_DOWN;
     const int R = q_im ? 2 : 1;
     const int NF = P->n_fam;
     const bool field = E != nullptr;
     PlanExtra* X = extra(P, false);
     const int64_t fs = P->nb * (int64_t)R * P->ld;   // family stride of expansion arrays
-    {
+    if (up) {
         PhaseTimer pt(X, s, 0);
         gather_charges(P->n, P->sort_idx.p, q_re, q_im, P->q_s.p, s);
     }
@@ -302,19 +340,21 @@ void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double*
     // The near field needs only the gathered charges: it runs on the plan's side
     // stream beside the whole far field and joins before L2P, which adds into the
     // potentials and fields P2P stores.
-    HFMM_CUDA(cudaEventRecord(P->nf_fork, s));
-    HFMM_CUDA(cudaStreamWaitEvent(P->nf_side, P->nf_fork, 0));
-    {
+    if (up) {
+        HFMM_CUDA(cudaEventRecord(P->nf_fork, s));
+        HFMM_CUDA(cudaStreamWaitEvent(P->nf_side, P->nf_fork, 0));
         ParticlePass p = base;
         p.op = ParticleOp::P2P;
         p.rows = P->leaves.p;
         p.nrows = P->n_leaves;
         p.off = P->near_off.p;
         p.srcs = P->near_src.p;
-        PhaseTimer pt(X, P->nf_side, 7);
-        particles(p, P->nf_side);
+        {
+            PhaseTimer pt(X, P->nf_side, 7);
+            particles(p, P->nf_side);
+        }
+        HFMM_CUDA(cudaEventRecord(P->nf_join, P->nf_side));
     }
-    HFMM_CUDA(cudaEventRecord(P->nf_join, P->nf_side));
 
     // scale_up / scale_dn: multiply row m of family f's result by the level's decode
     // scale d (the folded low-rank plan's GEMMs end in scaled SVD coordinates)
@@ -389,7 +429,9 @@ void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double*
     };
 
     // ---- upward pass
-    {
+    const bool use_mx = mixed && P->mixed_ready;
+    const bool use_cx = use_mx && P->compressed;
+    if (up) {
         ParticlePass p = base;
         p.op = ParticleOp::P2M;
         p.rows = P->leaves.p;
@@ -399,9 +441,8 @@ void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double*
         PhaseTimer pt(X, s, 1);
         particles(p, s);
     }
-    const bool use_mx = mixed && P->mixed_ready;
-    const bool use_cx = use_mx && P->compressed;
-    if (use_cx) {
+    if (!up) {
+    } else if (use_cx) {
         // folded tables (compress.cu): P->equiv holds y = d .* (U^T x) per box, from the
         // leaf check potentials (U, leaves) or the children's y (folded M2M, the rest)
         for (int l = P->md; l >= 2; --l) {
@@ -450,7 +491,7 @@ void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double*
         c.nb = P->nb;
         gemm_f64(c, P->d_err.p, st);
     };
-    if (use_cx) {   // compress every level's densities (x' = y Vt_up U_c), then split them
+    if (up && use_cx) {   // compress every level's densities (x' = y Vt_up U_c), then split them
         PhaseTimer pt(X, s, 14);
         for (int l = 2; l <= P->md; ++l)
             for (int f = 0; f < NF; ++f) {
@@ -464,12 +505,24 @@ void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double*
                 else
                     split_tf32(T.xc.p, T.xc_hi.p, T.xc_lo.p, nbl * R * T.ckld, s);
             }
-    } else if (use_mx) {   // TF32 hi/lo halves of every equivalent density (B operand of the M2L)
+    } else if (up && use_mx) {   // TF32 hi/lo halves of every equivalent density (B operand)
         PhaseTimer pt(X, s, 11);
         split_tf32(P->equiv.p, P->e_hi.p, P->e_lo.p, (int64_t)NF * fs, s);
     }
+    // split evaluate (a batch's queued M2L): the upward half ends here; the downward half
+    // starts with every level's expansion of the queue's check potentials
+    if (!down) return;
+    if (!up && use_cx) {
+        for (int l = 2; l <= P->md; ++l)
+            for (int f = 0; f < NF; ++f) {
+                LevelTables& T = P->tables[f][l];
+                PhaseTimer pt(X, s, 14);
+                gemm_1(K_EXP, l, f, level_base(T.yc.p, l, T.cmld), T.cmld, P->loc.p + f * fs, P->ld,
+                       s, T.dn_d.p);
+            }
+    }
     std::unique_ptr<PhaseTimer> m2l_timer;
-    if (use_cx) {
+    if (up && use_cx) {
         // A level's M2L reads only the compressed densities of the upward pass, so the
         // M2Ls of every level and family run at once on the plan's side streams (the
         // coarse levels have a handful of tiles each and would otherwise run alone on
@@ -483,35 +536,7 @@ void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double*
             HFMM_CUDA(cudaStreamWaitEvent(P->cx_side[k], P->cx_fork, 0));
         auto launch = [&](int l, int f, cudaStream_t ss) {
             LevelTables& T = P->tables[f][l];
-            MixedCall mc{};
-            mc.tile_tgt = P->mx_tiles[l][R - 1].tgt.p;
-            mc.ntiles = P->mx_tiles[l][R - 1].ntiles;
-            mc.src_tab = P->m2l_src.p;
-            mc.disp_compact = P->disp_compact.p;
-            mc.Bhi = level_base(T.xc_hi.p, l, T.ckld);
-            mc.Blo = level_base(T.xc_lo.p, l, T.ckld);
-            mc.Lhi = nullptr;
-            mc.Llo = nullptr;
-            mc.out = level_base(T.yc.p, l, T.cmld);
-            mc.src_lo = P->level_lo[l];   // the level's buffers hold its own boxes only
-            mc.src_hi = P->level_hi[l];
-            mc.R = R;
-            mc.ld = T.cmld;
-            mc.ldk = T.ckld;
-            mc.ldm = T.cmld;
-            mc.m_valid = T.cr;   // rows r..cmld of the C_d tables are zero
-            mc.n_fam = 1;
-            mc.has_l2l = 0;
-            mc.fam_stride = 0;
-            mc.out_fam_stride = 0;
-            mc.nb = P->nb;
-            mc.err = P->d_err.p;
-            if (R == 2 && T.grid && g_m2l_grid) {   // sources from the dense grid by TMA
-                mc.grid = 1;
-                mc.tile_tgt = P->gx_tiles[l].tgt.p;
-                mc.ntiles = P->gx_tiles[l].ntiles;
-                mc.tile_org = P->gx_org[l].p;
-            }
+            MixedCall mc = cx_call(P, l, f, R);
             m2l_tf32x3(static_cast<MixedMaps*>(P->cx_maps)[f * MAX_LEVELS + l], mc, ss);
             // expand into the level's downward coordinates: y_dn = d_dn .* (y' U_c^T U_dn)
             // (overwrites; the L2L and X list add to it on the main stream)
@@ -531,9 +556,10 @@ void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double*
             PhaseTimer pt(X, s, 12);
             generate_m2l_stream(P, l, use_mx, P->ws, s);
         }
-        if (use_cx) {   // this level's M2L ran above, on a side stream
-            for (int f = 0; f < NF; ++f) HFMM_CUDA(cudaStreamWaitEvent(s, P->cx_level[l][f], 0));
-            if (l == P->md) {
+        if (use_cx) {   // this level's M2L ran above, on a side stream (or in the batch queue)
+            if (up)
+                for (int f = 0; f < NF; ++f) HFMM_CUDA(cudaStreamWaitEvent(s, P->cx_level[l][f], 0));
+            if (up && l == P->md) {
                 for (int k = 0; k < hfmm_plan::CX_STREAMS; ++k)
                     HFMM_CUDA(cudaStreamWaitEvent(s, P->cx_join[k], 0));
                 m2l_timer.reset();

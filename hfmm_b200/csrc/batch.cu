@@ -10,7 +10,13 @@
 // workspaces. The whole batch -- fork, every evaluate, join -- is captured once
 // into a graph; a launch replays it with the charge and output pointers given
 // before capture.
+// Queued M2L: when every problem runs the low-rank mixed evaluate with the same
+// number of charge columns, the graph runs every plan's upward half, then one
+// persistent M2L kernel (m2l_queue.cu) over a device queue of every plan's M2L work
+// (tile x row block of each level and family), largest first, then every plan's
+// downward half: the small problems' few tiles no longer run as separate launches.
 #include "hfmm_internal.cuh"
+#include "mixed.cuh"
 
 #include <algorithm>
 #include <memory>
@@ -40,6 +46,15 @@ struct hfmm_batch {
     std::vector<cudaStream_t> streams;
     std::vector<cudaEvent_t> events;            // [0] fork, [1 + s] join of stream s
     std::vector<hfmm::DevBuf<double>> ws;       // per stream (streamed plans only)
+    // queued M2L (see above): calls, tensor maps and items in device memory
+    bool queue_on = true;                       // use the queue when the problems allow it
+    bool queued = false;                        // the captured graph uses it
+    std::string queue_note;                     // why the last capture did not use it
+    int queue_R = 0, n_items = 0;
+    hfmm::DevBuf<hfmm::MixedCall> q_calls;
+    hfmm::DevBuf<hfmm::MixedMaps> q_maps;
+    hfmm::DevBuf<hfmm::M2LItem> q_items;
+    hfmm::DevBuf<int> q_next;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     void drop_graph() {
@@ -111,6 +126,79 @@ __global__ void __launch_bounds__(256) k_check_sums(const double* __restrict__ p
 
 // Work estimate of one evaluate (complex charges): far field M2L+L2L FLOPs and
 // near-field pairs weighted by ~40 flops each; only the relative size matters.
+// The queued M2L's work list (before capture): every plan's low-rank M2L calls and
+// their tensor maps, one item per tile and 128-row block, largest first (an item's
+// cost is its k-chunks per entry; blocks of at most 64 live rows run at half cost).
+// Off when a problem is not a low-rank mixed evaluate or the column counts differ.
+void build_queue(hfmm_batch* B) {
+    B->queued = false;
+    B->queue_note.clear();
+    if (!B->queue_on) {
+        B->queue_note = "the queue is switched off";
+        return;
+    }
+    int R = 0;
+    for (size_t i = 0; i < B->plans.size(); ++i) {
+        hfmm_plan* P = B->plans[i];
+        const auto& io = B->io((int)i);
+        const int r = io.q_im ? 2 : 1;
+        // (a plan streaming its dense M2L tables is fine: only its FP64 evaluate reads them)
+        const std::string who = "problem " + std::to_string(i);
+        if (io.precision != HFMM_PREC_MIXED) B->queue_note = who + " runs the FP64 evaluate";
+        else if (!P->compressed) B->queue_note = who + " has no low-rank M2L tables";
+        else if (!P->mixed_ready) B->queue_note = who + " has no mixed-precision buffers";
+        else if (R && r != R) B->queue_note = who + " has other charge columns than problem 0";
+        if (!B->queue_note.empty()) return;
+        R = r;
+    }
+    std::vector<MixedCall> calls;
+    std::vector<MixedMaps> maps;
+    struct Keyed {
+        double cost;
+        M2LItem it;
+    };
+    std::vector<Keyed> list;
+    for (auto* P : B->plans)
+        for (int l = 2; l <= P->md; ++l)
+            for (int f = 0; f < P->n_fam; ++f) {
+                MixedCall c = cx_call(P, l, f, R);
+                if (c.ntiles == 0) continue;
+                c.wait_ns = 0;
+                c.starve = g_m2l_starve;
+                if ((int64_t)c.nb * R * c.ldk >= ((int64_t)1 << 31)) {
+                    B->queue_note = "a level's densities exceed 32-bit gather offsets";
+                    return;
+                }
+                const int id = (int)calls.size();
+                calls.push_back(c);
+                maps.push_back(static_cast<MixedMaps*>(P->cx_maps)[f * MAX_LEVELS + l]);
+                const int blocks = (c.ldm + 127) / 128;
+                const int valid = c.m_valid > 0 ? c.m_valid : c.ldm;
+                for (int t = 0; t < c.ntiles; ++t)
+                    for (int b = 0; b < blocks; ++b) {
+                        const double cost = (double)(c.ldk / 32) * (valid - 128 * b <= 64 ? 0.6 : 1.0);
+                        list.push_back({cost, M2LItem{id, t, b}});
+                    }
+            }
+    if (list.empty()) {
+        B->queue_note = "no M2L work";
+        return;
+    }
+    std::stable_sort(list.begin(), list.end(), [](const Keyed& a, const Keyed& b) { return a.cost > b.cost; });
+    std::vector<M2LItem> items;
+    for (auto& k : list) items.push_back(k.it);
+    B->q_calls.alloc(calls.size());
+    B->q_maps.alloc(maps.size());
+    B->q_items.alloc(items.size());
+    B->q_next.alloc(1);
+    HFMM_CUDA(cudaMemcpy(B->q_calls.p, calls.data(), calls.size() * sizeof(MixedCall), cudaMemcpyHostToDevice));
+    HFMM_CUDA(cudaMemcpy(B->q_maps.p, maps.data(), maps.size() * sizeof(MixedMaps), cudaMemcpyHostToDevice));
+    HFMM_CUDA(cudaMemcpy(B->q_items.p, items.data(), items.size() * sizeof(M2LItem), cudaMemcpyHostToDevice));
+    B->n_items = (int)items.size();
+    B->queue_R = R;
+    B->queued = true;
+}
+
 double plan_cost(const hfmm_plan* P) {
     const double ns = P->n_s;
     const double far = 2.0 * ns * ns * 2.0 * P->n_fam * ((double)P->nV + 8.0 * P->nb);
@@ -264,16 +352,35 @@ int hfmm_batch_capture(hfmm_batch* B) {
         B->drop_graph();
         const int S = (int)B->streams.size();
         cudaStream_t s0 = B->streams[0];
+        build_queue(B);
         HFMM_CUDA(cudaStreamBeginCapture(s0, cudaStreamCaptureModeRelaxed));
         try {
             HFMM_CUDA(cudaEventRecord(B->events[0], s0));
             for (int s = 1; s < S; ++s) HFMM_CUDA(cudaStreamWaitEvent(B->streams[s], B->events[0], 0));
+            if (B->queued) {   // every plan's upward half, then the queued M2L of all of them
+                for (int s = 0; s < S; ++s)
+                    for (int i : B->order[s]) {
+                        auto& io = B->io(i);
+                        evaluate_fp64(B->plans[i], io.q_re, io.q_im, io.phi, io.E, B->streams[s], true,
+                                      EVAL_UP);
+                    }
+                for (int s = 1; s < S; ++s) {
+                    HFMM_CUDA(cudaEventRecord(B->events[1 + s], B->streams[s]));
+                    HFMM_CUDA(cudaStreamWaitEvent(s0, B->events[1 + s], 0));
+                }
+                int sms = 148;
+                HFMM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, B->device));
+                m2l_queue(B->q_calls.p, B->q_maps.p, B->q_items.p, B->n_items, B->q_next.p, B->queue_R,
+                          sms, s0);
+                HFMM_CUDA(cudaEventRecord(B->events[0], s0));
+                for (int s = 1; s < S; ++s) HFMM_CUDA(cudaStreamWaitEvent(B->streams[s], B->events[0], 0));
+            }
             for (int s = 0; s < S; ++s)
                 for (int i : B->order[s]) {
                     auto& io = B->io(i);
                     hfmm_plan* P = B->plans[i];
                     evaluate_fp64(P, io.q_re, io.q_im, io.phi, io.E, B->streams[s],
-                                  io.precision == HFMM_PREC_MIXED);
+                                  io.precision == HFMM_PREC_MIXED, B->queued ? EVAL_DOWN : EVAL_ALL);
                     if (io.sums) {   // check the result against the direct sum, in the graph
                         double* rphi = io.ref.p;
                         double* rE = io.ref.p + 2 * io.n_t;
@@ -316,6 +423,22 @@ int hfmm_batch_launch(hfmm_batch* B, void* stream) {
 }
 
 void hfmm_batch_destroy(hfmm_batch* B) { delete B; }
+
+int hfmm_batch_set_queue(hfmm_batch* B, int32_t on) {
+    if (!B) return fail(HFMM_ERR_ARG, "batch is NULL");
+    B->queue_on = on != 0;
+    B->drop_graph();
+    return HFMM_OK;
+}
+
+int hfmm_batch_queued(const hfmm_batch* B) {
+    if (!B) return fail(HFMM_ERR_ARG, "batch is NULL");
+    return B->queued ? 1 : 0;
+}
+
+const char* hfmm_batch_queue_note(const hfmm_batch* B) {
+    return B ? B->queue_note.c_str() : "batch is NULL";
+}
 
 }  // extern "C"
 

@@ -238,8 +238,12 @@ void batch_forget_plan(struct hfmm_batch* B, hfmm_plan* P);
 void generate_m2l_stream(hfmm_plan* P, int level, bool mixed, void* ws, cudaStream_t s);
 void compressed_prepare(hfmm_plan* P);   // finalize: buffers, tensor maps, side streams
 void compressed_release(hfmm_plan* P);   // plan destroy: side streams and events
+// phase: EVAL_ALL; or the two halves of a batch whose low-rank M2L runs from one queue
+// (m2l_queue): EVAL_UP ends after the levels' compressed densities, EVAL_DOWN starts
+// with the expansions of the queue's check potentials
+enum { EVAL_UP = 1, EVAL_DOWN = 2, EVAL_ALL = 3 };
 void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double* phi,
-                   double* fld, cudaStream_t s, bool mixed = false);
+                   double* fld, cudaStream_t s, bool mixed = false, int phase = EVAL_ALL);
 void direct_sum(const double* pos, const double* q_re, const double* q_im, int64_t n,
                 const int32_t* targets, int64_t n_t, double k, double* phi, double* fld,
                 double* scratch, int n_split, cudaStream_t s, int* err, int yukawa = 0);

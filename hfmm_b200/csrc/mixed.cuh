@@ -56,6 +56,19 @@ void make_grid_map(CUtensorMap* map, const float* base, int ckld, int G);
 extern int g_m2l_grid;
 void split_transpose_tables(const double* at, float* hi, float* lo, int ld, int count);
 void m2l_tf32x3(const MixedMaps& maps, const MixedCall& c, cudaStream_t s);
+
+// the low-rank mixed M2L call of one plan, level and family for R charge columns
+MixedCall cx_call(hfmm_plan* P, int l, int f, int R);
+
+// One work item of the queued M2L: a tile x one 128-row block of calls[call].
+struct M2LItem {
+    int call, tile, mblock;
+};
+// Persistent M2L over items (sorted by the caller), n_ctas resident CTAs; `next` is a
+// device int the launch resets. calls, maps and items live in device memory.
+void m2l_queue(const MixedCall* calls, const MixedMaps* maps, const M2LItem* items, int n_items,
+               int* next, int R, int n_ctas, cudaStream_t s);
+size_t m2l_queue_smem();
 size_t m2l_tf32x3_smem();
 
 }  // namespace hfmm

@@ -299,6 +299,20 @@ int hfmm_batch_capture(hfmm_batch* batch);
 int hfmm_batch_launch(hfmm_batch* batch, void* stream);
 void hfmm_batch_destroy(hfmm_batch* batch);
 
+/* Queued M2L of a batch (no counterpart in the reference): with on != 0 (the
+ * default), a batch whose problems all run the low-rank mixed evaluate with the same
+ * charge columns is captured as every plan's upward half, ONE persistent M2L kernel
+ * draining a device queue of every plan's M2L work items (tile x row block of each
+ * level and family, largest first; the CTAs take items with an atomic counter), and
+ * every plan's downward half. on == 0 captures each plan's evaluate whole, on
+ * streams. Takes effect at the next hfmm_batch_capture; hfmm_batch_queued reports
+ * whether the captured graph uses the queue (1) or not (0), and
+ * hfmm_batch_queue_note why not (an empty string when it does; valid until the
+ * next capture or the batch's destruction). */
+int hfmm_batch_set_queue(hfmm_batch* batch, int32_t on);
+int hfmm_batch_queued(const hfmm_batch* batch);
+const char* hfmm_batch_queue_note(const hfmm_batch* batch);
+
 /* ---- expansion-order network (no counterpart in the reference) ---- */
 /* A 3 x 64 FP32 MLP (tanh hidden layers, linear output) over in_dim features
  * with out_dim outputs. Parameters are one flat device FP32 array of

@@ -142,8 +142,9 @@ def test_autotune_writes_and_reuses_wisdom(tmp_path):
     store = json.loads(w.read_text())
     assert len(store) == 1
     entry = next(iter(store.values()))
-    assert entry["n_streams"] == b.n_streams and set(entry["ms"]) == {"1", "2", "4"}
-    assert b.n_streams == min(times, key=times.get)
+    # the plans have no low-rank M2L, so the queue does not apply: "S,0" keys only
+    assert entry["n_streams"] == b.n_streams and set(entry["ms"]) == {"1,0", "2,0", "4,0"}
+    assert f"{b.n_streams},0" == min(times, key=times.get)
     b.close()
     b2, t2 = autotune(states, qs, candidates=(1, 2, 4), wisdom=str(w))
     assert b2.n_streams == entry["n_streams"] and t2 == entry["ms"]
@@ -187,6 +188,94 @@ def test_in_graph_check_matches_host_referee():
         want_E = float(torch.linalg.norm(E[tg.long()] - r_E) / torch.linalg.norm(r_E))
         assert e_phi == pytest.approx(want_phi, rel=1e-9) and e_E == pytest.approx(want_E, rel=1e-9)
         assert 0 < e_phi < 1e-3
+    b.close()
+    for st in states:
+        st.close()
+
+
+def _compressed_problems(n_probs=6):
+    rng = np.random.default_rng(21)
+    out = []
+    for i in range(n_probs):
+        n = int(np.exp(rng.uniform(np.log(4000), np.log(40000))))
+        x, k, q = _problem(n, float(rng.uniform(1.0, 12.0)), 30 + i, bool(i % 2))
+        out.append((x, k, q))
+    return out
+
+
+@pytest.mark.parametrize("n_streams", [1, 4])
+def test_queued_m2l_matches_individual_evaluates(n_streams):
+    """The batch's queued M2L (one persistent kernel over every problem's M2L tiles,
+    hfmm_batch_set_queue) computes each tile as the per-level kernel does, so the
+    batch's results equal each plan's own evaluate bit for bit, launch after launch."""
+    import hfmm_b200 as hf
+    from hfmm_b200.batch import Batch
+    probs = _compressed_problems()
+    states = [hf.setup(x, k, p=6, N_max=32, stream_tables=True, m2l_compress=1e-7)
+              for x, k, _ in probs]
+    qs = [torch.as_tensor(q).cuda() for _, _, q in probs]
+    b = Batch(states, n_streams, queue=True)
+    outs = b.bind(qs, field=True, precision=hf.PREC_MIXED)
+    assert b.queued, b.queue_note
+    refs = [hf.evaluate_field(st, q, hf.PREC_MIXED) for st, q in zip(states, qs)]
+    for _ in range(2):
+        b.launch()
+        torch.cuda.synchronize()
+        b.check_errors()
+        for (phi, E), (rp, re) in zip(outs, refs):
+            assert torch.equal(phi, rp) and torch.equal(E, re)
+    b.close()
+    # a problem with real charges: the column counts differ, the queue does not apply
+    qs[0] = qs[0].real.contiguous()
+    b = Batch(states, 2, queue=True)
+    outs = b.bind(qs, field=True, precision=hf.PREC_MIXED)
+    assert not b.queued
+    b.launch()
+    torch.cuda.synchronize()
+    for st, q, (phi, E) in zip(states, qs, outs):
+        rp, re = hf.evaluate_field(st, q, hf.PREC_MIXED)
+        assert torch.equal(phi, rp) and torch.equal(E, re)
+    b.close()
+    for st in states:
+        st.close()
+
+
+def test_queued_m2l_wait_runs_out_and_reports():
+    """The persistent queue kernel's bounded waits: a test switch starves every CTA's
+    first stage (20 ms limit); the launch ends with the timeout flag (4) on the plans,
+    and a graph captured again without the switch gives the plans' own results."""
+    import hfmm_b200 as hf
+    from hfmm_b200 import _lib
+    from hfmm_b200.batch import Batch
+    lib = _lib.load()
+    probs = _compressed_problems(4)
+    states = [hf.setup(x, k, p=6, N_max=32, stream_tables=True, m2l_compress=1e-7)
+              for x, k, _ in probs]
+    qs = [torch.as_tensor(q).cuda() for _, _, q in probs]
+    b = Batch(states, 2, queue=True)
+    try:
+        lib.hfmm_debug_m2l_wait(20_000_000, 1)
+        outs = b.bind(qs, field=True, precision=hf.PREC_MIXED)
+        assert b.queued, b.queue_note
+        b.launch()
+        torch.cuda.synchronize()
+    finally:
+        lib.hfmm_debug_m2l_wait(0, 0)
+    flagged = 0
+    for st in states:
+        try:
+            hf.check_errors(st)
+        except hf.HFMMError as e:
+            assert e.code == -5 and "device error flag 4" in str(e)
+            flagged += 1
+    assert flagged >= 1
+    outs = b.bind(qs, field=True, precision=hf.PREC_MIXED)
+    b.launch()
+    torch.cuda.synchronize()
+    b.check_errors()
+    for st, q, (phi, E) in zip(states, qs, outs):
+        rp, re = hf.evaluate_field(st, q, hf.PREC_MIXED)
+        assert torch.equal(phi, rp) and torch.equal(E, re)
     b.close()
     for st in states:
         st.close()
