@@ -54,3 +54,40 @@ def test_torch_in_torch_out_and_repeatability():
     b, Eb = hfmm_b200.evaluate_field(st, qt)
     assert isinstance(a, torch.Tensor) and a.is_cuda and a.dtype == torch.complex128
     assert torch.equal(a, b) and torch.equal(Ea, Eb)       # deterministic: no atomics
+
+
+@pytest.mark.parametrize("k", [50.0, 3000.0, 4.0e4, 2.0e5])
+def test_referee_phase_range(k):
+    """The referee's sin/cos: Cody-Waite reduction against pi/2 and the Taylor series
+    up to |k r| = 1e5, sincos beyond (direct.cu). Against NumPy's sin/cos of the same
+    FP64 phase, through the C ABI (hfmm_direct). Both sides round k r to FP64 the
+    same way up to an ulp of the phase, so the bar grows with the largest phase:
+    2e-15 relative x max(k r), plus 1e-13. k = 2e5 reaches k r = 3.4e5."""
+    import torch
+    from hfmm_b200 import _lib
+    lib = _lib.load()
+    n, m = 1500, 120
+    rng = np.random.default_rng(11)
+    pos = rng.random((n, 3))
+    q = rng.standard_normal(n) + 1j * rng.standard_normal(n)
+    tg = np.sort(rng.choice(n, m, replace=False)).astype(np.int32)
+    dev = "cuda"
+    p_d = torch.as_tensor(pos.reshape(-1), device=dev)
+    qr = torch.as_tensor(q.real.copy(), device=dev)
+    qi = torch.as_tensor(q.imag.copy(), device=dev)
+    t_d = torch.as_tensor(tg, device=dev)
+    phi = torch.empty(m, dtype=torch.complex128, device=dev)
+    E = torch.empty((m, 3), dtype=torch.complex128, device=dev)
+    _lib.check(lib.hfmm_direct(p_d.data_ptr(), qr.data_ptr(), qi.data_ptr(), n, t_d.data_ptr(), m,
+                               k, phi.data_ptr(), E.data_ptr(), None))
+    torch.cuda.synchronize()
+    d = pos[tg][:, None, :] - pos[None, :, :]
+    r = np.sqrt((d ** 2).sum(-1))
+    ok = r > 0
+    rs = np.where(ok, r, 1.0)
+    kr = k * rs
+    G = np.where(ok, (np.cos(kr) + 1j * np.sin(kr)) / rs, 0.0)
+    W = np.where(ok, (np.cos(kr) + 1j * np.sin(kr)) * (1 - 1j * kr) / rs ** 3, 0.0)
+    bar = 2e-15 * k * np.sqrt(3.0) + 1e-13
+    assert O.relative_error(phi.cpu().numpy(), G @ q) < bar
+    assert O.relative_error(E.cpu().numpy(), np.einsum("ts,tsc,s->tc", W, d, q)) < bar
