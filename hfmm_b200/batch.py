@@ -62,7 +62,7 @@ class Batch:
             raise ValueError("one charge vector per plan")
         precs = precision if isinstance(precision, (list, tuple)) else \
             [PREC_MIXED if precision is None else precision] * len(self.states)
-        self._keep, self.outputs = [], []
+        self._keep, self.outputs, self._q_dev, self._stage = [], [], [], None
         for i, (st, q) in enumerate(zip(self.states, charges)):
             if tuple(q.shape) != (st.n,):
                 raise ValueError(f"charges of problem {i} must have shape ({st.n},)")
@@ -77,6 +77,7 @@ class Batch:
                 self._h, i, q_re.data_ptr(), None if q_im is None else q_im.data_ptr(),
                 phi.data_ptr(), None if E is None else E.data_ptr(), int(precs[i])))
             self._keep.append((q_re, q_im))
+            self._q_dev.append((q_re, q_im))
             self.outputs.append((phi, E))
         self.check_sums = None
         if checks is not None:
@@ -97,6 +98,44 @@ class Batch:
         self.queued = bool(_lib.lib.hfmm_batch_queued(self._h))
         self.queue_note = _lib.lib.hfmm_batch_queue_note(self._h).decode(errors="replace")
         return self.outputs
+
+    def solve(self, charges):
+        """One launch on new charges from the host, without re-capturing: ``charges``
+        are NumPy arrays, one per problem with the bound shape (complex, or real where
+        the problem was bound with real charges). They are copied through page-locked
+        staging buffers (kept by the batch) into the device buffers the graph reads,
+        the graph runs on the current stream, and each output comes back into a fresh
+        page-locked host block. Returns [(phi, E or None), ...] as NumPy arrays."""
+        from . import _to_host
+        if self.outputs is None:
+            raise RuntimeError("bind the batch before solve")
+        if len(charges) != len(self.states):
+            raise ValueError("one charge vector per plan")
+        dev = self.states[0].device
+        with torch.cuda.device(dev):
+            s = torch.cuda.current_stream(dev)
+            if self._stage is None:   # page-locked staging, one complex128 vector a problem
+                self._stage = [(torch.empty(st.n, dtype=torch.complex128, pin_memory=True),
+                                torch.empty(st.n, dtype=torch.complex128, device=dev))
+                               for st in self.states]
+            for i, (q, (q_re, q_im), (h, d)) in enumerate(zip(charges, self._q_dev, self._stage)):
+                q = np.asarray(q)
+                if q.shape != (self.states[i].n,):
+                    raise ValueError(f"charges of problem {i} must have shape ({self.states[i].n},)")
+                if q_im is None and np.iscomplexobj(q):
+                    raise ValueError(f"problem {i} was bound with real charges")
+                if q.dtype == np.complex128 and q.flags.c_contiguous and q.flags.writeable:
+                    h.copy_(torch.from_numpy(q))   # torch's threaded host copy
+                else:
+                    h.numpy()[...] = q
+                d.copy_(h, non_blocking=True)
+                q_re.copy_(d.real)
+                if q_im is not None:
+                    q_im.copy_(d.imag)
+            self.launch(s)
+            out = [(_to_host(phi), None if E is None else _to_host(E)) for phi, E in self.outputs]
+            s.synchronize()
+        return [(a.numpy(), None if b is None else b.numpy()) for a, b in out]
 
     def launch(self, stream=None):
         s = stream if stream is not None else torch.cuda.current_stream(self.states[0].device)
@@ -239,6 +278,14 @@ class AutoBatch:
             self.batch = Batch(self.states, self.n_streams)
             self.batch.bind(qs, field, self.precisions, checks=self.checks)
         return self.batch.outputs
+
+    def solve(self, charges):
+        """The batched evaluate from the host: NumPy charges in (one array per problem),
+        one graph launch, NumPy (phi, E) out, and each problem's checked relative
+        errors (phi, E) from the launch's in-graph direct-sum check. Problems whose
+        error misses the tolerance are not rerun here; ``certify`` does that."""
+        outs = self.batch.solve(charges)
+        return outs, self.batch.check_rel_errors()
 
     def certify(self):
         """Read the in-graph check of the last launch (the direct sum at each problem's

@@ -120,12 +120,16 @@ def features_for(positions, k, tol, device=None):
 def label_p(ps, errs, tol):
     """Smallest (fractional) p from which every swept order meets ``tol``.
 
-    ``errs[i]`` is the error at ``ps[i]`` (ascending). Between the last miss and
-    the first hit the crossing is interpolated linearly in log10(error); when no
-    order meets ``tol`` the label is ``ps[-1] + 1``.
+    ``errs[i]`` is the error at ``ps[i]`` (ascending); NaN marks an order the sweep
+    did not run (merged sweeps cover different orders) and is left out, inf an order
+    that does not apply (the mixed path below p = 5). Between the last miss and the
+    first hit the crossing is interpolated linearly in log10(error); when no order
+    meets ``tol`` the label is one above the largest order run.
     """
     ps = np.asarray(ps, np.float64)
     e = np.asarray(errs, np.float64)
+    run = ~np.isnan(e)
+    ps, e = ps[run], e[run]
     ok = np.isfinite(e) & (e <= tol)
     if not ok[-1]:
         return float(ps[-1] + 1)

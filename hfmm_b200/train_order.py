@@ -10,13 +10,16 @@ leaf size. Labels for any tolerance are then read off the error curves
 (``learned.label_p``), so one sweep yields a sample per tolerance.
 
     python -m hfmm_b200.train_order generate --problems 120 --out sweep.npz
-    python -m hfmm_b200.train_order train --data sweep.npz --out order_net.npz
+    python -m hfmm_b200.train_order generate --high-k --problems 24 --seed 1 --out high.npz
+    python -m hfmm_b200.train_order merge sweep.npz high.npz --out all.npz
+    python -m hfmm_b200.train_order train --data all.npz --out order_net.npz
 
 Problems: N log-uniform in [5e4, 5e5]; uniform in the unit cube or 1-16
 Gaussian clusters with sigma in [0.01, 0.1] (clipped to the cube); the eight
 cube corners are added so that the domain extent is exactly 1 and the decode
 factors repeat across problems of the same k (they are cached);
-k from a grid in [1, 24]; complex N(0, 1) charges.
+k from a grid in [1, 24] (p swept 4..14), or, for the high-frequency sweep, from
+{32, 40, 50} (p swept 6..16); complex N(0, 1) charges.
 """
 import argparse
 import math
@@ -30,6 +33,10 @@ from .learned import N_FEATURES, LEAVES, TOL_MIXED, label_p
 
 K_GRID = (1.0, 1.5, 2.0, 3.0, 4.0, 6.0, 8.0, 12.0, 16.0, 24.0)
 P_SWEEP = tuple(range(4, 15))
+# the high-frequency sweep (k x extent 32..50, the 8M-point clustered workload's 44
+# among them): orders up to the clamp P_MAX = 16, starting at 6
+K_GRID_HIGH = (32.0, 40.0, 50.0)
+P_SWEEP_HIGH = tuple(range(6, 17))
 # tolerances the network is trained for: 1e-3 .. 10^-6.5 in quarter decades. Below
 # about 2e-7 the FP64 method itself stalls (the cos component's eps_rel = 1e-7
 # damping, HFMM.py:75-77), most problems cannot meet the tolerance at any swept p,
@@ -37,7 +44,7 @@ P_SWEEP = tuple(range(4, 15))
 TOLS = tuple(10.0 ** (-e) for e in np.arange(3.0, 6.51, 0.25))
 
 
-def make_problem(rng):
+def make_problem(rng, k_grid=K_GRID):
     n = int(math.exp(rng.uniform(math.log(5e4), math.log(5e5))))
     if rng.random() < 1 / 3:
         kind, x = "uniform", rng.random((n, 3))
@@ -49,7 +56,7 @@ def make_problem(rng):
         x = np.clip(c[rng.integers(0, nc, n)] + sig * rng.standard_normal((n, 3)), 0.0, 1.0)
     corners = np.array([[i & 1, (i >> 1) & 1, (i >> 2) & 1] for i in range(8)], np.float64)
     x = np.vstack([x, corners])
-    k = float(rng.choice(K_GRID))
+    k = float(rng.choice(k_grid))
     q = rng.standard_normal(len(x)) + 1j * rng.standard_normal(len(x))
     return x, k, q, kind
 
@@ -63,13 +70,13 @@ class _DecodeCache:
         self.k = None
         self.memo = {}
 
-    def __call__(self, p, level, extent, k, imaginary, eps_rel):
+    def __call__(self, p, level, extent, k, imaginary, eps_rel, kind="helmholtz"):
         if k != self.k:
             self.memo.clear()
             self.k = k
-        key = (p, level, extent, imaginary, eps_rel)
+        key = (p, level, extent, imaginary, eps_rel, kind)
         if key not in self.memo:
-            self.memo[key] = self.orig(p, level, extent, k, imaginary, eps_rel)
+            self.memo[key] = self.orig(p, level, extent, k, imaginary, eps_rel, kind)
         return self.memo[key]
 
 
@@ -87,10 +94,10 @@ def _time_eval(hf, st, q_re, q_im, phi, E, prec, reps=1, warmup=0):
     return a.elapsed_time(b) / reps
 
 
-def generate(n_problems, seed=0, n_check=256, verbose=True):
+def generate(n_problems, seed=0, n_check=256, verbose=True, k_grid=K_GRID, p_sweep=P_SWEEP):
     import hfmm_b200 as hf
     rng = np.random.default_rng(seed)
-    probs = [make_problem(np.random.default_rng([seed, i])) for i in range(n_problems)]
+    probs = [make_problem(np.random.default_rng([seed, i]), k_grid) for i in range(n_problems)]
     order = sorted(range(n_problems), key=lambda i: probs[i][1])   # group by k for the cache
     cache = _DecodeCache()
     hf.level_decodes = cache      # the name _load_tables calls
@@ -110,7 +117,7 @@ def generate(n_problems, seed=0, n_check=256, verbose=True):
             e64, emx, t64, tmx = [], [], [], []
             ref = None
             cmp = learned.compress_for(1e-6, hf.PREC_MIXED)
-            for p in P_SWEEP:
+            for p in p_sweep:
                 st = hf.setup(x, k, p=p, N_max=learned.FEATURE_LEAF, device=dev,
                               m2l_compress=cmp if p >= 5 else None)
                 if ref is None:
@@ -129,7 +136,7 @@ def generate(n_problems, seed=0, n_check=256, verbose=True):
                 st.close()
                 del phi, E
             # leaf timing at the order the mixed path needs for 1e-6
-            lp = int(min(learned.P_MAX, max(5, math.ceil(label_p(P_SWEEP, emx, TOL_MIXED)))))
+            lp = int(min(learned.P_MAX, max(5, math.ceil(label_p(p_sweep, emx, TOL_MIXED)))))
             lt = []
             for leaf in LEAVES:
                 st = hf.setup(x, k, p=lp, N_max=leaf, device=dev, m2l_compress=cmp)
@@ -150,7 +157,28 @@ def generate(n_problems, seed=0, n_check=256, verbose=True):
     finally:
         hf.level_decodes = cache.orig
     res = {k: np.asarray(v) for k, v in out.items()}
-    res["ps"] = np.asarray(P_SWEEP)
+    res["ps"] = np.asarray(p_sweep)
+    return res
+
+
+def merge(datasets):
+    """One training set from sweeps over different orders: every problem's error and
+    time curves are laid on the union of the swept orders, NaN where its sweep did not
+    run that order (label_p leaves those out)."""
+    ps = np.unique(np.concatenate([d["ps"] for d in datasets]))
+    out = {}
+    for d in datasets:
+        idx = np.searchsorted(ps, d["ps"])
+        for key, v in d.items():
+            if key == "ps":
+                continue
+            if key in ("err64", "errmx", "t64", "tmx"):
+                w = np.full((v.shape[0], len(ps)), np.nan)
+                w[:, idx] = v
+                v = w
+            out.setdefault(key, []).append(v)
+    res = {k: np.concatenate(v) for k, v in out.items()}
+    res["ps"] = ps
     return res
 
 
@@ -235,6 +263,11 @@ def main(argv=None):
     g.add_argument("--problems", type=int, default=120)
     g.add_argument("--seed", type=int, default=0)
     g.add_argument("--out", required=True)
+    g.add_argument("--high-k", action="store_true",
+                   help="the high-frequency sweep: k in K_GRID_HIGH, p in P_SWEEP_HIGH")
+    m = sp.add_parser("merge")
+    m.add_argument("inputs", nargs="+")
+    m.add_argument("--out", required=True)
     t = sp.add_parser("train")
     t.add_argument("--data", required=True)
     t.add_argument("--steps", type=int, default=None, help="default: chosen by cross-validation")
@@ -242,7 +275,11 @@ def main(argv=None):
     t.add_argument("--out", required=True)
     a = ap.parse_args(argv)
     if a.cmd == "generate":
-        res = generate(a.problems, a.seed)
+        kw = dict(k_grid=K_GRID_HIGH, p_sweep=P_SWEEP_HIGH) if a.high_k else {}
+        res = generate(a.problems, a.seed, **kw)
+        np.savez_compressed(a.out, **res)
+    elif a.cmd == "merge":
+        res = merge([dict(np.load(f, allow_pickle=False)) for f in a.inputs])
         np.savez_compressed(a.out, **res)
     else:
         data = dict(np.load(a.data, allow_pickle=False))

@@ -279,3 +279,42 @@ def test_queued_m2l_wait_runs_out_and_reports():
     b.close()
     for st in states:
         st.close()
+
+
+def test_solve_from_host_rescales_exactly():
+    """Batch.solve runs new host charges through the captured graph (no re-capture):
+    charges scaled by 2 give results scaled by 2 bit for bit (every step of the
+    evaluate is linear in the charges and a power of two scales exactly), real
+    charges into a complex-bound problem count as zero imaginary parts, and a wrong
+    shape, count or a complex vector into a real-bound problem is refused."""
+    import hfmm_b200 as hf
+    from hfmm_b200.batch import Batch
+    probs = _batch_problems()[:3]
+    states = [hf.setup(x, k, p=p, N_max=32, stream_tables=True) for x, k, q, p in probs]
+    qs = [torch.as_tensor(q).cuda() for _, _, q, _ in probs]
+    qs[2] = qs[2].real.contiguous()
+    precs = [hf.PREC_MIXED, hf.PREC_FP64, hf.PREC_MIXED]
+    b = Batch(states, 2)
+    outs = b.bind(qs, field=True, precision=precs)
+    b.launch()
+    torch.cuda.synchronize()
+    ref = [(phi.cpu().numpy(), E.cpu().numpy()) for phi, E in outs]
+    host = [2.0 * q for _, _, q, _ in probs]
+    host[2] = host[2].real.copy()
+    for _ in range(2):
+        res = b.solve(host)
+        for (phi, E), (rp, re) in zip(res, ref):
+            assert np.array_equal(phi, 2.0 * rp) and np.array_equal(E, 2.0 * re)
+    res = b.solve([host[0].real.copy(), host[1], host[2]])
+    r0 = hf.evaluate_field(states[0], torch.as_tensor(host[0].real.copy()).cuda(), hf.PREC_MIXED)
+    r0 = r0[0].cpu().numpy()   # the one-column evaluate: same values to the mixed path's rounding
+    assert np.linalg.norm(res[0][0] - r0) < 1e-6 * np.linalg.norm(r0)
+    with pytest.raises(ValueError):
+        b.solve(host[:2])
+    with pytest.raises(ValueError):
+        b.solve([host[0][:-1], host[1], host[2]])
+    with pytest.raises(ValueError):
+        b.solve([host[0], host[1], host[2] + 1j])
+    b.close()
+    for st in states:
+        st.close()

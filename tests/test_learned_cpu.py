@@ -135,3 +135,53 @@ def test_network_is_consulted_only_in_its_range():
     f[1] = 10.0
     assert not network_applies(f, TOL_LEARNED / 2)
 
+
+
+def test_label_p_skips_orders_not_swept():
+    """Merged sweeps: NaN marks an order a problem's sweep did not run; labels come
+    from the orders that ran (inf still marks an order that does not apply)."""
+    from hfmm_b200.learned import label_p
+    ps = [4, 5, 6, 7, 8, 9]
+    errs = [1e-2, 1e-3, 1e-4, 1e-5, np.nan, np.nan]        # swept 4..7 only
+    assert label_p(ps, errs, 1e-4) == pytest.approx(6.0)
+    assert label_p(ps, errs, 1e-6) == 8.0                    # unreachable: last run + 1
+    errs = [np.nan, np.nan, 1e-4, 1e-5, 1e-6, 1e-7]          # swept 6..9 only
+    assert label_p(ps, errs, 1e-3) == 6.0                    # first run order meets it
+    assert label_p(ps, errs, 10 ** -5.5) == pytest.approx(7.5)
+
+
+def test_merge_lays_sweeps_on_the_union_of_orders():
+    from hfmm_b200 import train_order
+    rng = np.random.default_rng(0)
+
+    def sweep(ps, n):
+        m = len(ps)
+        return dict(feats=rng.random((n, 24)), err64=10.0 ** -rng.uniform(2, 8, (n, m)),
+                    errmx=10.0 ** -rng.uniform(2, 8, (n, m)), t64=rng.random((n, m)),
+                    tmx=rng.random((n, m)), leaf_t=rng.random((n, 4)), leaf_p=np.full(n, 8),
+                    n=np.full(n, 1000), k=rng.random(n), kind=np.array(["uniform"] * n),
+                    ps=np.asarray(ps))
+    a, b = sweep(range(4, 15), 3), sweep(range(6, 17), 2)
+    m = train_order.merge([a, b])
+    assert list(m["ps"]) == list(range(4, 17)) and m["err64"].shape == (5, 13)
+    assert np.isnan(m["err64"][:3, 11:]).all() and np.isnan(m["err64"][3:, :2]).all()
+    assert np.array_equal(m["err64"][:3, :11], a["err64"])
+    assert np.array_equal(m["errmx"][3:, 2:], b["errmx"])
+    Xa, Ta = train_order.samples(a)
+    Xm, Tm = train_order.samples(m)
+    assert np.array_equal(Tm[:len(Ta)], Ta)                  # a's labels are unchanged
+
+
+def test_decode_cache_stands_in_for_level_decodes():
+    """The sweep swaps operators.level_decodes for a memoising wrapper: same
+    parameters, same results, one computation per key."""
+    import inspect
+    from hfmm_b200 import operators, train_order
+    cache = train_order._DecodeCache()
+    mine = list(inspect.signature(cache.__call__).parameters.values())
+    theirs = list(inspect.signature(operators.level_decodes).parameters.values())
+    assert len(mine) == len(theirs) and [q.default for q in mine] == [q.default for q in theirs]
+    a = cache(3, 2, 1.0, 2.0, False, 1e-7, "helmholtz")
+    b = operators.level_decodes(3, 2, 1.0, 2.0, False, 1e-7, "helmholtz")
+    assert all(np.array_equal(x, y) for x, y in zip(a, b))
+    assert cache(3, 2, 1.0, 2.0, False, 1e-7, "helmholtz") is a and len(cache.memo) == 1
