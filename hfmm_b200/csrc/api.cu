@@ -395,6 +395,8 @@ void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double*
         c.a_fam_stride = k_entries[kind];
         c.n_fam = NF;
         c.nb = P->nb;
+        c.part = P->gemm_part.p;   // coarse levels' small grids split their entries
+        c.part_cap = P->gemm_part.n;
         gemm_f64(c, P->d_err.p, s);
     };
     // The decode scale vector differs per family: run the first decode step once per family.
@@ -942,6 +944,7 @@ int hfmm_plan_finalize(hfmm_plan* P) {
     }
     const size_t exp = (size_t)P->n_fam * P->nb * 2 * P->ld;
     P->check.alloc(exp);
+    P->gemm_part.alloc(GEMM_PART_CAP);
     P->equiv.alloc(exp);
     P->loc.alloc(exp);
     P->tmp.alloc(exp);

@@ -18,7 +18,14 @@
 // Tensor path: mma.sync.m16n8k4 f64 (DMMA). tcgen05 has no f64 kind, so this
 // is the FP64 tensor path on sm_100a. CTA tile 64 (m) x 64 (n = targets x R),
 // k-chunk 16, 4 warps of 32 x 32, two-stage cp.async pipeline.
+// Small grids (coarse levels: a few dozen output tiles, each walking all its entries)
+// are latency-bound, so there the entries are split into contiguous ranges, one CTA
+// per range and output tile; each writes its partial tile to a scratch array and
+// k_gemm_reduce adds the partials in range order before the usual epilogue, so the
+// result does not depend on scheduling.
 #include "hfmm_internal.cuh"
+
+#include <algorithm>
 
 namespace hfmm {
 
@@ -61,11 +68,14 @@ struct __align__(16) Smem {
 };
 
 template <int R>
-__global__ void __launch_bounds__(128) k_gemm_f64(GemmCall c, int* err) {
+__global__ void __launch_bounds__(128, 5) k_gemm_f64(GemmCall c, int* err) {
     constexpr int TT = TN / R;
     __shared__ Smem sm;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int tile = blockIdx.x, m0 = blockIdx.y * TM, fam = blockIdx.z;
+    const int S = c.n_split > 1 ? c.n_split : 1;
+    const int tile = blockIdx.x, m0 = blockIdx.y * TM, fam = blockIdx.z / S, split = blockIdx.z % S;
+    const int e_lo = (int)((int64_t)split * c.n_entries / S);
+    const int e_hi = (int)((int64_t)(split + 1) * c.n_entries / S);
     const double* const* A = c.A + (int64_t)fam * c.a_fam_stride;
     const double* B0 = c.B0 + (int64_t)fam * c.fam_stride;
     const double* B1 = c.B1 ? c.B1 + (int64_t)fam * c.fam_stride : nullptr;
@@ -108,7 +118,7 @@ __global__ void __launch_bounds__(128) k_gemm_f64(GemmCall c, int* err) {
         int base = 0;
         for (int e0 = 0; e0 < c.n_entries; e0 += 32) {
             int e = e0 + lane;
-            const bool act = e < c.n_entries && A[e] != nullptr && sm.used[e];
+            const bool act = e >= e_lo && e < e_hi && A[e] != nullptr && sm.used[e];
             unsigned bal = __ballot_sync(0xffffffffu, act);
             if (act) sm.act[base + __popc(bal & ((1u << lane) - 1))] = (short)e;
             base += __popc(bal);
@@ -201,6 +211,11 @@ __global__ void __launch_bounds__(128) k_gemm_f64(GemmCall c, int* err) {
             sm.u.C[n + 1][m + 8] = acc[mi][ni][3];
         }
     __syncthreads();
+    if (S > 1) {   // a split: the partial tile goes to the scratch, k_gemm_reduce finishes it
+        double* dst = c.part + ((int64_t)(blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x) * TN * TM;
+        for (int idx = tid; idx < TN * TM; idx += 128) dst[idx] = sm.u.C[idx / TM][idx % TM];
+        return;
+    }
     const double* sc = (fam == 1 && c.scale_f1) ? c.scale_f1 : c.scale;
     for (int idx = tid; idx < TN * (TM / 2); idx += 128) {
         int col = idx / (TM / 2), mm = (idx % (TM / 2)) * 2;
@@ -223,6 +238,63 @@ __global__ void __launch_bounds__(128) k_gemm_f64(GemmCall c, int* err) {
     }
 }
 
+// The split GEMM's epilogue: per output tile, the n_split partial tiles added in
+// entry-range order, then the scale, accumulation and store of k_gemm_f64.
+template <int R>
+__global__ void __launch_bounds__(128) k_gemm_reduce(GemmCall c, int* err) {
+    constexpr int TT = TN / R;
+    __shared__ int tgt[TT];
+    const int tid = threadIdx.x;
+    const int tile = blockIdx.x, m0 = blockIdx.y * TM, fam = blockIdx.z, S = c.n_split;
+    double* out = c.out + (int64_t)fam * c.fam_stride;
+    if (tid < TT) {
+        int t = c.tile_tgt[(int64_t)tile * TT + tid];
+        if (t >= c.nb) {
+            atomicOr(err, ERRF_BOUNDS);
+            t = -1;
+        }
+        tgt[tid] = t;
+    }
+    __syncthreads();
+    const double* sc = (fam == 1 && c.scale_f1) ? c.scale_f1 : c.scale;
+    for (int idx = tid; idx < TN * (TM / 2); idx += 128) {
+        int col = idx / (TM / 2), mm = (idx % (TM / 2)) * 2;
+        int j = col / R, r = col % R;
+        int t = tgt[j];
+        int m = m0 + mm;
+        if (t < 0 || m >= c.ldm) continue;
+        double v0 = 0.0, v1 = 0.0;
+        for (int sp = 0; sp < S; ++sp) {
+            const double* src = c.part +
+                ((int64_t)((fam * S + sp) * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x) * TN * TM;
+            v0 += src[col * TM + mm];
+            v1 += src[col * TM + mm + 1];
+        }
+        if (sc) {
+            v0 *= sc[m];
+            v1 *= sc[m + 1];
+        }
+        double2* o = reinterpret_cast<double2*>(out + ((int64_t)t * R + r) * c.ldm + m);
+        if (c.accumulate) {
+            double2 old = *o;
+            v0 += old.x;
+            v1 += old.y;
+        }
+        *o = make_double2(v0, v1);
+    }
+}
+
+int sm_count() {
+    static int n = 0;
+    if (n == 0) {
+        int dev = 0, v = 0;
+        HFMM_CUDA(cudaGetDevice(&dev));
+        HFMM_CUDA(cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev));
+        n = v > 0 ? v : 148;
+    }
+    return n;
+}
+
 }  // namespace
 
 void gemm_f64(const GemmCall& call, int* d_err, cudaStream_t s) {
@@ -234,10 +306,25 @@ void gemm_f64(const GemmCall& call, int* d_err, cudaStream_t s) {
         throw Error{HFMM_ERR_STATE, "gemm_f64: ld must be a multiple of 16"};
     if (c.k_valid > c.ldk) throw Error{HFMM_ERR_STATE, "gemm_f64: k_valid beyond ldk"};
     if (c.n_entries > MAX_ENTRIES) throw Error{HFMM_ERR_STATE, "gemm_f64: too many entries"};
+    if (c.R != 1 && c.R != 2) throw Error{HFMM_ERR_ARG, "gemm_f64: R must be 1 or 2"};
     dim3 grid(c.ntiles, (c.ldm + TM - 1) / TM, c.n_fam);
+    // entry splits when the grid fills less than the GPU: about two CTAs per SM
+    const int64_t ctas = (int64_t)grid.x * grid.y * grid.z;
+    const int sms = sm_count();
+    int S = 1;
+    if (c.part && c.n_entries > 1 && ctas < sms) {
+        S = (int)std::min<int64_t>({(int64_t)c.n_entries, 16, (2 * sms + ctas - 1) / ctas});
+        while (S > 1 && ctas * S * TN * TM > c.part_cap) --S;
+    }
+    c.n_split = S;
+    grid.z *= S;
     if (c.R == 1) HFMM_LAUNCH(k_gemm_f64<1>, grid, 128, 0, s, c, d_err);
-    else if (c.R == 2) HFMM_LAUNCH(k_gemm_f64<2>, grid, 128, 0, s, c, d_err);
-    else throw Error{HFMM_ERR_ARG, "gemm_f64: R must be 1 or 2"};
+    else HFMM_LAUNCH(k_gemm_f64<2>, grid, 128, 0, s, c, d_err);
+    if (S > 1) {
+        grid.z /= S;
+        if (c.R == 1) HFMM_LAUNCH(k_gemm_reduce<1>, grid, 128, 0, s, c, d_err);
+        else HFMM_LAUNCH(k_gemm_reduce<2>, grid, 128, 0, s, c, d_err);
+    }
 }
 
 }  // namespace hfmm

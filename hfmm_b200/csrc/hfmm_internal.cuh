@@ -218,6 +218,7 @@ struct hfmm_plan {
     // evaluate scratch (allocated at finalize for R = 2)
     hfmm::DevBuf<double> q_s;        // R x n sorted charges
     hfmm::DevBuf<double> check, equiv, loc, tmp;   // [fam][box][R][ld]
+    hfmm::DevBuf<double> gemm_part;  // partial tiles of the main stream's split GEMMs
     hfmm::DevBuf<double> pot;        // per sorted particle: [fam][R] potentials
     hfmm::DevBuf<double> fld;        // per sorted particle: [fam][R][3]
     hfmm::DevBuf<int> d_err;
@@ -276,8 +277,12 @@ struct GemmCall {
     int64_t a_fam_stride;      // entries between the families' A pointer sets
     int n_fam;
     int64_t nb;                // box count (bounds checks)
+    double* part;              // nullable: scratch for entry splits of small grids
+    int64_t part_cap;          // its size in doubles
+    int n_split;               // set by gemm_f64: CTAs per output tile (entry ranges)
 };
 void gemm_f64(const GemmCall& c, int* d_err, cudaStream_t s);
+constexpr int64_t GEMM_PART_CAP = 448LL * 64 * 64;   // doubles: 448 partial 64 x 64 tiles
 
 // ---------------------------------------------------------------- device helpers
 __host__ __device__ inline uint64_t expand_bits(uint64_t v) {
