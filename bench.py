@@ -658,9 +658,11 @@ def run_auto(a, cfg, rank, world, local_rank):
     launches = hfmm_b200.launch_count() - launches0
     clocks = sampler.stop() if sampler else None
     phase = np.zeros(_lib.N_PHASES)
-    _lib.check(_lib.lib.hfmm_plan_phase_times(st.handle, phase.ctypes.data))
-    phase /= a.steps
-    _lib.check(_lib.lib.hfmm_plan_set_profiling(st.handle, 0))
+    if ap.state is st:        # (an order raised inside the timed steps rebuilt the plan)
+        _lib.check(_lib.lib.hfmm_plan_phase_times(st.handle, phase.ctypes.data))
+        phase /= a.steps
+        _lib.check(_lib.lib.hfmm_plan_set_profiling(st.handle, 0))
+    st = ap.state
     ms = _max_over_ranks(dist, torch, dev, ms)
     phi, E = out_dev["r"]
     tg = np.random.default_rng(42 + n + 1).choice(n, min(a.targets, n), replace=False)
@@ -689,6 +691,7 @@ def run_auto(a, cfg, rank, world, local_rank):
     st_info = dict(n_s=st.info["n_s"], max_depth=st.max_depth, n_boxes=st.info["n_boxes"],
                    ranks=dict(getattr(st, "m2l_ranks", {})))
     ap_cmp, ap_report, n_check = ap.m2l_compress, dict(ap.report), int(len(ap.check_idx))
+    ap_p_network = ap.p_network
     ap.close()
     torch.cuda.empty_cache()
 
@@ -805,6 +808,7 @@ def run_auto(a, cfg, rank, world, local_rank):
             "config": {"workload": f"{workload}, tol {a.tol:g}, learned p and leaf, "
                                    "mixed precision, certified on 256 targets, potential+field",
                        "n_points": n, "k": cfg["k"], "tol": a.tol, "p": last["p"],
+                       "p_network": ap_p_network,
                        "leaf": last["leaf"], "n_s": st_info["n_s"], "max_depth": st_info["max_depth"],
                        "precision": "mixed" if last["precision"] == 1 else "fp64",
                        "m2l_compress": ap_cmp,
@@ -816,6 +820,11 @@ def run_auto(a, cfg, rank, world, local_rank):
             "certification": {"targets": n_check, "tol": a.tol,
                               "steps_certified": int(sum(r["certified"] for r in reports)),
                               "steps_fallback": int(sum(r["fallback"] for r in reports)),
+                              "steps_raised": int(sum(r.get("raised", 0) > 0 for r in reports)),
+                              "note": "a miss raises the plan's order (mixed, up to the "
+                                      "conservative one) and the plan keeps the certified "
+                                      "order; warm-up steps absorb that, p_network is the "
+                                      "network's own choice",
                               "error_256": last["error"]},
             "accuracy": acc, "setup_s": setup_s,
             "phase_ms": {k: float(v) for k, v in zip(_lib.PHASES, phase)},
@@ -862,6 +871,15 @@ def run_batch(a, cfg, rank, world, local_rank):
     ab.bind([q for _, _, q in probs], field=True)
     torch.cuda.synchronize()
     setup_s = time.time() - t0
+    p_network = [c[0] for c in ab.choice]
+    raised = 0
+    for _ in range(3):        # problems whose in-graph check missed take the next order
+        ab.batch.launch(stream)
+        torch.cuda.synchronize()
+        r = ab.raise_missed()
+        raised += len(r)
+        if not r:
+            break
     for _ in range(a.warmup):
         ab.batch.launch(stream)
     torch.cuda.synchronize()
@@ -904,7 +922,8 @@ def run_batch(a, cfg, rank, world, local_rank):
             "data": "synthetic (seeded uniform points and N(0,1) complex charges)",
             "config": {"workload": cfg["workload"], "problems": len(probs), "points_total": n_tot,
                        "n_streams": ab.batch.n_streams, "queued_m2l": bool(ab.batch.queued),
-                       "autotune_ms": getattr(ab, "tune_ms", None), "p_chosen": ps, "tol": a.tol,
+                       "autotune_ms": getattr(ab, "tune_ms", None), "p_chosen": ps,
+                       "p_network": p_network, "orders_raised_before_timing": raised, "tol": a.tol,
                        "parallelism": f"replicas x{world}",
                        "l2": "inputs larger than L2 (64 problems' expansions and workspaces)"},
             "certification": {"certified": int(sum(r["certified"] for r in rep)),

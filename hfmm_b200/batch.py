@@ -37,6 +37,7 @@ class Batch:
             raise ValueError("a batch needs at least one plan")
         self.states = list(states)
         self.n_streams = int(n_streams)
+        self.queue = bool(queue)
         arr = (_lib.ctypes.c_void_p * len(states))(*[s.handle for s in states])
         h = _lib.ctypes.c_void_p()
         with torch.cuda.device(states[0].device):
@@ -286,6 +287,35 @@ class AutoBatch:
         error misses the tolerance are not rerun here; ``certify`` does that."""
         outs = self.batch.solve(charges)
         return outs, self.batch.check_rel_errors()
+
+    def raise_missed(self, field=None):
+        """After a launch: every problem whose in-graph check missed the tolerance moves
+        to the next order (same leaf size, the precision rule of that order, up to
+        P_MAX), and the batch is captured again with the same stream count and queue
+        setting. Returns the indices raised (empty: every problem certified)."""
+        from . import setup
+        from .learned import P_MAX, precision_for, compress_for
+        field = self._field if field is None else field
+        errs = self.batch.check_rel_errors()
+        missed = [i for i, (a, b) in enumerate(errs)
+                  if max(a, b if field else 0.0) > self.tol and self.choice[i][0] < P_MAX]
+        if not missed:
+            return []
+        S, queue = self.batch.n_streams, self.batch.queue
+        self.batch.close()
+        for i in missed:
+            p, leaf = self.choice[i]
+            p += 1
+            prec = precision_for(self.tol, p)
+            x, k = self.problems[i]
+            self.states[i].close()
+            self.states[i] = setup(x, k, p=p, N_max=leaf, device=self.device, stream_tables=True,
+                                   m2l_compress=compress_for(self.tol, prec))
+            self.choice[i] = (p, leaf)
+            self.precisions[i] = prec
+        self.batch = Batch(self.states, S, queue)
+        self.batch.bind(self._q, self._field, self.precisions, checks=self.checks)
+        return missed
 
     def certify(self):
         """Read the in-graph check of the last launch (the direct sum at each problem's

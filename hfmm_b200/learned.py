@@ -41,7 +41,7 @@ LEAVES = (16, 32, 64, 128)
 FEATURE_LEAF = 64          # the tree the features are read from
 TOL_MIXED = 1e-6           # the mixed-precision path is used at tolerances >= this
 TOL_LEARNED = 3e-7         # below this the network is not consulted (outside its training range)
-KD_TRAINED = 24.0          # largest k x domain extent of the committed training sweep
+KD_TRAINED = 50.0          # largest k x domain extent of the committed training sweep
 KD_TRUSTED = 1.5 * KD_TRAINED   # beyond this the network is not consulted either
 DEFAULT_WEIGHTS = os.path.join(os.path.dirname(__file__), "data", "order_net.npz")
 
@@ -55,9 +55,9 @@ def conservative_p(tol):
 def network_applies(feats, tol):
     """Whether the network's order may be used for these features: the tolerance is
     in its training range and k x extent at most 1.5 times the largest one it saw
-    (24 in the sweep). Measured: at k x extent up to 30 (the batched workload) its
-    orders certified 62 of 64 problems; at 44 (8M clustered points, k = 40) p = 9
-    missed 1e-6 and every step fell back to the plain FP64 rerun."""
+    (50 in the sweep). Measured with an earlier network trained up to 24: at 44 (8M
+    clustered points, k = 40) its p = 9 missed 1e-6 and every step fell back to the
+    plain FP64 rerun, which is what the guard is for."""
     return tol >= TOL_LEARNED and float(feats[1]) <= KD_TRUSTED
 
 
@@ -255,7 +255,10 @@ class AutoPlan:
     conservative order in place of the network's (the ablation: the same
     precision rule, leaf size and certification, only the network removed). ``n_check`` random
     targets (seeded) are compared against the FP64 direct sum on every evaluate.
-    After a call, ``report`` holds the order, leaf, precision, measured error and
+    When the network's order misses the tolerance, the plan steps its order up (in
+    mixed precision while it applies, up to the conservative order) and keeps the
+    order that certified; past that the plain FP64 rerun decides. After a call,
+    ``report`` holds the order, leaf, precision, measured error, the steps raised and
     whether the plain rerun was taken.
     """
 
@@ -277,6 +280,7 @@ class AutoPlan:
                 net = OrderNet.load(device=self.device) if net is None else net
                 self.p, self.leaf = net.choose(self.feats, margin)
                 self.network_used = True
+        self.p_network = self.p if self.network_used else None
         self.precision = precision_for(self.tol, self.p)
         self.m2l_compress = compress_for(self.tol, self.precision)
         self.state = setup(positions, k, p=self.p, N_max=self.leaf, device=self.device,
@@ -330,6 +334,16 @@ class AutoPlan:
             err = torch.maximum(err, rel(E[i], ref[1]))
         return float(err.item())
 
+    def _raise_order(self, p):
+        """Rebuild the plan at order ``p`` (same leaf size, the precision rule of p)."""
+        from . import setup
+        self.state.close()
+        self.p = int(p)
+        self.precision = precision_for(self.tol, self.p)
+        self.m2l_compress = compress_for(self.tol, self.precision)
+        self.state = setup(self.positions, self.k, p=self.p, N_max=self.leaf, device=self.device,
+                           m2l_compress=self.m2l_compress)
+
     def _plain_state(self, p):
         from . import setup
         if p not in self._plain:
@@ -367,7 +381,17 @@ class AutoPlan:
             check_errors(self.state)
             err = self._error(phi, E, ref)
             rep = dict(p=self.p, leaf=self.leaf, precision=int(self.precision), error=err,
-                       fallback=False, p_final=self.p, network=self.network_used)
+                       fallback=False, p_final=self.p, network=self.network_used, raised=0)
+            # a miss at the network's order: the next orders in the plan's own precision
+            # first (up to the conservative one); the plan keeps the order that certified,
+            # so later evaluates start there (the network's p stays in p_network)
+            while err > self.tol and self.network_used and self.p < self.p_plain:
+                self._raise_order(self.p + 1)
+                evaluate_into(self.state, q_re, q_im, phi, E, self.precision)
+                check_errors(self.state)
+                err = self._error(phi, E, ref)
+                rep.update(p_final=self.p, error=err, precision=int(self.precision),
+                           raised=rep["raised"] + 1)
             p = self.p_plain
             while err > self.tol and p <= P_MAX:
                 st = self._plain_state(p)

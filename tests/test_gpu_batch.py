@@ -318,3 +318,33 @@ def test_solve_from_host_rescales_exactly():
     b.close()
     for st in states:
         st.close()
+
+
+def test_auto_batch_raises_the_missed_orders():
+    """AutoBatch.raise_missed: problems whose in-graph check missed the tolerance take
+    the next order and the batch is captured again; a few rounds certify every one."""
+    from hfmm_b200.batch import AutoBatch
+    probs = _batch_problems()[:3]
+    ab = AutoBatch([(x, k) for x, k, _, _ in probs], tol=1e-6, net=False, n_streams=2)
+    ab.choice = [(6, leaf) for _, leaf in ab.choice]        # start every problem too low
+    import hfmm_b200 as hf
+    from hfmm_b200.learned import precision_for, compress_for
+    for i, ((x, k), (p, leaf)) in enumerate(zip(ab.problems, ab.choice)):
+        ab.states[i].close()
+        ab.precisions[i] = precision_for(ab.tol, p)
+        ab.states[i] = hf.setup(x, k, p=p, N_max=leaf, stream_tables=True,
+                                m2l_compress=compress_for(ab.tol, ab.precisions[i]))
+    ab.bind([q for _, _, q, _ in probs], field=True)
+    raised = []
+    for _ in range(8):
+        ab.batch.launch()
+        torch.cuda.synchronize()
+        r = ab.raise_missed()
+        raised += r
+        if not r:
+            break
+    assert raised and not r
+    rep = ab.certify()
+    assert all(x["certified"] and not x["fallback"] for x in rep)
+    assert all(c[0] >= 6 for c in ab.choice) and max(c[0] for c in ab.choice) > 6
+    ab.close()

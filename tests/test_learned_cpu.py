@@ -128,7 +128,9 @@ def test_network_is_consulted_only_in_its_range():
     f = np.zeros(24, np.float32)
     f[1] = 30.0                                   # the batched workload's largest k x extent
     assert network_applies(f, 1e-6)
-    f[1] = 44.0                                   # 8M clustered points at k = 40
+    f[1] = 44.0                                   # 8M clustered points at k = 40: in the sweep
+    assert network_applies(f, 1e-6)
+    f[1] = KD_TRUSTED + 1.0                       # beyond 1.5 x the sweep's largest (50)
     assert not network_applies(f, 1e-6)
     f[1] = KD_TRUSTED
     assert network_applies(f, 1e-6)
