@@ -83,6 +83,9 @@ def parse():
     ap.add_argument("--tol", type=float, default=1e-6)
     ap.add_argument("--no-plain", action="store_true",
                     help="auto mode: skip the plain FP64 comparison run")
+    ap.add_argument("--per-level-m2l", action="store_true",
+                    help="the low-rank M2L as one launch per level and family on side streams "
+                         "instead of the plan's queued launch (hfmm_plan_set_m2l_queue)")
     ap.add_argument("--no-plain-at-tol", action="store_true",
                     help="auto mode: skip the plain FP64 run at the lowest p meeting the tolerance")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
@@ -627,6 +630,8 @@ def run_auto(a, cfg, rank, world, local_rank):
     n = cfg["n"]
     t0 = time.time()
     ap = learned.AutoPlan(pos, cfg["k"], tol=a.tol, device=dev)
+    if a.per_level_m2l:
+        _lib.check(_lib.lib.hfmm_plan_set_m2l_queue(ap.state.handle, 0))
     torch.cuda.synchronize()
     setup_s = time.time() - t0
     q_dev = torch.as_tensor(q).to(dev)

@@ -306,6 +306,72 @@ MixedCall cx_call(hfmm_plan* P, int l, int f, int R) {
     return mc;
 }
 
+std::string queue_items(hfmm_plan* const* plans, int n_plans, int R, std::vector<MixedCall>& calls,
+                        std::vector<MixedMaps>& maps, std::vector<M2LItem>& items) {
+    struct Keyed {
+        double cost;
+        M2LItem it;
+    };
+    std::vector<Keyed> list;
+    calls.clear();
+    maps.clear();
+    items.clear();
+    for (int i = 0; i < n_plans; ++i) {
+        hfmm_plan* P = plans[i];
+        for (int l = 2; l <= P->md; ++l)
+            for (int f = 0; f < P->n_fam; ++f) {
+                MixedCall c = cx_call(P, l, f, R);
+                if (c.ntiles == 0) continue;
+                c.wait_ns = 0;
+                c.starve = 0;
+                if ((int64_t)c.nb * R * c.ldk >= ((int64_t)1 << 31))
+                    return "a level's densities exceed 32-bit gather offsets";
+                const int id = (int)calls.size();
+                calls.push_back(c);
+                maps.push_back(static_cast<MixedMaps*>(P->cx_maps)[f * MAX_LEVELS + l]);
+                const int blocks = (c.ldm + 127) / 128;
+                const int valid = c.m_valid > 0 ? c.m_valid : c.ldm;
+                for (int t = 0; t < c.ntiles; ++t)
+                    for (int b = 0; b < blocks; ++b) {
+                        const double cost = (double)(c.ldk / 32) * (valid - 128 * b <= 64 ? 0.6 : 1.0);
+                        list.push_back({cost, M2LItem{id, t, b}});
+                    }
+            }
+    }
+    if (list.empty()) return "no M2L work";
+    std::stable_sort(list.begin(), list.end(), [](const Keyed& a, const Keyed& b) { return a.cost > b.cost; });
+    for (auto& k : list) items.push_back(k.it);
+    return "";
+}
+
+void plan_queue_release(hfmm_plan* P) {
+    for (auto*& q : P->cxq) {
+        delete static_cast<PlanQueue*>(q);
+        q = nullptr;
+    }
+}
+
+void plan_queue_build(hfmm_plan* P) {
+    plan_queue_release(P);
+    if (!P->compressed || !P->mixed_ready) return;
+    for (int R = 1; R <= 2; ++R) {
+        std::vector<MixedCall> calls;
+        std::vector<MixedMaps> maps;
+        std::vector<M2LItem> items;
+        if (!queue_items(&P, 1, R, calls, maps, items).empty()) continue;
+        auto* q = new PlanQueue;
+        P->cxq[R - 1] = q;
+        q->calls.alloc(calls.size());
+        q->maps.alloc(maps.size());
+        q->items.alloc(items.size());
+        q->next.alloc(1);
+        HFMM_CUDA(cudaMemcpy(q->calls.p, calls.data(), calls.size() * sizeof(MixedCall), cudaMemcpyHostToDevice));
+        HFMM_CUDA(cudaMemcpy(q->maps.p, maps.data(), maps.size() * sizeof(MixedMaps), cudaMemcpyHostToDevice));
+        HFMM_CUDA(cudaMemcpy(q->items.p, items.data(), items.size() * sizeof(M2LItem), cudaMemcpyHostToDevice));
+        q->n_items = (int)items.size();
+    }
+}
+
 void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double* phi, double* E,
                    cudaStream_t s, bool mixed, int phase) {
     const bool up = phase & EVAL_UP, down = phase & EVAL_DOWN;
@@ -523,8 +589,28 @@ void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double*
                        s, T.dn_d.p);
             }
     }
+    // The plan's own queued M2L (every level and family in one persistent launch, the
+    // largest items first) in place of the per-level launches on side streams; the test
+    // switches of the M2L kernels (grid mode off) take the per-level path.
+    PlanQueue* pq = (up && use_cx && g_m2l_grid && P->queue_m2l) ? static_cast<PlanQueue*>(P->cxq[R - 1])
+                                                                 : nullptr;
+    if (pq) {
+        {
+            PhaseTimer pt(X, s, 4);
+            m2l_queue(pq->calls.p, pq->maps.p, pq->items.p, pq->n_items, pq->next.p, R, sm_count(), s,
+                      g_m2l_starve);
+        }
+        for (int l = 2; l <= P->md; ++l)
+            for (int f = 0; f < NF; ++f) {
+                LevelTables& T = P->tables[f][l];
+                PhaseTimer pt(X, s, 14);
+                gemm_1(K_EXP, l, f, level_base(T.yc.p, l, T.cmld), T.cmld, P->loc.p + f * fs, P->ld,
+                       s, T.dn_d.p);
+            }
+    }
+    const bool cx_side = up && use_cx && !pq;   // the per-level M2L launches on side streams
     std::unique_ptr<PhaseTimer> m2l_timer;
-    if (up && use_cx) {
+    if (cx_side) {
         // A level's M2L reads only the compressed densities of the upward pass, so the
         // M2Ls of every level and family run at once on the plan's side streams (the
         // coarse levels have a handful of tiles each and would otherwise run alone on
@@ -558,10 +644,10 @@ void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double*
             PhaseTimer pt(X, s, 12);
             generate_m2l_stream(P, l, use_mx, P->ws, s);
         }
-        if (use_cx) {   // this level's M2L ran above, on a side stream (or in the batch queue)
-            if (up)
+        if (use_cx) {   // this level's M2L ran above: on a side stream, or queued
+            if (cx_side)
                 for (int f = 0; f < NF; ++f) HFMM_CUDA(cudaStreamWaitEvent(s, P->cx_level[l][f], 0));
-            if (up && l == P->md) {
+            if (cx_side && l == P->md) {
                 for (int k = 0; k < hfmm_plan::CX_STREAMS; ++k)
                     HFMM_CUDA(cudaStreamWaitEvent(s, P->cx_join[k], 0));
                 m2l_timer.reset();
@@ -986,6 +1072,7 @@ int hfmm_plan_finalize(hfmm_plan* P) {
         P->e_lo.zero();
         P->mixed_ready = true;
     }
+    plan_queue_build(P);
     P->q_s.alloc(2 * P->n);
     P->pot.alloc((size_t)P->n_fam * 2 * P->n);
     P->fld.alloc((size_t)P->n_fam * 2 * 3 * P->n);
@@ -1017,6 +1104,12 @@ int hfmm_evaluate(hfmm_plan* P, const double* q_re, const double* q_im, double* 
     evaluate_fp64(P, q_re, q_im, phi, E, (cudaStream_t)stream, precision == HFMM_PREC_MIXED);
     return HFMM_OK;
     API_END
+}
+
+int hfmm_plan_set_m2l_queue(hfmm_plan* P, int32_t on) {
+    if (!P) return fail(HFMM_ERR_ARG, "plan is NULL");
+    P->queue_m2l = on != 0;
+    return HFMM_OK;
 }
 
 int hfmm_plan_check(hfmm_plan* P, void* stream) {
@@ -1086,6 +1179,7 @@ void hfmm_plan_destroy(hfmm_plan* P) {
     drop_extra(P);
     delete[] static_cast<MixedMaps*>(P->mx_maps);
     P->mx_maps = nullptr;
+    plan_queue_release(P);
     delete[] static_cast<MixedMaps*>(P->cx_maps);
     P->cx_maps = nullptr;
     compressed_release(P);

@@ -126,9 +126,8 @@ __global__ void __launch_bounds__(256) k_check_sums(const double* __restrict__ p
 
 // Work estimate of one evaluate (complex charges): far field M2L+L2L FLOPs and
 // near-field pairs weighted by ~40 flops each; only the relative size matters.
-// The queued M2L's work list (before capture): every plan's low-rank M2L calls and
-// their tensor maps, one item per tile and 128-row block, largest first (an item's
-// cost is its k-chunks per entry; blocks of at most 64 live rows run at half cost).
+// The queued M2L's work list (before capture, queue_items): every plan's low-rank M2L
+// calls and their tensor maps, one item per tile and 128-row block, largest first.
 // Off when a problem is not a low-rank mixed evaluate or the column counts differ.
 void build_queue(hfmm_batch* B) {
     B->queued = false;
@@ -153,40 +152,9 @@ void build_queue(hfmm_batch* B) {
     }
     std::vector<MixedCall> calls;
     std::vector<MixedMaps> maps;
-    struct Keyed {
-        double cost;
-        M2LItem it;
-    };
-    std::vector<Keyed> list;
-    for (auto* P : B->plans)
-        for (int l = 2; l <= P->md; ++l)
-            for (int f = 0; f < P->n_fam; ++f) {
-                MixedCall c = cx_call(P, l, f, R);
-                if (c.ntiles == 0) continue;
-                c.wait_ns = 0;
-                c.starve = g_m2l_starve;
-                if ((int64_t)c.nb * R * c.ldk >= ((int64_t)1 << 31)) {
-                    B->queue_note = "a level's densities exceed 32-bit gather offsets";
-                    return;
-                }
-                const int id = (int)calls.size();
-                calls.push_back(c);
-                maps.push_back(static_cast<MixedMaps*>(P->cx_maps)[f * MAX_LEVELS + l]);
-                const int blocks = (c.ldm + 127) / 128;
-                const int valid = c.m_valid > 0 ? c.m_valid : c.ldm;
-                for (int t = 0; t < c.ntiles; ++t)
-                    for (int b = 0; b < blocks; ++b) {
-                        const double cost = (double)(c.ldk / 32) * (valid - 128 * b <= 64 ? 0.6 : 1.0);
-                        list.push_back({cost, M2LItem{id, t, b}});
-                    }
-            }
-    if (list.empty()) {
-        B->queue_note = "no M2L work";
-        return;
-    }
-    std::stable_sort(list.begin(), list.end(), [](const Keyed& a, const Keyed& b) { return a.cost > b.cost; });
     std::vector<M2LItem> items;
-    for (auto& k : list) items.push_back(k.it);
+    B->queue_note = queue_items(B->plans.data(), (int)B->plans.size(), R, calls, maps, items);
+    if (!B->queue_note.empty()) return;
     B->q_calls.alloc(calls.size());
     B->q_maps.alloc(maps.size());
     B->q_items.alloc(items.size());
@@ -371,7 +339,7 @@ int hfmm_batch_capture(hfmm_batch* B) {
                 int sms = 148;
                 HFMM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, B->device));
                 m2l_queue(B->q_calls.p, B->q_maps.p, B->q_items.p, B->n_items, B->q_next.p, B->queue_R,
-                          sms, s0);
+                          sms, s0, g_m2l_starve);
                 HFMM_CUDA(cudaEventRecord(B->events[0], s0));
                 for (int s = 1; s < S; ++s) HFMM_CUDA(cudaStreamWaitEvent(B->streams[s], B->events[0], 0));
             }

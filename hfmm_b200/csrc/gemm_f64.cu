@@ -284,6 +284,8 @@ __global__ void __launch_bounds__(128) k_gemm_reduce(GemmCall c, int* err) {
     }
 }
 
+}  // namespace
+
 int sm_count() {
     static int n = 0;
     if (n == 0) {
@@ -294,8 +296,6 @@ int sm_count() {
     }
     return n;
 }
-
-}  // namespace
 
 void gemm_f64(const GemmCall& call, int* d_err, cudaStream_t s) {
     if (call.ntiles == 0) return;

@@ -197,6 +197,8 @@ struct hfmm_plan {
     void* mx_maps = nullptr;                // MixedMaps per level (host array)
     bool compressed = false;                // every level has a compressed M2L (mixed path)
     void* cx_maps = nullptr;                // MixedMaps [2][MAX_LEVELS] of the C_d tables
+    void* cxq[2] = {nullptr, nullptr};      // PlanQueue per charge-column count (finalize)
+    bool queue_m2l = true;                  // run the low-rank M2L as the plan's queue
     cudaStream_t nf_side = nullptr;         // the near field's stream (runs beside the far field)
     cudaEvent_t nf_fork = nullptr, nf_join = nullptr;
     static constexpr int CX_STREAMS = 4;    // side streams of the concurrent compressed M2L
@@ -282,6 +284,7 @@ struct GemmCall {
     int n_split;               // set by gemm_f64: CTAs per output tile (entry ranges)
 };
 void gemm_f64(const GemmCall& c, int* d_err, cudaStream_t s);
+int sm_count();   // multiprocessors of the current device (read once)
 constexpr int64_t GEMM_PART_CAP = 448LL * 64 * 64;   // doubles: 448 partial 64 x 64 tiles
 
 // ---------------------------------------------------------------- device helpers

@@ -125,7 +125,8 @@ __device__ __forceinline__ bool next_item(QueueCtl& ctl, const MixedCall* __rest
 template <int R>
 __global__ void __launch_bounds__(THREADS, 1)
     k_m2l_queue(const MixedCall* __restrict__ calls, const MixedMaps* __restrict__ maps,
-                const M2LItem* __restrict__ items, int n_items, int* next, uint64_t wait_ns_in) {
+                const M2LItem* __restrict__ items, int n_items, int* next, uint64_t wait_ns_in,
+                int starve) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     unsigned char* sm = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     QueueCtl& ctl = *reinterpret_cast<QueueCtl*>(sm + STAGES * STAGE_BYTES);
@@ -217,7 +218,7 @@ __global__ void __launch_bounds__(THREADS, 1)
                         cp_async16(sbh + soff[i], c.Bhi + o, ok);
                         cp_async16(sbl + soff[i], c.Blo + o, ok);
                     }
-                    if (!(c.starve && qg == 0))   // (test: the CTA's first stage never fills)
+                    if (!(starve && qg == 0))   // (test: the CTA's first stage never fills)
                         asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(
                                          smem_u32(&ctl.full[st]))
                                      : "memory");
@@ -310,7 +311,7 @@ __global__ void __launch_bounds__(THREADS, 1)
                 for (int q = 0; q < nq; ++q) {
                     const int qg = q_total + q, st = qg % STAGES;
                     if (!mbar_wait(smem_u32(&ctl.empty[st]), ((qg / STAGES) & 1) ^ 1, abort_flag, wait_ns)) break;
-                    if (c.grid && c.starve && qg == 0) continue;   // (test: stage 0 never fills)
+                    if (c.grid && starve && qg == 0) continue;   // (test: stage 0 never fills)
                     const int e = ctl.act[q / kch];
                     const int z = ctl.zidx[q / kch];
                     const int k0 = (q % kch) * BK;
@@ -430,7 +431,7 @@ void check_queue_split() {
 size_t m2l_queue_smem() { return (size_t)STAGES * STAGE_BYTES + sizeof(QueueCtl) + 1024; }
 
 void m2l_queue(const MixedCall* calls, const MixedMaps* maps, const M2LItem* items, int n_items,
-               int* next, int R, int n_ctas, cudaStream_t s) {
+               int* next, int R, int n_ctas, cudaStream_t s, int starve) {
     if (n_items <= 0) return;
     check_queue_split();
     const size_t smem = m2l_queue_smem();
@@ -438,10 +439,12 @@ void m2l_queue(const MixedCall* calls, const MixedMaps* maps, const M2LItem* ite
     HFMM_CUDA(cudaMemsetAsync(next, 0, sizeof(int), s));
     if (R == 1) {
         HFMM_CUDA(cudaFuncSetAttribute(k_m2l_queue<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        HFMM_LAUNCH(k_m2l_queue<1>, grid, THREADS, smem, s, calls, maps, items, n_items, next, g_m2l_wait_ns);
+        HFMM_LAUNCH(k_m2l_queue<1>, grid, THREADS, smem, s, calls, maps, items, n_items, next, g_m2l_wait_ns,
+                    starve);
     } else {
         HFMM_CUDA(cudaFuncSetAttribute(k_m2l_queue<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        HFMM_LAUNCH(k_m2l_queue<2>, grid, THREADS, smem, s, calls, maps, items, n_items, next, g_m2l_wait_ns);
+        HFMM_LAUNCH(k_m2l_queue<2>, grid, THREADS, smem, s, calls, maps, items, n_items, next, g_m2l_wait_ns,
+                    starve);
     }
 }
 

@@ -4,6 +4,9 @@
 
 #include <cuda.h>
 
+#include <string>
+#include <vector>
+
 namespace hfmm {
 
 // TMA descriptors of one level's TF32 hi/lo tables, per kernel family:
@@ -65,9 +68,27 @@ struct M2LItem {
     int call, tile, mblock;
 };
 // Persistent M2L over items (sorted by the caller), n_ctas resident CTAs; `next` is a
-// device int the launch resets. calls, maps and items live in device memory.
+// device int the launch resets. calls, maps and items live in device memory. The wait
+// limit comes from g_m2l_wait_ns at launch; starve (a test switch) leaves every CTA's
+// first stage unfilled.
 void m2l_queue(const MixedCall* calls, const MixedMaps* maps, const M2LItem* items, int n_items,
-               int* next, int R, int n_ctas, cudaStream_t s);
+               int* next, int R, int n_ctas, cudaStream_t s, int starve = 0);
+// The work list of a queued M2L over the plans given: every (plan, level, family)
+// low-rank call with its tensor maps, one item per tile and 128-row block, largest
+// first (cost: k-chunks per entry, 0.6 for a block of at most 64 live rows). Returns
+// "" when it applies, else why not (32-bit gather offsets would overflow).
+std::string queue_items(hfmm_plan* const* plans, int n_plans, int R, std::vector<MixedCall>& calls,
+                        std::vector<MixedMaps>& maps, std::vector<M2LItem>& items);
+// A plan's own queued M2L for R charge columns, built and uploaded at finalize.
+struct PlanQueue {
+    DevBuf<MixedCall> calls;
+    DevBuf<MixedMaps> maps;
+    DevBuf<M2LItem> items;
+    DevBuf<int> next;
+    int n_items = 0;
+};
+void plan_queue_build(hfmm_plan* P);     // both charge-column counts
+void plan_queue_release(hfmm_plan* P);
 size_t m2l_queue_smem();
 size_t m2l_tf32x3_smem();
 

@@ -310,6 +310,12 @@ void hfmm_batch_destroy(hfmm_batch* batch);
  * hfmm_batch_queue_note why not (an empty string when it does; valid until the
  * next capture or the batch's destruction). */
 int hfmm_batch_set_queue(hfmm_batch* batch, int32_t on);
+/* The low-rank mixed M2L of one plan's evaluate (no counterpart in the reference): with
+ * on != 0 (the default) every level and family runs in ONE persistent launch over the
+ * plan's own queue of (level, family, tile, row block) items, largest first, built at
+ * finalize; on == 0 launches one kernel per level and family on the plan's side
+ * streams. Results are the same bit for bit. */
+int hfmm_plan_set_m2l_queue(hfmm_plan* plan, int32_t on);
 int hfmm_batch_queued(const hfmm_batch* batch);
 const char* hfmm_batch_queue_note(const hfmm_batch* batch);
 
