@@ -779,8 +779,11 @@ def run_auto(a, cfg, rank, world, local_rank):
         roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                 "frac": (achieved / peak) if achieved else None, "traffic": _traffic(a, "auto"),
                 "traffic_unit": "bytes per evaluate (all M2L launches), from profiles/traffic.json",
-                "kernel": ("k_m2l_tf32x3 (M2L, 3xTF32 on tcgen05, all levels"
-                           + (", on the low-rank C_d tables)" if ap_cmp else ")")),
+                "kernel": (("k_m2l_queue (the plan's low-rank M2L: every level and family in "
+                            "one persistent launch, 3xTF32 on tcgen05, on the C_d tables)")
+                           if ap_cmp and not a.per_level_m2l else
+                           ("k_m2l_tf32x3 (M2L, 3xTF32 on tcgen05, one launch per level and family"
+                            + (", on the low-rank C_d tables)" if ap_cmp else ")"))),
                 "algorithmic_flops_per_evaluate": flops, "kernel_ms_per_evaluate": dom_ms,
                 "flop_count": ("3 TF32 products x 2 r^2 per V pair, charge column and family, "
                                "r = the rank of the pair's level and family (unpadded)"

@@ -308,12 +308,13 @@ void gemm_f64(const GemmCall& call, int* d_err, cudaStream_t s) {
     if (c.n_entries > MAX_ENTRIES) throw Error{HFMM_ERR_STATE, "gemm_f64: too many entries"};
     if (c.R != 1 && c.R != 2) throw Error{HFMM_ERR_ARG, "gemm_f64: R must be 1 or 2"};
     dim3 grid(c.ntiles, (c.ldm + TM - 1) / TM, c.n_fam);
-    // entry splits when the grid fills less than the GPU: about two CTAs per SM
+    // entry splits when the grid gives the SMs fewer than four CTAs each (a CTA of 128
+    // threads hides little latency on its own): up to about four per SM
     const int64_t ctas = (int64_t)grid.x * grid.y * grid.z;
     const int sms = sm_count();
     int S = 1;
-    if (c.part && c.n_entries > 1 && ctas < sms) {
-        S = (int)std::min<int64_t>({(int64_t)c.n_entries, 16, (2 * sms + ctas - 1) / ctas});
+    if (c.part && c.n_entries > 1 && ctas < 4 * sms) {
+        S = (int)std::min<int64_t>({(int64_t)c.n_entries, 16, (4 * sms + ctas - 1) / ctas});
         while (S > 1 && ctas * S * TN * TM > c.part_cap) --S;
     }
     c.n_split = S;

@@ -285,7 +285,7 @@ struct GemmCall {
 };
 void gemm_f64(const GemmCall& c, int* d_err, cudaStream_t s);
 int sm_count();   // multiprocessors of the current device (read once)
-constexpr int64_t GEMM_PART_CAP = 448LL * 64 * 64;   // doubles: 448 partial 64 x 64 tiles
+constexpr int64_t GEMM_PART_CAP = 768LL * 64 * 64;   // doubles: 768 partial 64 x 64 tiles
 
 // ---------------------------------------------------------------- device helpers
 __host__ __device__ inline uint64_t expand_bits(uint64_t v) {
