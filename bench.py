@@ -448,6 +448,8 @@ def run_ours(a, cfg, rank, world, local_rank):
     t0 = time.time()
     st = hfmm_b200.setup(pos, cfg["k"], p=cfg["p"], N_max=cfg["leaf"], max_depth=cfg["max_depth"],
                          device=dev, m2l_compress=a.m2l_compress)
+    if a.per_level_m2l:
+        _lib.check(_lib.lib.hfmm_plan_set_m2l_queue(st.handle, 0))
     torch.cuda.synchronize()
     setup_s = time.time() - t0
     n = cfg["n"]
