@@ -372,8 +372,32 @@ void plan_queue_build(hfmm_plan* P) {
     }
 }
 
+namespace {
+// The far-field chain (every phase but the near field) runs on the plan's own stream of
+// the highest priority, forked from the caller's stream and joined back on every exit:
+// the block scheduler then serves the chain first and the near field, on its default-
+// priority side stream, fills the SMs the chain leaves free.
+struct CritStream {
+    cudaStream_t caller, s;
+    hfmm_plan* P;
+    CritStream(hfmm_plan* p, cudaStream_t c) : caller(c), s(c), P(p) {
+        if (!P->crit) return;
+        HFMM_CUDA(cudaEventRecord(P->crit_fork, caller));
+        HFMM_CUDA(cudaStreamWaitEvent(P->crit, P->crit_fork, 0));
+        s = P->crit;
+    }
+    ~CritStream() {
+        if (s == caller) return;
+        cudaEventRecord(P->crit_join, s);
+        cudaStreamWaitEvent(caller, P->crit_join, 0);
+    }
+};
+}  // namespace
+
 void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double* phi, double* E,
-                   cudaStream_t s, bool mixed, int phase) {
+                   cudaStream_t s_caller, bool mixed, int phase) {
+    CritStream crit(P, s_caller);
+    cudaStream_t s = crit.s;
     const bool up = phase & EVAL_UP, down = phase & EVAL_DOWN;
     const int R = q_im ? 2 : 1;
     const int NF = P->n_fam;
@@ -1023,6 +1047,13 @@ int hfmm_plan_finalize(hfmm_plan* P) {
     compressed_prepare(P);
     PlanExtra* X = extra(P, true);
     build_a_ptrs(P, X->ix);   // streamed plans without a workspace yet: see evaluate
+    if (!P->crit) {
+        int lo = 0, hi = 0;
+        HFMM_CUDA(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+        HFMM_CUDA(cudaStreamCreateWithPriority(&P->crit, cudaStreamNonBlocking, hi));
+        HFMM_CUDA(cudaEventCreateWithFlags(&P->crit_fork, cudaEventDisableTiming));
+        HFMM_CUDA(cudaEventCreateWithFlags(&P->crit_join, cudaEventDisableTiming));
+    }
     if (!P->nf_side) {
         HFMM_CUDA(cudaStreamCreateWithFlags(&P->nf_side, cudaStreamNonBlocking));
         HFMM_CUDA(cudaEventCreateWithFlags(&P->nf_fork, cudaEventDisableTiming));
@@ -1184,6 +1215,9 @@ void hfmm_plan_destroy(hfmm_plan* P) {
     P->cx_maps = nullptr;
     compressed_release(P);
     if (P->nf_side) cudaStreamDestroy(P->nf_side);
+    if (P->crit) cudaStreamDestroy(P->crit);
+    if (P->crit_fork) cudaEventDestroy(P->crit_fork);
+    if (P->crit_join) cudaEventDestroy(P->crit_join);
     if (P->nf_fork) cudaEventDestroy(P->nf_fork);
     if (P->nf_join) cudaEventDestroy(P->nf_join);
     delete P;

@@ -200,6 +200,8 @@ struct hfmm_plan {
     void* cxq[2] = {nullptr, nullptr};      // PlanQueue per charge-column count (finalize)
     bool queue_m2l = true;                  // run the low-rank M2L as the plan's queue
     cudaStream_t nf_side = nullptr;         // the near field's stream (runs beside the far field)
+    cudaStream_t crit = nullptr;            // highest-priority stream of the far-field chain
+    cudaEvent_t crit_fork = nullptr, crit_join = nullptr;
     cudaEvent_t nf_fork = nullptr, nf_join = nullptr;
     static constexpr int CX_STREAMS = 4;    // side streams of the concurrent compressed M2L
     cudaStream_t cx_side[CX_STREAMS] = {};
