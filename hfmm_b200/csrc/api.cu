@@ -429,9 +429,10 @@ void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double*
 
     // The near field needs only the gathered charges: it runs on the plan's side
     // stream beside the whole far field and joins before L2P, which adds into the
-    // potentials and fields P2P stores.
-    if (up) {
-        HFMM_CUDA(cudaEventRecord(P->nf_fork, s));
+    // potentials and fields P2P stores. It is enqueued after P2M (below), so that the
+    // far field's first kernel takes the SMs first.
+    if (up) HFMM_CUDA(cudaEventRecord(P->nf_fork, s));
+    auto launch_near_field = [&]() {
         HFMM_CUDA(cudaStreamWaitEvent(P->nf_side, P->nf_fork, 0));
         ParticlePass p = base;
         p.op = ParticleOp::P2P;
@@ -444,7 +445,7 @@ void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double*
             particles(p, P->nf_side);
         }
         HFMM_CUDA(cudaEventRecord(P->nf_join, P->nf_side));
-    }
+    };
 
     // scale_up / scale_dn: multiply row m of family f's result by the level's decode
     // scale d (the folded low-rank plan's GEMMs end in scaled SVD coordinates)
@@ -530,8 +531,11 @@ void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double*
         p.nrows = P->n_leaves;
         p.surf = P->check_pts.p;
         p.out = P->check.p;
-        PhaseTimer pt(X, s, 1);
-        particles(p, s);
+        {
+            PhaseTimer pt(X, s, 1);
+            particles(p, s);
+        }
+        launch_near_field();
     }
     if (!up) {
     } else if (use_cx) {
