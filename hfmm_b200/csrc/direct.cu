@@ -136,20 +136,25 @@ __global__ void __launch_bounds__(DT) k_direct_partial(const double* __restrict_
         for (int v = 0; v < NV; ++v) scratch[((int64_t)split * n_t + ti) * NV + v] = acc[v];
 }
 
+// The chunks' partial sums of one (target, value) pair added by one warp: lane j takes
+// chunks j, j + 32, ... in order, then a fixed shuffle tree adds the lanes, so the
+// result does not depend on scheduling. (One thread per target had walked all chunks
+// serially: 0.26 ms for the 256-target check at 1e6 sources.)
 __global__ void k_direct_reduce(const double* __restrict__ scratch, int64_t n_t, int n_split,
                                 int field, double* phi, double* fld) {
-    int64_t ti = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (ti >= n_t) return;
-    double acc[NV] = {0, 0, 0, 0, 0, 0, 0, 0};
-    for (int s = 0; s < n_split; ++s)
-        for (int v = 0; v < NV; ++v) acc[v] += scratch[((int64_t)s * n_t + ti) * NV + v];
-    phi[2 * ti] = acc[0];
-    phi[2 * ti + 1] = acc[1];
-    if (field && fld)
-        for (int a = 0; a < 3; ++a) {
-            fld[(ti * 3 + a) * 2] = acc[2 + 2 * a];
-            fld[(ti * 3 + a) * 2 + 1] = acc[3 + 2 * a];
-        }
+    const int64_t w = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (w >= n_t * NV) return;
+    const int64_t ti = w / NV;
+    const int v = (int)(w % NV);
+    if (!field && v >= 2) return;
+    double acc = 0.0;
+    for (int s = lane; s < n_split; s += 32) acc += scratch[((int64_t)s * n_t + ti) * NV + v];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane != 0) return;
+    if (v < 2) phi[2 * ti + v] = acc;
+    else if (fld) fld[(ti * 3 + (v - 2) / 2) * 2 + (v - 2) % 2] = acc;
 }
 
 }  // namespace
@@ -168,7 +173,7 @@ void direct_sum(const double* pos, const double* q_re, const double* q_im, int64
     dim3 grid((unsigned)ceil_div(n_t, DT), (unsigned)n_split);
     HFMM_LAUNCH(k_direct_partial, grid, DT, 0, s, pos, q_re, q_im, n, targets, n_t, k,
                 fld ? 1 : 0, n_split, scratch, err, yukawa);
-    HFMM_LAUNCH(k_direct_reduce, (unsigned)ceil_div(n_t, 256), 256, 0, s, scratch, n_t, n_split,
+    HFMM_LAUNCH(k_direct_reduce, (unsigned)ceil_div(n_t * NV * 32, 256), 256, 0, s, scratch, n_t, n_split,
                 fld ? 1 : 0, phi, fld);
 }
 

@@ -321,18 +321,28 @@ class AutoPlan:
                 t.record_stream(self._side)
         return self._ref_phi, (self._ref_E if field else None)
 
-    def _error(self, phi, E, ref):
-        """Relative L2 error at the check targets (potential, and field when computed);
-        waits for the side stream."""
+    def _error_async(self, phi, E, ref):
+        """The relative L2 error at the check targets (potential, and field when
+        computed) as a device scalar, enqueued behind the side stream's direct sum:
+        nothing waits on the host, so the GPU runs it right after the evaluate."""
         torch.cuda.current_stream(self.device).wait_stream(self._side)
-        if int(self._derr.item()):
-            raise RuntimeError("direct-sum check: a target index is out of range")
-        i = self._check_dev.long()
+        if getattr(self, "_check_long", None) is None:
+            self._check_long = self._check_dev.long()
+        i = self._check_long
         rel = lambda a, b: torch.linalg.norm(a - b) / torch.clamp(torch.linalg.norm(b), min=1e-300)
         err = rel(phi[i], ref[0])
         if E is not None:
             err = torch.maximum(err, rel(E[i], ref[1]))
+        return err
+
+    def _error_value(self, err):
+        if int(self._derr.item()):
+            raise RuntimeError("direct-sum check: a target index is out of range")
         return float(err.item())
+
+    def _error(self, phi, E, ref):
+        """Relative L2 error at the check targets; waits for the side stream."""
+        return self._error_value(self._error_async(phi, E, ref))
 
     def _raise_order(self, p):
         """Rebuild the plan at order ``p`` (same leaf size, the precision rule of p)."""
@@ -378,8 +388,9 @@ class AutoPlan:
             E = torch.empty((n, 3), dtype=torch.complex128, device=dev) if field else None
             ref = self._direct(q_re, q_im, field)
             evaluate_into(self.state, q_re, q_im, phi, E, self.precision)
+            err_t = self._error_async(phi, E, ref)   # enqueued before the first host wait
             check_errors(self.state)
-            err = self._error(phi, E, ref)
+            err = self._error_value(err_t)
             rep = dict(p=self.p, leaf=self.leaf, precision=int(self.precision), error=err,
                        fallback=False, p_final=self.p, network=self.network_used, raised=0)
             # a miss at the network's order: the next orders in the plan's own precision
