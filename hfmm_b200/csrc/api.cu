@@ -709,6 +709,14 @@ void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double*
             if (l >= 3)   // L2L (phases.py:273-278) in FP64, added to the check potential
                 gemm(K_L2L, l, P->dn_tiles[l][R - 1], P->m2l_src.p + N_DISP, M2L_ENTRIES, P->loc.p,
                      nullptr, P->check.p);
+        } else if (P->rot_P > 0) {   // rotation-based M2L (m2l_rotation.cu), then the L2L GEMM
+            {
+                PhaseTimer pt(X, s, 4);
+                rot_m2l(P, l, R, fs, s);
+            }
+            if (l >= 3)
+                gemm(K_L2L, l, P->dn_tiles[l][R - 1], P->m2l_src.p + N_DISP, M2L_ENTRIES, P->loc.p,
+                     nullptr, P->check.p);
         } else {
             gemm(K_DN, l, P->dn_tiles[l][R - 1], P->m2l_src.p, M2L_ENTRIES, P->equiv.p, P->loc.p,
                  P->check.p);

@@ -84,6 +84,10 @@ struct LevelTables {
     DevBuf<double> m2m;                 // 8 x (A^T) for this level as PARENT
     DevBuf<double> l2l;                 // 8 x (A^T) for this level as CHILD
     DevBuf<double> m2l;                 // 316 x (A^T), non-adjacent displacements
+    // rotation-based M2L (m2l_rotation.cu): multipole-from-equivalent Q, check-from-local
+    // E (complex, interleaved) and the coaxial shift matrices of every distance
+    DevBuf<double> rot_Q, rot_E, rot_C;
+    double rot_pref = 0.0;
     // mixed path: TF32 hi/lo halves of M2L and L2L as A[m][k] (fp32 containers)
     DevBuf<float> m2l_hi, m2l_lo, l2l_hi, l2l_lo;
     // compressed M2L of the mixed path, K_d ~ U C_d U^T (rank cr): the K side padded
@@ -111,6 +115,7 @@ struct LevelTables {
         m2l_hi.release(); m2l_lo.release(); l2l_hi.release(); l2l_lo.release();
         cr = ckld = cmld = 0;
         c_cmp.release(); c_exp.release(); c_hi.release(); c_lo.release();
+        rot_Q.release(); rot_E.release(); rot_C.release();
         xc.release(); yc.release(); xc_hi.release(); xc_lo.release();
         grid = 0;
         xg_hi.release(); xg_lo.release();
@@ -223,6 +228,10 @@ struct hfmm_plan {
     hfmm::DevBuf<double> q_s;        // R x n sorted charges
     hfmm::DevBuf<double> check, equiv, loc, tmp;   // [fam][box][R][ld]
     hfmm::DevBuf<double> gemm_part;  // partial tiles of the main stream's split GEMMs
+    int rot_P = 0, rot_n_dist = 0;   // rotation-based M2L of the FP64 evaluate (0: dense tables)
+    hfmm::DevBuf<double> rot_T;      // rotation blocks per displacement slot (complex)
+    hfmm::DevBuf<int32_t> rot_dist;  // coaxial matrix per slot
+    hfmm::DevBuf<double> rot_M;      // multipole work array of one level
     hfmm::DevBuf<double> pot;        // per sorted particle: [fam][R] potentials
     hfmm::DevBuf<double> fld;        // per sorted particle: [fam][R][3]
     hfmm::DevBuf<int> d_err;
@@ -287,6 +296,9 @@ struct GemmCall {
 };
 void gemm_f64(const GemmCall& c, int* d_err, cudaStream_t s);
 int sm_count();   // multiprocessors of the current device (read once)
+// rotation-based M2L of level l into the check potentials (m2l_rotation.cu)
+void rot_m2l(hfmm_plan* P, int l, int R, int64_t fam_stride, cudaStream_t s);
+size_t rot_workspace_doubles(const hfmm_plan* P);
 constexpr int64_t GEMM_PART_CAP = 768LL * 64 * 64;   // doubles: 768 partial 64 x 64 tiles
 
 // ---------------------------------------------------------------- device helpers

@@ -1,0 +1,238 @@
+"""Rotation-based M2L of the FP64 path: rotate, shift along z, rotate back.
+
+The reference's Helmholtz path translates with KIFMM operators only (kifmm/phases.py:
+176-237); its rotation-based M2L is Laplace's (kernels/laplace/transf.py:143-250,
+rotations kernels/laplace/rotation.py). This module builds the Helmholtz version of
+that scheme for the two kernel families, as an alternative to the dense M2L tables
+of the FP64 evaluate (``hfmm_plan_set_m2l_rotation``):
+
+* a box's equivalent density x (n_s points on its equivalent surface, radius
+  R_EQUIV x half side) becomes multipole coefficients about the box centre,
+  M_nm = sum_s x_s j_n(k |y_s|) conj(Y_nm(y_s)), n <= P (orthonormal complex Y);
+* per V pair with displacement d: rotate the coefficients into the frame where d is
+  the z axis (T_n, per degree), shift coaxially by |d| (one matrix per order m), rotate
+  back (T_n^H), accumulated over the target's V list;
+* the target's check potential is Re(pref sum L_nm j_n(k |c|) Y_nm(c)) at its check
+  points (the same unit point set, scaled), pref = -4 pi k for cos(kr)/r = -k y_0(kr)
+  and 4 pi k for sin(kr)/r = k j_0(kr).
+
+Coaxial coefficients (shift t along +z, multipole (n, m) -> local (n', m)), from the
+addition theorem with Gaunt integrals:
+    C^m_{n'n}(t) = 4 pi sum_nu i^(n'+nu-n) G(n' m; nu 0; n m) z_nu(k t) sqrt((2 nu+1)/(4 pi)),
+G = int Y_{n'm} Y_{nu 0} conj(Y_{nm}), z = y for the cos family (singular), j for
+the sin family (regular everywhere); i^(n'+nu-n) is real wherever G is nonzero.
+The formula is pinned against numerical projection in tests/test_rotation_cpu.py.
+Rotation blocks T_n[m, m''] = int Y_{nm''}(s) conj(Y_nm(R s)) d Omega are integrated
+exactly (Gauss-Legendre x uniform azimuth, enough points for degree 2P).
+
+Cost per V pair, family and charge column: two rotations of sum (2n+1)^2 and one
+coaxial shift of sum (P+1-|m|)^2 complex multiply-adds, O(P^3): at P = 20 about
+31,000, against n_s^2 = 87,616 multiply-adds of the dense p = 8 table. Accuracy is
+set by P: at p = 8 the nearest face displacement (2, 0, 0) converges slowest
+(relative 2.9e-6 at P = 20, 1.1e-6 at 24, 3.8e-7 at 28); the sin family is exact to
+rounding at any P used here.
+"""
+import math
+from fractions import Fraction
+from functools import lru_cache
+
+import numpy as np
+from numpy.polynomial.legendre import leggauss
+from scipy.special import sph_harm_y, spherical_jn, spherical_yn
+
+from .operators import surface_pts, level_scale, R_EQUIV
+
+__all__ = ["gaunt", "rotation_blocks", "coaxial", "level_operators", "direction_blocks",
+           "n_coeff", "pack_rotations", "pack_coaxial", "enable", "disable"]
+
+
+def n_coeff(P):
+    return (P + 1) * (P + 1)
+
+
+def _sph(v):
+    r = np.linalg.norm(v, axis=-1)
+    th = np.arccos(np.clip(v[..., 2] / np.where(r > 0, r, 1.0), -1.0, 1.0))
+    return r, th, np.arctan2(v[..., 1], v[..., 0])
+
+
+@lru_cache(maxsize=None)
+def _fact(n):
+    return math.factorial(n)
+
+
+def wigner_3j(j1, j2, j3, m1, m2, m3):
+    """The Wigner 3j symbol by the Racah formula in exact integer arithmetic."""
+    if m1 + m2 + m3 != 0 or j3 < abs(j1 - j2) or j3 > j1 + j2:
+        return 0.0
+    if abs(m1) > j1 or abs(m2) > j2 or abs(m3) > j3:
+        return 0.0
+    f = _fact
+    tri = Fraction(f(j1 + j2 - j3) * f(j1 - j2 + j3) * f(-j1 + j2 + j3), f(j1 + j2 + j3 + 1))
+    pre = tri * f(j1 + m1) * f(j1 - m1) * f(j2 + m2) * f(j2 - m2) * f(j3 + m3) * f(j3 - m3)
+    s = Fraction(0)
+    for k in range(0, j1 + j2 + j3 + 1):
+        a = (k, j3 - j2 + k + m1, j3 - j1 + k - m2, j1 + j2 - j3 - k, j1 - k - m1, j2 - k + m2)
+        if min(a) < 0:
+            continue
+        s += Fraction((-1) ** k, f(a[0]) * f(a[1]) * f(a[2]) * f(a[3]) * f(a[4]) * f(a[5]))
+    sign = -1.0 if (j1 - j2 - m3) % 2 else 1.0
+    # sqrt(pre) * s with pre, s exact: the product's square is exact, its sign is s's
+    val = math.sqrt(pre * s * s)
+    return sign * (val if s >= 0 else -val)
+
+
+def gaunt(l1, m1, l2, m2, l3, m3):
+    """int Y_{l1 m1} Y_{l2 m2} Y_{l3 m3} dOmega (orthonormal complex harmonics)."""
+    if (l1 + l2 + l3) % 2:
+        return 0.0
+    return (math.sqrt((2 * l1 + 1) * (2 * l2 + 1) * (2 * l3 + 1) / (4 * math.pi))
+            * wigner_3j(l1, l2, l3, 0, 0, 0) * wigner_3j(l1, l2, l3, m1, m2, m3))
+
+
+@lru_cache(maxsize=None)
+def _coax_table(P):
+    """W[m + P, n', n, nu] = 4 pi i^(n'+nu-n) G(n' m; nu 0; n m) sqrt((2 nu+1)/(4 pi)) (real)."""
+    W = np.zeros((2 * P + 1, P + 1, P + 1, 2 * P + 1))
+    for m in range(-P, P + 1):
+        for n2 in range(abs(m), P + 1):
+            for n in range(abs(m), P + 1):
+                for nu in range(abs(n - n2), n + n2 + 1, 2):
+                    g = gaunt(n2, m, nu, 0, n, -m) * (-1) ** (m % 2)
+                    if g == 0.0:
+                        continue
+                    e = (n2 + nu - n) % 4   # i^e: 0 -> 1, 2 -> -1 (odd e has g = 0)
+                    W[m + P, n2, n, nu] = (1.0 if e == 0 else -1.0) * 4 * math.pi * g * \
+                        math.sqrt((2 * nu + 1) / (4 * math.pi))
+    return W
+
+
+def coaxial(P, k, t, regular):
+    """C[m + P] ((P+1) x (P+1), real): local (n', m) from multipole (n, m) for a shift t
+    along +z; rows and columns below |m| are zero."""
+    z = spherical_jn if regular else spherical_yn
+    zs = np.array([z(nu, k * t) for nu in range(2 * P + 1)])
+    return np.einsum("mabn,n->mab", _coax_table(P), zs)
+
+
+def rotation_blocks(P, R):
+    """T_n ((2n+1) x (2n+1) complex) for n <= P: coefficients in the frame R maps to."""
+    nq = P + 2
+    x, w = leggauss(nq)
+    th = np.arccos(x)
+    ph = np.linspace(0, 2 * np.pi, 2 * nq + 1, endpoint=False)
+    TH, PH = np.meshgrid(th, ph, indexing="ij")
+    W = np.outer(w, np.full(len(ph), 2 * np.pi / len(ph))).ravel()
+    S = np.stack([np.sin(TH) * np.cos(PH), np.sin(TH) * np.sin(PH), np.cos(TH)], -1).reshape(-1, 3)
+    _, t1, p1 = _sph(S)
+    _, t2, p2 = _sph(S @ R.T)
+    out = []
+    for n in range(P + 1):
+        A = np.stack([sph_harm_y(n, m, t1, p1) for m in range(-n, n + 1)])
+        B = np.stack([sph_harm_y(n, m, t2, p2) for m in range(-n, n + 1)])
+        out.append((np.conj(B) * W) @ A.T)
+    return out
+
+
+def rotation_to_z(d):
+    """A proper rotation R with R d / |d| = z."""
+    u = np.asarray(d, float) / np.linalg.norm(d)
+    z = np.array([0.0, 0.0, 1.0])
+    v = np.cross(u, z)
+    c, s = float(u @ z), float(np.linalg.norm(v))
+    if s < 1e-14:
+        return np.eye(3) if c > 0 else np.diag([1.0, -1.0, -1.0])
+    vx = np.array([[0, -v[2], v[1]], [v[2], 0, -v[0]], [-v[1], v[0], 0]])
+    return np.eye(3) + vx + vx @ vx * ((1 - c) / s ** 2)
+
+
+def displacements():
+    """The 343 displacement slots (dx, dy, dz) in [-3, 3]^3, (dx+3)*49 + (dy+3)*7 + (dz+3)."""
+    return np.array([(i // 49 - 3, (i // 7) % 7 - 3, i % 7 - 3) for i in range(343)], float)
+
+
+def direction_blocks(P):
+    """Rotation blocks of every non-adjacent slot (None for the others); the slot's
+    displacement d = target - source (the source's multipole is shifted by d)."""
+    out = []
+    for d in displacements():
+        out.append(rotation_blocks(P, rotation_to_z(d)) if np.abs(d).max() > 1 else None)
+    return out
+
+
+def pack_rotations(P, blocks):
+    """[343][sum (2n+1)^2] complex128 as interleaved re, im (zeros for adjacent slots)."""
+    size = sum((2 * n + 1) ** 2 for n in range(P + 1))
+    out = np.zeros((343, size), np.complex128)
+    for e, T in enumerate(blocks):
+        if T is None:
+            continue
+        out[e] = np.concatenate([t.ravel() for t in T])
+    return out
+
+
+def distances():
+    """Distinct |d|^2 of the non-adjacent slots (sorted) and each slot's index (-1: adjacent)."""
+    d = displacements()
+    d2 = (d * d).sum(1).astype(int)
+    far = np.abs(d).max(1) > 1
+    uniq = np.unique(d2[far])
+    slot = np.where(far, np.searchsorted(uniq, d2), -1).astype(np.int32)
+    return uniq, slot
+
+
+def pack_coaxial(P, k, s, regular):
+    """[n_dist][2P+1][P+1][P+1] real: the coaxial matrices of a level (half side s; a slot's
+    shift is 2 s |d|)."""
+    uniq, _ = distances()
+    return np.stack([coaxial(P, k, 2 * s * math.sqrt(d2), regular) for d2 in uniq])
+
+
+def level_operators(p, level, extent, k, imaginary, P):
+    """(Q, E, pref) of one level and family: Q ((P+1)^2 x n_s complex) makes multipole
+    coefficients from an equivalent density, E (n_s x (P+1)^2 complex) check potentials
+    (times pref, real part) from local coefficients."""
+    s = level_scale(extent, level)
+    eq = surface_pts(p, R_EQUIV) * s
+    r, th, ph = _sph(eq)
+    Ys = np.stack([sph_harm_y(n, m, th, ph) for n in range(P + 1) for m in range(-n, n + 1)])
+    Jn = np.stack([spherical_jn(n, k * r) for n in range(P + 1) for m in range(-n, n + 1)])
+    Q = np.conj(Ys) * Jn
+    E = (Ys * Jn).T
+    pref = 4 * math.pi * k * (1.0 if imaginary else -1.0)
+    return Q, E, pref
+
+
+def enable(state, order):
+    """Switch a plan's FP64 evaluate to the rotation-based M2L of ``order`` P (the
+    Helmholtz kernel; the dense tables stay in the plan for the other paths). Builds
+    the operators on the host (the coaxial coefficients' Gaunt table once per order,
+    about 20 s at P = 20) and uploads them."""
+    from . import _lib
+    from ._lib import check
+    if getattr(state, "kind", "helmholtz") != "helmholtz":
+        raise ValueError("the rotation-based M2L is built for the Helmholtz kernel")
+    P = int(order)
+    T = np.ascontiguousarray(pack_rotations(P, direction_blocks(P)))
+    uniq, slot = distances()
+    slot = np.ascontiguousarray(slot, np.int32)
+    check(_lib.lib.hfmm_plan_set_m2l_rotation(state.handle, P, T.ctypes.data, slot.ctypes.data,
+                                               len(uniq)))
+    extent = state.info["domain_extent"]
+    for fam in range(state.n_families):
+        for level in range(2, state.max_depth + 1):
+            Q, E, pref = level_operators(state.p, level, extent, state.k, fam == 1, P)
+            C = np.ascontiguousarray(pack_coaxial(P, state.k, level_scale(extent, level), fam == 1))
+            Q = np.ascontiguousarray(Q.astype(np.complex128))
+            E = np.ascontiguousarray(E.astype(np.complex128))
+            check(_lib.lib.hfmm_plan_set_rotation_level(state.handle, fam, level, Q.ctypes.data,
+                                                         E.ctypes.data, C.ctypes.data, float(pref)))
+    state.rotation_order = P
+
+
+def disable(state):
+    """Back to the dense M2L tables."""
+    from . import _lib
+    from ._lib import check
+    check(_lib.lib.hfmm_plan_set_m2l_rotation(state.handle, 0, None, None, 0))
+    state.rotation_order = 0

@@ -316,6 +316,24 @@ int hfmm_batch_set_queue(hfmm_batch* batch, int32_t on);
  * finalize; on == 0 launches one kernel per level and family on the plan's side
  * streams. Results are the same bit for bit. */
 int hfmm_plan_set_m2l_queue(hfmm_plan* plan, int32_t on);
+
+/* Rotation-based M2L of the FP64 evaluate (the reference's rotation M2L is Laplace's,
+ * kernels/laplace/transf.py:143-250; its Helmholtz path uses KIFMM tables,
+ * kifmm/phases.py:176-237): per V pair, the source box's multipole coefficients of
+ * order `order` are rotated into the frame whose z axis is the displacement, shifted
+ * along z and rotated back, O(order^3). T_host: [343][sum_{n<=order} (2n+1)^2] complex
+ * (re, im interleaved) rotation blocks per displacement slot ((dx+3)*49 + (dy+3)*7 +
+ * (dz+3)), zero for adjacent slots; dist_host[343]: each slot's coaxial matrix index
+ * (-1 adjacent), n_dist of them. order 0 returns to the dense M2L tables. Then, per
+ * family and level, hfmm_plan_set_rotation_level with Q [(order+1)^2][n_s] complex
+ * (multipole from equivalent density), E [n_s][(order+1)^2] complex (check potential
+ * from local coefficients, times pref, real part) and C [n_dist][2 order+1][order+1]
+ * [order+1] real (the coaxial shifts). hfmm_b200/rotation.py builds all of them. Only the
+ * FP64 evaluate uses it; after hfmm_plan_rebuild set it again. */
+int hfmm_plan_set_m2l_rotation(hfmm_plan* plan, int32_t order, const double* T_host,
+                               const int32_t* dist_host, int32_t n_dist);
+int hfmm_plan_set_rotation_level(hfmm_plan* plan, int32_t family, int32_t level, const double* Q_host,
+                                 const double* E_host, const double* C_host, double pref);
 int hfmm_batch_queued(const hfmm_batch* batch);
 const char* hfmm_batch_queue_note(const hfmm_batch* batch);
 
