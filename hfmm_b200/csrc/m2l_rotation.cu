@@ -4,18 +4,22 @@
 // operators, kifmm/phases.py:176-237; its rotation M2L is Laplace's,
 // kernels/laplace/transf.py:143-250). Per level and kernel family:
 //   1. k_rot_multipole: multipole coefficients of every box of the level from its
-//      equivalent density, M[b][r] = Q x[b][r] (Q: (P+1)^2 x n_s complex);
-//   2. k_rot_m2l: one CTA per target box walks its V list; per source it rotates the
-//      source's coefficients into the frame whose z axis is the displacement (T_n per
+//      equivalent density, M[b][r] = Q x[b][r] (Q: (P+1)^2 x n_s complex), a tile of
+//      boxes per CTA so that each row of Q is read once per tile;
+//   2. k_rot_m2l: a CTA owns a tile of target boxes (TT targets x R charge columns,
+//      at most 16 columns) and walks the 343 displacement slots in order. Per slot it
+//      gathers the tile's sources' coefficients (zero where a target has no source
+//      there), rotates them into the frame whose z axis is the displacement (T_n per
 //      degree n, (2n+1)^2 complex), shifts them coaxially by |d| (one real
-//      (P+1-|m|)^2 matrix per order m), rotates the result back (T_n^H) and adds it to
-//      the target's local coefficients in shared memory; at the end the target's
-//      check potential is Re(pref E L) (E: n_s x (P+1)^2 complex), which the L2L GEMM
-//      and the decode then use as in the dense path.
+//      (P+1-|m|)^2 matrix per order m) and rotates the result back (T_n^H) into the
+//      targets' local coefficients, which stay in registers. The slot's tables are
+//      read once per tile instead of once per pair. At the end the targets' check
+//      potentials are Re(pref E L) (E: n_s x (P+1)^2 complex), which the L2L GEMM and
+//      the decode then use as in the dense path.
 // The operators are built on the host in FP64 (hfmm_b200/rotation.py) and uploaded by
-// hfmm_plan_set_m2l_rotation / hfmm_plan_set_rotation_level. Every stage is O(P^3)
-// per pair. Accumulation order is fixed (V entries in slot order), so results are
-// deterministic.
+// hfmm_plan_set_m2l_rotation / hfmm_plan_set_rotation_level (Q and E transposed on
+// upload, for reads coalesced over the thread index). Every stage is O(P^3) per
+// pair. Each target sums its slots in slot order, so results are deterministic.
 #include "hfmm_internal.cuh"
 
 #include <algorithm>
@@ -25,135 +29,191 @@ namespace hfmm {
 
 namespace {
 
+constexpr int ROT_THREADS = 512;
+constexpr int ROT_MAXI = 12;     // stage items per thread: (P+1)^2 x columns <= 6144
+constexpr int ROT_MAXCOL = 16;   // charge columns (targets x R) per CTA
+constexpr int ROT_MP_THREADS = 256;
+
 struct RotCall {
     const double2* T;          // [343][TS] rotation blocks per displacement slot
     const int32_t* dist;       // [343] coaxial matrix index (-1: adjacent slot)
-    const double2* Q;          // [NC][n_s]
-    const double2* E;          // [n_s][NC]
+    const double2* QT;         // [n_s][NC]
+    const double2* ET;         // [NC][n_s]
     const double* C;           // [n_dist][2P+1][P+1][P+1]
     const int32_t* src_tab;    // [nb][351]
     const double* equiv;       // family base of the equivalent densities [nb][R][ld]
     double* check;             // family base of the check potentials [nb][R][ld]
     double2* M;                // work: [hi - lo][R][NC]
     double pref;
-    int P, NC, TS, n_s, ld, R;
-    int64_t lo, hi, nb;
+    int P, NC, TS, n_s, ld, R, TT;
+    int64_t lo, hi;
     int* err;
 };
 
 __device__ __forceinline__ int tri_off(int n) { return n * (4 * n * n - 1) / 3; }   // sum (2k+1)^2, k < n
+__device__ __forceinline__ int deg_of(int q) { return (int)sqrtf((float)q + 0.5f); }  // q = n^2 + n + m
 
-__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
-    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+__device__ __forceinline__ void cmac(double2& acc, double2 a, double2 b) {   // acc += a b
+    acc.x = fma(a.x, b.x, acc.x);
+    acc.x = fma(-a.y, b.y, acc.x);
+    acc.y = fma(a.x, b.y, acc.y);
+    acc.y = fma(a.y, b.x, acc.y);
 }
-__device__ __forceinline__ double2 cmulc(double2 a, double2 b) {   // conj(a) b
-    return make_double2(a.x * b.x + a.y * b.y, a.x * b.y - a.y * b.x);
+__device__ __forceinline__ void cmacc(double2& acc, double2 a, double2 b) {  // acc += conj(a) b
+    acc.x = fma(a.x, b.x, acc.x);
+    acc.x = fma(a.y, b.y, acc.x);
+    acc.y = fma(a.x, b.y, acc.y);
+    acc.y = fma(-a.y, b.x, acc.y);
 }
 
-__global__ void __launch_bounds__(256) k_rot_multipole(RotCall c) {
-    extern __shared__ double xs[];   // [R][n_s]
-    const int64_t b = c.lo + blockIdx.x;
-    for (int i = threadIdx.x; i < c.R * c.n_s; i += blockDim.x) {
-        const int r = i / c.n_s, s = i % c.n_s;
-        xs[i] = c.equiv[(b * c.R + r) * c.ld + s];
+// M[b][r][q] = sum_s Q[q][s] x[b][r][s] for a tile of TT boxes (TT R <= ROT_MAXCOL).
+__global__ void __launch_bounds__(ROT_MP_THREADS) k_rot_multipole(RotCall c) {
+    extern __shared__ double xs[];   // [TT R][n_s]
+    const int64_t b0 = c.lo + (int64_t)blockIdx.x * c.TT;
+    const int nt = (int)min((int64_t)c.TT, c.hi - b0);
+    const int ncol = nt * c.R;
+    for (int i = threadIdx.x; i < ncol * c.n_s; i += blockDim.x) {
+        const int cc = i / c.n_s, s = i - cc * c.n_s;
+        xs[i] = c.equiv[(b0 * c.R + cc) * c.ld + s];   // column cc = tt R + r of box b0 + tt
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < c.R * c.NC; i += blockDim.x) {
-        const int r = i / c.NC, q = i % c.NC;
-        const double2* qr = c.Q + (int64_t)q * c.n_s;
-        const double* x = xs + r * c.n_s;
-        double2 acc = make_double2(0.0, 0.0);
+    for (int q = threadIdx.x; q < c.NC; q += blockDim.x) {
+        double2 acc[ROT_MAXCOL];
+#pragma unroll
+        for (int cc = 0; cc < ROT_MAXCOL; ++cc) acc[cc] = make_double2(0.0, 0.0);
         for (int s = 0; s < c.n_s; ++s) {
-            const double2 w = qr[s];
-            acc.x += w.x * x[s];
-            acc.y += w.y * x[s];
+            const double2 w = __ldg(c.QT + (int64_t)s * c.NC + q);
+#pragma unroll
+            for (int cc = 0; cc < ROT_MAXCOL; ++cc)
+                if (cc < ncol) {
+                    const double x = xs[cc * c.n_s + s];
+                    acc[cc].x = fma(w.x, x, acc[cc].x);
+                    acc[cc].y = fma(w.y, x, acc[cc].y);
+                }
         }
-        c.M[((int64_t)blockIdx.x * c.R + r) * c.NC + q] = acc;
+#pragma unroll
+        for (int cc = 0; cc < ROT_MAXCOL; ++cc)
+            if (cc < ncol) c.M[((b0 - c.lo) * c.R + cc) * c.NC + q] = acc[cc];
     }
 }
 
-__global__ void __launch_bounds__(256) k_rot_m2l(RotCall c) {
+__global__ void __launch_bounds__(ROT_THREADS) k_rot_m2l(RotCall c) {
     extern __shared__ double2 sm[];
-    double2* A = sm;                    // [R][NC] source coefficients, then the shifted ones
-    double2* B = sm + c.R * c.NC;       // [R][NC] rotated
-    double2* L = sm + 2 * c.R * c.NC;   // [R][NC] the target's local coefficients
-    const int64_t t = c.lo + blockIdx.x;
-    const int RN = c.R * c.NC, P = c.P;
-    for (int i = threadIdx.x; i < RN; i += blockDim.x) L[i] = make_double2(0.0, 0.0);
+    __shared__ int32_t src[ROT_MAXCOL];
+    const int NC = c.NC, NCOL = c.TT * c.R, NI = NC * NCOL, P = c.P;
+    double2* X = sm;        // [NC][NCOL] gathered source coefficients, then the shifted ones
+    double2* Y = sm + NI;   // [NC][NCOL] rotated
+    const int64_t t0 = c.lo + (int64_t)blockIdx.x * c.TT;
+    const int nt = (int)min((int64_t)c.TT, c.hi - t0);
+    double2 L[ROT_MAXI];    // the tile's local coefficients, item i = threadIdx.x + k ROT_THREADS
+#pragma unroll
+    for (int k = 0; k < ROT_MAXI; ++k) L[k] = make_double2(0.0, 0.0);
     for (int e = 0; e < N_DISP; ++e) {
         const int di = c.dist[e];
-        if (di < 0) continue;
-        const int s_ = c.src_tab[t * M2L_ENTRIES + e];
-        if (s_ < 0) continue;
-        if (s_ < c.lo || s_ >= c.hi) {   // sources share the target's level
-            if (threadIdx.x == 0) atomicOr(c.err, ERRF_BOUNDS);
-            continue;
-        }
-        __syncthreads();   // the previous entry's last stage has read A
-        const double2* Ms = c.M + (int64_t)(s_ - c.lo) * RN;
-        for (int i = threadIdx.x; i < RN; i += blockDim.x) A[i] = Ms[i];
-        __syncthreads();
-        const double2* T = c.T + (int64_t)e * c.TS;
-        // rotate: B[(n, m)] = sum_m'' T_n[m][m''] A[(n, m'')]
-        for (int i = threadIdx.x; i < RN; i += blockDim.x) {
-            const int r = i / c.NC, q = i % c.NC;
-            const int n = (int)sqrtf((float)q + 0.5f), m = q - n * n - n;
-            const double2* Tn = T + tri_off(n) + (m + n) * (2 * n + 1);
-            const double2* a = A + r * c.NC + n * n;
-            double2 acc = make_double2(0.0, 0.0);
-            for (int j = 0; j <= 2 * n; ++j) {
-                const double2 p = cmul(Tn[j], a[j]);
-                acc.x += p.x;
-                acc.y += p.y;
+        if (di < 0) continue;   // adjacent slot: no V pair
+        __syncthreads();        // the previous slot's last stage has read X and src
+        if (threadIdx.x < c.TT) {
+            int sb = -1;
+            if (threadIdx.x < nt) {
+                sb = c.src_tab[(t0 + threadIdx.x) * M2L_ENTRIES + e];
+                if (sb >= 0 && (sb < c.lo || sb >= c.hi)) {   // sources share the target's level
+                    atomicOr(c.err, ERRF_BOUNDS);
+                    sb = -1;
+                }
             }
-            B[i] = acc;
+            src[threadIdx.x] = sb < 0 ? -1 : (int)(sb - c.lo);
         }
         __syncthreads();
-        // shift along z: A[(n', m)] = sum_{n >= |m|} C[m][n'][n] B[(n, m)]
-        const double* Cd = c.C + (int64_t)di * (2 * P + 1) * (P + 1) * (P + 1);
-        for (int i = threadIdx.x; i < RN; i += blockDim.x) {
-            const int r = i / c.NC, q = i % c.NC;
-            const int n2 = (int)sqrtf((float)q + 0.5f), m = q - n2 * n2 - n2;
-            const int am = m < 0 ? -m : m;
-            const double* Cm = Cd + ((int64_t)(m + P) * (P + 1) + n2) * (P + 1);
-            const double2* b = B + r * c.NC;
-            double2 acc = make_double2(0.0, 0.0);
-            for (int n = am; n <= P; ++n) {
-                const double w = Cm[n];
-                const double2 v = b[n * n + n + m];
-                acc.x += w * v.x;
-                acc.y += w * v.y;
-            }
-            A[i] = acc;
+        bool any = false;
+        for (int tt = 0; tt < nt; ++tt) any |= src[tt] >= 0;
+        if (!any) continue;     // the same answer for every thread of the CTA
+        for (int i = threadIdx.x; i < NI; i += ROT_THREADS) {   // coalesced over q
+            const int cc = i / NC, q = i - cc * NC;
+            const int tt = cc / c.R, r = cc - tt * c.R;
+            const int sb = src[tt];
+            X[q * NCOL + cc] = sb >= 0 ? c.M[((int64_t)sb * c.R + r) * NC + q] : make_double2(0.0, 0.0);
         }
         __syncthreads();
-        // rotate back and accumulate: L[(n, m'')] += sum_m conj(T_n[m][m'']) A[(n, m)]
-        for (int i = threadIdx.x; i < RN; i += blockDim.x) {
-            const int r = i / c.NC, q = i % c.NC;
-            const int n = (int)sqrtf((float)q + 0.5f), mm = q - n * n - n;
-            const double2* Tn = T + tri_off(n) + (mm + n);
-            const double2* a = A + r * c.NC + n * n;
-            double2 acc = L[i];
-            for (int j = 0; j <= 2 * n; ++j) {
-                const double2 p = cmulc(Tn[j * (2 * n + 1)], a[j]);
-                acc.x += p.x;
-                acc.y += p.y;
+        const double2* __restrict__ T = c.T + (int64_t)e * c.TS;
+        // rotate: Y[(n, m)] = sum_j T_n[m][j] X[(n, j - n)]
+#pragma unroll
+        for (int k = 0; k < ROT_MAXI; ++k) {
+            const int i = threadIdx.x + k * ROT_THREADS;
+            if (i < NI) {
+                const int q = i / NCOL, cc = i - q * NCOL;
+                const int n = deg_of(q), m = q - n * n - n;
+                const double2* Tn = T + tri_off(n) + (m + n) * (2 * n + 1);
+                const double2* x = X + n * n * NCOL + cc;
+                double2 acc = make_double2(0.0, 0.0);
+                for (int j = 0; j <= 2 * n; ++j) cmac(acc, __ldg(Tn + j), x[j * NCOL]);
+                Y[i] = acc;
             }
-            L[i] = acc;
+        }
+        __syncthreads();
+        // shift along z: X[(n', m)] = sum_{n >= |m|} C[m][n'][n] Y[(n, m)]
+        const double* __restrict__ Cd = c.C + (int64_t)di * (2 * P + 1) * (P + 1) * (P + 1);
+#pragma unroll
+        for (int k = 0; k < ROT_MAXI; ++k) {
+            const int i = threadIdx.x + k * ROT_THREADS;
+            if (i < NI) {
+                const int q = i / NCOL, cc = i - q * NCOL;
+                const int n2 = deg_of(q), m = q - n2 * n2 - n2;
+                const int am = m < 0 ? -m : m;
+                const double* Cm = Cd + ((int64_t)(m + P) * (P + 1) + n2) * (P + 1);
+                const double2* y = Y + cc;
+                double2 acc = make_double2(0.0, 0.0);
+                for (int n = am; n <= P; ++n) {
+                    const double w = __ldg(Cm + n);
+                    const double2 v = y[(n * n + n + m) * NCOL];
+                    acc.x = fma(w, v.x, acc.x);
+                    acc.y = fma(w, v.y, acc.y);
+                }
+                X[i] = acc;
+            }
+        }
+        __syncthreads();
+        // rotate back and accumulate: L[(n, m)] += sum_j conj(T_n[j][m]) X[(n, j - n)]
+#pragma unroll
+        for (int k = 0; k < ROT_MAXI; ++k) {
+            const int i = threadIdx.x + k * ROT_THREADS;
+            if (i < NI) {
+                const int q = i / NCOL, cc = i - q * NCOL;
+                const int n = deg_of(q), m = q - n * n - n;
+                const double2* Tn = T + tri_off(n) + (m + n);
+                const double2* x = X + n * n * NCOL + cc;
+                double2 acc = L[k];
+                for (int j = 0; j <= 2 * n; ++j) cmacc(acc, __ldg(Tn + j * (2 * n + 1)), x[j * NCOL]);
+                L[k] = acc;
+            }
         }
     }
     __syncthreads();
-    // the check potential at the target's check points: Re(pref E L), padding zeroed
-    for (int i = threadIdx.x; i < c.R * c.ld; i += blockDim.x) {
-        const int r = i / c.ld, j = i % c.ld;
-        double v = 0.0;
-        if (j < c.n_s) {
-            const double2* Ej = c.E + (int64_t)j * c.NC;
-            const double2* l = L + r * c.NC;
-            for (int q = 0; q < c.NC; ++q) v += Ej[q].x * l[q].x - Ej[q].y * l[q].y;
-            v *= c.pref;
-        }
-        c.check[(t * c.R + r) * c.ld + j] = v;
+#pragma unroll
+    for (int k = 0; k < ROT_MAXI; ++k) {
+        const int i = threadIdx.x + k * ROT_THREADS;
+        if (i < NI) X[i] = L[k];
+    }
+    __syncthreads();
+    // the check potentials at the targets' check points: Re(pref E L), padding zeroed
+    const int ncol = nt * c.R;
+    for (int j = threadIdx.x; j < c.ld; j += ROT_THREADS) {
+        double acc[ROT_MAXCOL];
+#pragma unroll
+        for (int cc = 0; cc < ROT_MAXCOL; ++cc) acc[cc] = 0.0;
+        if (j < c.n_s)
+            for (int q = 0; q < NC; ++q) {
+                const double2 w = __ldg(c.ET + (int64_t)q * c.n_s + j);
+                const double2* l = X + q * NCOL;
+#pragma unroll
+                for (int cc = 0; cc < ROT_MAXCOL; ++cc)
+                    if (cc < ncol) {
+                        acc[cc] = fma(w.x, l[cc].x, acc[cc]);
+                        acc[cc] = fma(-w.y, l[cc].y, acc[cc]);
+                    }
+            }
+#pragma unroll
+        for (int cc = 0; cc < ROT_MAXCOL; ++cc)
+            if (cc < ncol) c.check[(t0 * c.R + cc) * c.ld + j] = c.pref * acc[cc];
     }
 }
 
@@ -169,14 +229,17 @@ void rot_m2l(hfmm_plan* P, int l, int R, int64_t fam_stride, cudaStream_t s) {
     const int Pn = P->rot_P, NC = (Pn + 1) * (Pn + 1);
     if (P->rot_M.n < rot_workspace_doubles(P))   // a rebuilt tree with a wider level
         throw Error{HFMM_ERR_STATE, "rotation M2L: set the rotation again after the plan was rebuilt"};
+    // targets per CTA: at most ROT_MAXCOL charge columns and ROT_MAXI items per thread
+    const int TT = std::min(ROT_MAXCOL / R, ROT_THREADS * ROT_MAXI / (NC * R));
+    if (TT < 1) throw Error{HFMM_ERR_ARG, "rotation M2L: order too high for one CTA"};
     for (int f = 0; f < P->n_fam; ++f) {
         LevelTables& T = P->tables[f][l];
         if (!T.rot_Q.p) throw Error{HFMM_ERR_STATE, "rotation M2L: level operators missing"};
         RotCall c{};
         c.T = reinterpret_cast<const double2*>(P->rot_T.p);
         c.dist = P->rot_dist.p;
-        c.Q = reinterpret_cast<const double2*>(T.rot_Q.p);
-        c.E = reinterpret_cast<const double2*>(T.rot_E.p);
+        c.QT = reinterpret_cast<const double2*>(T.rot_Q.p);
+        c.ET = reinterpret_cast<const double2*>(T.rot_E.p);
         c.C = T.rot_C.p;
         c.src_tab = P->m2l_src.p;
         c.equiv = P->equiv.p + f * fam_stride;
@@ -185,20 +248,24 @@ void rot_m2l(hfmm_plan* P, int l, int R, int64_t fam_stride, cudaStream_t s) {
         c.pref = T.rot_pref;
         c.P = Pn;
         c.NC = NC;
-        c.TS = Pn >= 0 ? (Pn + 1) * (4 * (Pn + 1) * (Pn + 1) - 1) / 3 : 0;
+        c.TS = (Pn + 1) * (4 * (Pn + 1) * (Pn + 1) - 1) / 3;
         c.n_s = P->n_s;
         c.ld = P->ld;
         c.R = R;
         c.lo = P->level_lo[l];
         c.hi = P->level_hi[l];
-        c.nb = P->nb;
         c.err = P->d_err.p;
-        const unsigned nbl = (unsigned)(c.hi - c.lo);
+        const int64_t nbl = c.hi - c.lo;
         if (nbl == 0) continue;
-        HFMM_LAUNCH(k_rot_multipole, nbl, 256, (size_t)R * P->n_s * sizeof(double), s, c);
-        const size_t smem = (size_t)3 * R * NC * sizeof(double2);
+        c.TT = ROT_MAXCOL / R;
+        const size_t smem_mp = (size_t)c.TT * R * P->n_s * sizeof(double);
+        HFMM_CUDA(cudaFuncSetAttribute(k_rot_multipole, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem_mp));
+        HFMM_LAUNCH(k_rot_multipole, (unsigned)ceil_div(nbl, (int64_t)c.TT), ROT_MP_THREADS, smem_mp, s, c);
+        c.TT = TT;
+        const size_t smem = (size_t)2 * NC * TT * R * sizeof(double2);
         HFMM_CUDA(cudaFuncSetAttribute(k_rot_m2l, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        HFMM_LAUNCH(k_rot_m2l, nbl, 256, smem, s, c);
+        HFMM_LAUNCH(k_rot_m2l, (unsigned)ceil_div(nbl, (int64_t)TT), ROT_THREADS, smem, s, c);
     }
 }
 
@@ -252,11 +319,20 @@ int hfmm_plan_set_rotation_level(hfmm_plan* P, int32_t family, int32_t level, co
         const size_t NC = (size_t)(P->rot_P + 1) * (P->rot_P + 1);
         const size_t nc = (size_t)P->rot_n_dist * (2 * P->rot_P + 1) * (P->rot_P + 1) * (P->rot_P + 1);
         LevelTables& T = P->tables[family][level];
-        T.rot_Q.alloc(NC * P->n_s * 2);
-        T.rot_E.alloc(NC * P->n_s * 2);
+        const size_t ns = (size_t)P->n_s;
+        // stored transposed: Q^T [n_s][NC] and E^T [NC][n_s] (complex as re, im pairs)
+        std::vector<double> qt(NC * ns * 2), et(NC * ns * 2);
+        for (size_t q = 0; q < NC; ++q)
+            for (size_t j = 0; j < ns; ++j)
+                for (int z = 0; z < 2; ++z) {
+                    qt[(j * NC + q) * 2 + z] = Q_host[(q * ns + j) * 2 + z];
+                    et[(q * ns + j) * 2 + z] = E_host[(j * NC + q) * 2 + z];
+                }
+        T.rot_Q.alloc(NC * ns * 2);
+        T.rot_E.alloc(NC * ns * 2);
         T.rot_C.alloc(nc);
-        HFMM_CUDA(cudaMemcpy(T.rot_Q.p, Q_host, NC * P->n_s * 2 * sizeof(double), cudaMemcpyHostToDevice));
-        HFMM_CUDA(cudaMemcpy(T.rot_E.p, E_host, NC * P->n_s * 2 * sizeof(double), cudaMemcpyHostToDevice));
+        HFMM_CUDA(cudaMemcpy(T.rot_Q.p, qt.data(), NC * ns * 2 * sizeof(double), cudaMemcpyHostToDevice));
+        HFMM_CUDA(cudaMemcpy(T.rot_E.p, et.data(), NC * ns * 2 * sizeof(double), cudaMemcpyHostToDevice));
         HFMM_CUDA(cudaMemcpy(T.rot_C.p, C_host, nc * sizeof(double), cudaMemcpyHostToDevice));
         T.rot_pref = pref;
         return HFMM_OK;

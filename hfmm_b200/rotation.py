@@ -38,7 +38,7 @@ from functools import lru_cache
 
 import numpy as np
 from numpy.polynomial.legendre import leggauss
-from scipy.special import sph_harm_y, spherical_jn, spherical_yn
+from scipy.special import spherical_jn, spherical_yn
 
 from .operators import surface_pts, level_scale, R_EQUIV
 
@@ -61,6 +61,7 @@ def _fact(n):
     return math.factorial(n)
 
 
+@lru_cache(maxsize=None)
 def wigner_3j(j1, j2, j3, m1, m2, m3):
     """The Wigner 3j symbol by the Racah formula in exact integer arithmetic."""
     if m1 + m2 + m3 != 0 or j3 < abs(j1 - j2) or j3 > j1 + j2:
@@ -115,8 +116,41 @@ def coaxial(P, k, t, regular):
     return np.einsum("mabn,n->mab", _coax_table(P), zs)
 
 
-def rotation_blocks(P, R):
-    """T_n ((2n+1) x (2n+1) complex) for n <= P: coefficients in the frame R maps to."""
+def _harmonics(P, th, ph):
+    """Y_nm (orthonormal, Condon-Shortley phase) at the given angles for every n <= P,
+    m = -n..n, rows in (n, m) order. Column recurrence of the normalised associated
+    Legendre functions, P~_mm = -sqrt((2m+1)/(2m)) sin(th) P~_(m-1)(m-1),
+    P~_(m+1)m = sqrt(2m+3) cos(th) P~_mm, then
+    P~_nm = a (cos(th) P~_(n-1)m - b P~_(n-2)m), a = sqrt((4n^2-1)/(n^2-m^2)),
+    b = sqrt(((n-1)^2-m^2)/(4(n-1)^2-1)); Y_n(-m) = (-1)^m conj(Y_nm)."""
+    th, ph = np.ravel(th), np.ravel(ph)
+    x, s = np.cos(th), np.sin(th)
+    out = np.empty(((P + 1) ** 2, th.size), np.complex128)
+    pmm = np.full(th.size, math.sqrt(1.0 / (4 * math.pi)))
+    for m in range(P + 1):
+        if m > 0:
+            pmm = -math.sqrt((2 * m + 1) / (2 * m)) * s * pmm
+        e = np.exp(1j * m * ph)
+        sign = -1.0 if m % 2 else 1.0
+        p2, p1 = None, pmm
+        for n in range(m, P + 1):
+            if n == m + 1:
+                p2, p1 = p1, math.sqrt(2 * m + 3) * x * p1
+            elif n > m + 1:
+                a = math.sqrt((4 * n * n - 1) / (n * n - m * m))
+                b = math.sqrt(((n - 1) ** 2 - m * m) / (4 * (n - 1) ** 2 - 1))
+                p2, p1 = p1, a * (x * p1 - b * p2)
+            y = p1 * e
+            out[n * n + n + m] = y
+            if m:
+                out[n * n + n - m] = sign * np.conj(y)
+    return out
+
+
+@lru_cache(maxsize=None)
+def _rotation_quadrature(P):
+    """Gauss-Legendre x uniform azimuth nodes exact for degree 2P, their weights and
+    the harmonics there."""
     nq = P + 2
     x, w = leggauss(nq)
     th = np.arccos(x)
@@ -125,13 +159,15 @@ def rotation_blocks(P, R):
     W = np.outer(w, np.full(len(ph), 2 * np.pi / len(ph))).ravel()
     S = np.stack([np.sin(TH) * np.cos(PH), np.sin(TH) * np.sin(PH), np.cos(TH)], -1).reshape(-1, 3)
     _, t1, p1 = _sph(S)
+    return S, W, _harmonics(P, t1, p1)
+
+
+def rotation_blocks(P, R):
+    """T_n ((2n+1) x (2n+1) complex) for n <= P: coefficients in the frame R maps to."""
+    S, W, A = _rotation_quadrature(P)
     _, t2, p2 = _sph(S @ R.T)
-    out = []
-    for n in range(P + 1):
-        A = np.stack([sph_harm_y(n, m, t1, p1) for m in range(-n, n + 1)])
-        B = np.stack([sph_harm_y(n, m, t2, p2) for m in range(-n, n + 1)])
-        out.append((np.conj(B) * W) @ A.T)
-    return out
+    B = _harmonics(P, t2, p2)
+    return [(np.conj(B[n * n:(n + 1) ** 2]) * W) @ A[n * n:(n + 1) ** 2].T for n in range(P + 1)]
 
 
 def rotation_to_z(d):
@@ -171,6 +207,12 @@ def pack_rotations(P, blocks):
     return out
 
 
+@lru_cache(maxsize=4)
+def _packed_rotations(P):
+    """pack_rotations of direction_blocks(P), kept per order (it depends on nothing else)."""
+    return np.ascontiguousarray(pack_rotations(P, direction_blocks(P)))
+
+
 def distances():
     """Distinct |d|^2 of the non-adjacent slots (sorted) and each slot's index (-1: adjacent)."""
     d = displacements()
@@ -195,8 +237,9 @@ def level_operators(p, level, extent, k, imaginary, P):
     s = level_scale(extent, level)
     eq = surface_pts(p, R_EQUIV) * s
     r, th, ph = _sph(eq)
-    Ys = np.stack([sph_harm_y(n, m, th, ph) for n in range(P + 1) for m in range(-n, n + 1)])
-    Jn = np.stack([spherical_jn(n, k * r) for n in range(P + 1) for m in range(-n, n + 1)])
+    Ys = _harmonics(P, th, ph)
+    deg = np.array([n for n in range(P + 1) for _ in range(-n, n + 1)])
+    Jn = spherical_jn(deg[:, None], k * r[None, :])
     Q = np.conj(Ys) * Jn
     E = (Ys * Jn).T
     pref = 4 * math.pi * k * (1.0 if imaginary else -1.0)
@@ -213,7 +256,7 @@ def enable(state, order):
     if getattr(state, "kind", "helmholtz") != "helmholtz":
         raise ValueError("the rotation-based M2L is built for the Helmholtz kernel")
     P = int(order)
-    T = np.ascontiguousarray(pack_rotations(P, direction_blocks(P)))
+    T = _packed_rotations(P)
     uniq, slot = distances()
     slot = np.ascontiguousarray(slot, np.int32)
     check(_lib.lib.hfmm_plan_set_m2l_rotation(state.handle, P, T.ctypes.data, slot.ctypes.data,

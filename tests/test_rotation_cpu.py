@@ -37,6 +37,18 @@ def test_coaxial_coefficients_match_projection(regular):
         assert abs(C[m + P, n2, n] - num) <= 1e-11 * max(1.0, abs(num)), (n, m, n2)
 
 
+@pytest.mark.parametrize("P", [0, 1, 7, 24, 40])
+def test_harmonics_recurrence_matches_scipy(P):
+    rng = np.random.default_rng(P)
+    th = np.arccos(rng.uniform(-1, 1, 300))
+    th[:2] = 0.0, np.pi   # the poles
+    ph = rng.uniform(-np.pi, np.pi, 300)
+    n = np.array([a for a in range(P + 1) for _ in range(-a, a + 1)])
+    m = np.array([b for a in range(P + 1) for b in range(-a, a + 1)])
+    ref = sph_harm_y(n[:, None], m[:, None], th[None, :], ph[None, :])
+    assert np.abs(rot._harmonics(P, th, ph) - ref).max() < 1e-13
+
+
 def test_rotation_blocks_are_unitary_and_rotate():
     P = 8
     d = np.array([2.0, -1.0, 3.0])
