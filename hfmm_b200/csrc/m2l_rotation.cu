@@ -12,13 +12,15 @@
 //      there), rotates them into the frame whose z axis is the displacement (T_n per
 //      degree n, (2n+1)^2 complex), shifts them coaxially by |d| (one real
 //      (P+1-|m|)^2 matrix per order m) and rotates the result back (T_n^H) into the
-//      targets' local coefficients, which stay in registers. The slot's tables are
-//      read once per tile instead of once per pair. At the end the targets' check
+//      targets' local coefficients, which stay in registers. A thread owns whole
+//      coefficient rows across the tile's columns, so each table value it loads feeds
+//      every column; the slot's tables are read once per tile instead of once per pair. At the end the targets' check
 //      potentials are Re(pref E L) (E: n_s x (P+1)^2 complex), which the L2L GEMM and
 //      the decode then use as in the dense path.
 // The operators are built on the host in FP64 (hfmm_b200/rotation.py) and uploaded by
-// hfmm_plan_set_m2l_rotation / hfmm_plan_set_rotation_level (Q and E transposed on
-// upload, for reads coalesced over the thread index). Every stage is O(P^3) per
+// hfmm_plan_set_m2l_rotation / hfmm_plan_set_rotation_level (the rotation blocks
+// also transposed, Q, E and the coaxial matrices transposed on upload, for reads
+// coalesced over the thread index). Every stage is O(P^3) per
 // pair. Each target sums its slots in slot order, so results are deterministic.
 #include "hfmm_internal.cuh"
 
@@ -30,16 +32,17 @@ namespace hfmm {
 namespace {
 
 constexpr int ROT_THREADS = 512;
-constexpr int ROT_MAXI = 12;     // stage items per thread: (P+1)^2 x columns <= 6144
+constexpr int ROT_MAXI = 12;     // local coefficients a thread holds: rows x columns
 constexpr int ROT_MAXCOL = 16;   // charge columns (targets x R) per CTA
 constexpr int ROT_MP_THREADS = 256;
 
 struct RotCall {
-    const double2* T;          // [343][TS] rotation blocks per displacement slot
+    const double2* T;          // [343][TS] rotation blocks per displacement slot, T_n[m][m'']
+    const double2* Tt;         // [343][TS] the same blocks transposed, T_n^T
     const int32_t* dist;       // [343] coaxial matrix index (-1: adjacent slot)
     const double2* QT;         // [n_s][NC]
     const double2* ET;         // [NC][n_s]
-    const double* C;           // [n_dist][2P+1][P+1][P+1]
+    const double* C;           // [n_dist][2P+1][P+1][P+1], C[d][m][n][n'] (source n, local n')
     const int32_t* src_tab;    // [nb][351]
     const double* equiv;       // family base of the equivalent densities [nb][R][ld]
     double* check;             // family base of the check potentials [nb][R][ld]
@@ -97,21 +100,38 @@ __global__ void __launch_bounds__(ROT_MP_THREADS) k_rot_multipole(RotCall c) {
     }
 }
 
+// One thread per coefficient row (n, m) and every charge column of the tile: each
+// table value a thread loads feeds all of the tile's columns. ROWS = rows per thread
+// ((P+1)^2 <= ROWS x ROT_THREADS), NCM = the columns the registers hold for them.
+template <int ROWS>
 __global__ void __launch_bounds__(ROT_THREADS) k_rot_m2l(RotCall c) {
+    constexpr int NCM = ROT_MAXI / ROWS;
     extern __shared__ double2 sm[];
     __shared__ int32_t src[ROT_MAXCOL];
     const int NC = c.NC, NCOL = c.TT * c.R, NI = NC * NCOL, P = c.P;
     double2* X = sm;        // [NC][NCOL] gathered source coefficients, then the shifted ones
     double2* Y = sm + NI;   // [NC][NCOL] rotated
+    int16_t* mq = reinterpret_cast<int16_t*>(sm + 2 * NI);   // [NC] rows in m-major order
+    for (int i = threadIdx.x; i < NC; i += ROT_THREADS) {    // i -> (m, n), m = -P..P, n = |m|..P
+        int m = -P, base = 0;
+        while (base + P + 1 - (m < 0 ? -m : m) <= i) {
+            base += P + 1 - (m < 0 ? -m : m);
+            ++m;
+        }
+        const int n = (m < 0 ? -m : m) + (i - base);
+        mq[i] = (int16_t)(n * n + n + m);
+    }
     const int64_t t0 = c.lo + (int64_t)blockIdx.x * c.TT;
     const int nt = (int)min((int64_t)c.TT, c.hi - t0);
-    double2 L[ROT_MAXI];    // the tile's local coefficients, item i = threadIdx.x + k ROT_THREADS
+    double2 L[ROWS][NCM];   // local coefficients of rows threadIdx.x + k ROT_THREADS
 #pragma unroll
-    for (int k = 0; k < ROT_MAXI; ++k) L[k] = make_double2(0.0, 0.0);
+    for (int k = 0; k < ROWS; ++k)
+#pragma unroll
+        for (int cc = 0; cc < NCM; ++cc) L[k][cc] = make_double2(0.0, 0.0);
     for (int e = 0; e < N_DISP; ++e) {
         const int di = c.dist[e];
         if (di < 0) continue;   // adjacent slot: no V pair
-        __syncthreads();        // the previous slot's last stage has read X and src
+        __syncthreads();        // the previous slot's last stage has read X and src (and mq is built)
         if (threadIdx.x < c.TT) {
             int sb = -1;
             if (threadIdx.x < nt) {
@@ -134,64 +154,88 @@ __global__ void __launch_bounds__(ROT_THREADS) k_rot_m2l(RotCall c) {
             X[q * NCOL + cc] = sb >= 0 ? c.M[((int64_t)sb * c.R + r) * NC + q] : make_double2(0.0, 0.0);
         }
         __syncthreads();
-        const double2* __restrict__ T = c.T + (int64_t)e * c.TS;
-        // rotate: Y[(n, m)] = sum_j T_n[m][j] X[(n, j - n)]
+        const int64_t toff = (int64_t)e * c.TS;
+        // rotate: Y[(n, m)] = sum_j T_n[m][j] X[(n, j - n)], T_n^T read along m (coalesced)
 #pragma unroll
-        for (int k = 0; k < ROT_MAXI; ++k) {
-            const int i = threadIdx.x + k * ROT_THREADS;
-            if (i < NI) {
-                const int q = i / NCOL, cc = i - q * NCOL;
-                const int n = deg_of(q), m = q - n * n - n;
-                const double2* Tn = T + tri_off(n) + (m + n) * (2 * n + 1);
-                const double2* x = X + n * n * NCOL + cc;
-                double2 acc = make_double2(0.0, 0.0);
-                for (int j = 0; j <= 2 * n; ++j) cmac(acc, __ldg(Tn + j), x[j * NCOL]);
-                Y[i] = acc;
+        for (int k = 0; k < ROWS; ++k) {
+            const int q = threadIdx.x + k * ROT_THREADS;
+            if (q < NC) {
+                const int n = deg_of(q), m = q - n * n - n, w = 2 * n + 1;
+                const double2* __restrict__ Tt = c.Tt + toff + tri_off(n) + (m + n);
+                const double2* x = X + n * n * NCOL;
+                double2 acc[NCM];
+#pragma unroll
+                for (int cc = 0; cc < NCM; ++cc) acc[cc] = make_double2(0.0, 0.0);
+                for (int j = 0; j < w; ++j) {
+                    const double2 t = __ldg(Tt + j * w);
+                    const double2* xj = x + j * NCOL;
+#pragma unroll
+                    for (int cc = 0; cc < NCM; ++cc)
+                        if (cc < NCOL) cmac(acc[cc], t, xj[cc]);
+                }
+#pragma unroll
+                for (int cc = 0; cc < NCM; ++cc)
+                    if (cc < NCOL) Y[q * NCOL + cc] = acc[cc];
             }
         }
         __syncthreads();
-        // shift along z: X[(n', m)] = sum_{n >= |m|} C[m][n'][n] Y[(n, m)]
+        // shift along z: X[(n', m)] = sum_{n >= |m|} C[m][n'][n] Y[(n, m)], rows in m-major
+        // order so that a warp reads the same Y rows; C stored as [m][n][n'] (coalesced)
         const double* __restrict__ Cd = c.C + (int64_t)di * (2 * P + 1) * (P + 1) * (P + 1);
 #pragma unroll
-        for (int k = 0; k < ROT_MAXI; ++k) {
+        for (int k = 0; k < ROWS; ++k) {
             const int i = threadIdx.x + k * ROT_THREADS;
-            if (i < NI) {
-                const int q = i / NCOL, cc = i - q * NCOL;
+            if (i < NC) {
+                const int q = mq[i];
                 const int n2 = deg_of(q), m = q - n2 * n2 - n2;
                 const int am = m < 0 ? -m : m;
-                const double* Cm = Cd + ((int64_t)(m + P) * (P + 1) + n2) * (P + 1);
-                const double2* y = Y + cc;
-                double2 acc = make_double2(0.0, 0.0);
+                const double* Cm = Cd + (int64_t)(m + P) * (P + 1) * (P + 1) + n2;
+                double2 acc[NCM];
+#pragma unroll
+                for (int cc = 0; cc < NCM; ++cc) acc[cc] = make_double2(0.0, 0.0);
                 for (int n = am; n <= P; ++n) {
-                    const double w = __ldg(Cm + n);
-                    const double2 v = y[(n * n + n + m) * NCOL];
-                    acc.x = fma(w, v.x, acc.x);
-                    acc.y = fma(w, v.y, acc.y);
+                    const double w = __ldg(Cm + n * (P + 1));
+                    const double2* y = Y + (n * n + n + m) * NCOL;
+#pragma unroll
+                    for (int cc = 0; cc < NCM; ++cc)
+                        if (cc < NCOL) {
+                            const double2 v = y[cc];
+                            acc[cc].x = fma(w, v.x, acc[cc].x);
+                            acc[cc].y = fma(w, v.y, acc[cc].y);
+                        }
                 }
-                X[i] = acc;
+#pragma unroll
+                for (int cc = 0; cc < NCM; ++cc)
+                    if (cc < NCOL) X[q * NCOL + cc] = acc[cc];
             }
         }
         __syncthreads();
         // rotate back and accumulate: L[(n, m)] += sum_j conj(T_n[j][m]) X[(n, j - n)]
 #pragma unroll
-        for (int k = 0; k < ROT_MAXI; ++k) {
-            const int i = threadIdx.x + k * ROT_THREADS;
-            if (i < NI) {
-                const int q = i / NCOL, cc = i - q * NCOL;
-                const int n = deg_of(q), m = q - n * n - n;
-                const double2* Tn = T + tri_off(n) + (m + n);
-                const double2* x = X + n * n * NCOL + cc;
-                double2 acc = L[k];
-                for (int j = 0; j <= 2 * n; ++j) cmacc(acc, __ldg(Tn + j * (2 * n + 1)), x[j * NCOL]);
-                L[k] = acc;
+        for (int k = 0; k < ROWS; ++k) {
+            const int q = threadIdx.x + k * ROT_THREADS;
+            if (q < NC) {
+                const int n = deg_of(q), m = q - n * n - n, w = 2 * n + 1;
+                const double2* __restrict__ Tn = c.T + toff + tri_off(n) + (m + n);
+                const double2* x = X + n * n * NCOL;
+                for (int j = 0; j < w; ++j) {
+                    const double2 t = __ldg(Tn + j * w);
+                    const double2* xj = x + j * NCOL;
+#pragma unroll
+                    for (int cc = 0; cc < NCM; ++cc)
+                        if (cc < NCOL) cmacc(L[k][cc], t, xj[cc]);
+                }
             }
         }
     }
     __syncthreads();
 #pragma unroll
-    for (int k = 0; k < ROT_MAXI; ++k) {
-        const int i = threadIdx.x + k * ROT_THREADS;
-        if (i < NI) X[i] = L[k];
+    for (int k = 0; k < ROWS; ++k) {
+        const int q = threadIdx.x + k * ROT_THREADS;
+        if (q < NC)
+#pragma unroll
+            for (int cc = 0; cc < NCM; ++cc)
+                if (cc < NCOL) X[q * NCOL + cc] = L[k][cc];
     }
     __syncthreads();
     // the check potentials at the targets' check points: Re(pref E L), padding zeroed
@@ -229,14 +273,16 @@ void rot_m2l(hfmm_plan* P, int l, int R, int64_t fam_stride, cudaStream_t s) {
     const int Pn = P->rot_P, NC = (Pn + 1) * (Pn + 1);
     if (P->rot_M.n < rot_workspace_doubles(P))   // a rebuilt tree with a wider level
         throw Error{HFMM_ERR_STATE, "rotation M2L: set the rotation again after the plan was rebuilt"};
-    // targets per CTA: at most ROT_MAXCOL charge columns and ROT_MAXI items per thread
-    const int TT = std::min(ROT_MAXCOL / R, ROT_THREADS * ROT_MAXI / (NC * R));
+    // rows per thread, then targets per CTA: the columns a thread's registers hold
+    const int rows = (int)ceil_div(NC, ROT_THREADS);
+    const int TT = rows <= 4 ? std::min(ROT_MAXCOL, ROT_MAXI / rows) / R : 0;
     if (TT < 1) throw Error{HFMM_ERR_ARG, "rotation M2L: order too high for one CTA"};
     for (int f = 0; f < P->n_fam; ++f) {
         LevelTables& T = P->tables[f][l];
         if (!T.rot_Q.p) throw Error{HFMM_ERR_STATE, "rotation M2L: level operators missing"};
         RotCall c{};
         c.T = reinterpret_cast<const double2*>(P->rot_T.p);
+        c.Tt = c.T + (int64_t)N_DISP * ((Pn + 1) * (4 * (Pn + 1) * (Pn + 1) - 1) / 3);
         c.dist = P->rot_dist.p;
         c.QT = reinterpret_cast<const double2*>(T.rot_Q.p);
         c.ET = reinterpret_cast<const double2*>(T.rot_E.p);
@@ -263,9 +309,17 @@ void rot_m2l(hfmm_plan* P, int l, int R, int64_t fam_stride, cudaStream_t s) {
                                        (int)smem_mp));
         HFMM_LAUNCH(k_rot_multipole, (unsigned)ceil_div(nbl, (int64_t)c.TT), ROT_MP_THREADS, smem_mp, s, c);
         c.TT = TT;
-        const size_t smem = (size_t)2 * NC * TT * R * sizeof(double2);
-        HFMM_CUDA(cudaFuncSetAttribute(k_rot_m2l, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        HFMM_LAUNCH(k_rot_m2l, (unsigned)ceil_div(nbl, (int64_t)TT), ROT_THREADS, smem, s, c);
+        // X and Y, then the m-major row table (int16) rounded up to 16 bytes
+        const size_t smem = (size_t)2 * NC * TT * R * sizeof(double2) + (size_t)ceil_div(NC * 2, 16) * 16;
+        const unsigned grid = (unsigned)ceil_div(nbl, (int64_t)TT);
+        auto launch = [&](auto kern) {
+            HFMM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            HFMM_LAUNCH(kern, grid, ROT_THREADS, smem, s, c);
+        };
+        if (rows == 1) launch(k_rot_m2l<1>);
+        else if (rows == 2) launch(k_rot_m2l<2>);
+        else if (rows == 3) launch(k_rot_m2l<3>);
+        else launch(k_rot_m2l<4>);
     }
 }
 
@@ -289,8 +343,20 @@ int hfmm_plan_set_m2l_rotation(hfmm_plan* P, int32_t order, const double* T_host
         std::vector<int32_t> d(dist_host, dist_host + N_DISP);
         for (int e = 0; e < N_DISP; ++e)
             if (d[e] >= n_dist) return fail(HFMM_ERR_ARG, "distance index out of range");
-        P->rot_T.alloc(N_DISP * TS * 2);
+        // the blocks as given, then each block transposed (T_n^T), complex as re, im pairs
+        std::vector<double> tt(N_DISP * TS * 2);
+        for (size_t e = 0; e < (size_t)N_DISP; ++e)
+            for (int n = 0, off = 0; n <= order; off += (2 * n + 1) * (2 * n + 1), ++n) {
+                const size_t w = 2 * n + 1, b = e * TS + off;
+                for (size_t a = 0; a < w; ++a)
+                    for (size_t j = 0; j < w; ++j)
+                        for (int z = 0; z < 2; ++z)
+                            tt[(b + j * w + a) * 2 + z] = T_host[(b + a * w + j) * 2 + z];
+            }
+        P->rot_T.alloc(2 * N_DISP * TS * 2);
         HFMM_CUDA(cudaMemcpy(P->rot_T.p, T_host, N_DISP * TS * 2 * sizeof(double), cudaMemcpyHostToDevice));
+        HFMM_CUDA(cudaMemcpy(P->rot_T.p + N_DISP * TS * 2, tt.data(), N_DISP * TS * 2 * sizeof(double),
+                             cudaMemcpyHostToDevice));
         P->rot_dist.alloc(N_DISP);
         HFMM_CUDA(cudaMemcpy(P->rot_dist.p, d.data(), N_DISP * sizeof(int32_t), cudaMemcpyHostToDevice));
         P->rot_P = order;
@@ -330,10 +396,16 @@ int hfmm_plan_set_rotation_level(hfmm_plan* P, int32_t family, int32_t level, co
                 }
         T.rot_Q.alloc(NC * ns * 2);
         T.rot_E.alloc(NC * ns * 2);
+        // C[d][m][n'][n] stored as [d][m][n][n'] (the shift reads it along n')
+        const size_t p1 = (size_t)P->rot_P + 1;
+        std::vector<double> ct(nc);
+        for (size_t dm = 0; dm < nc / (p1 * p1); ++dm)
+            for (size_t a = 0; a < p1; ++a)
+                for (size_t b = 0; b < p1; ++b) ct[(dm * p1 + b) * p1 + a] = C_host[(dm * p1 + a) * p1 + b];
         T.rot_C.alloc(nc);
         HFMM_CUDA(cudaMemcpy(T.rot_Q.p, qt.data(), NC * ns * 2 * sizeof(double), cudaMemcpyHostToDevice));
         HFMM_CUDA(cudaMemcpy(T.rot_E.p, et.data(), NC * ns * 2 * sizeof(double), cudaMemcpyHostToDevice));
-        HFMM_CUDA(cudaMemcpy(T.rot_C.p, C_host, nc * sizeof(double), cudaMemcpyHostToDevice));
+        HFMM_CUDA(cudaMemcpy(T.rot_C.p, ct.data(), nc * sizeof(double), cudaMemcpyHostToDevice));
         T.rot_pref = pref;
         return HFMM_OK;
     } catch (const Error& e) {
