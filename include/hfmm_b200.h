@@ -328,8 +328,10 @@ int hfmm_plan_set_m2l_queue(hfmm_plan* plan, int32_t on);
  * family and level, hfmm_plan_set_rotation_level with Q [(order+1)^2][n_s] complex
  * (multipole from equivalent density), E [n_s][(order+1)^2] complex (check potential
  * from local coefficients, times pref, real part) and C [n_dist][2 order+1][order+1]
- * [order+1] real (the coaxial shifts). hfmm_b200/rotation.py builds all of them. Only the
- * FP64 evaluate uses it; after hfmm_plan_rebuild set it again. */
+ * [order+1] real (the coaxial shifts: C[d][m + order][n'][n] takes multipole (n, m) to
+ * local (n', m)). The library keeps its own transposed copies. hfmm_b200/rotation.py
+ * builds all of them. Only the FP64 evaluate uses it; after hfmm_plan_rebuild set it
+ * again. */
 int hfmm_plan_set_m2l_rotation(hfmm_plan* plan, int32_t order, const double* T_host,
                                const int32_t* dist_host, int32_t n_dist);
 int hfmm_plan_set_rotation_level(hfmm_plan* plan, int32_t family, int32_t level, const double* Q_host,

@@ -354,24 +354,36 @@ def eval_direct(s, kern, ppts, pchg, rev, field, batch=512):
     R = pchg.shape[2]
     buf = np.zeros((mb, w, R, 3) if field else (mb, w, R))
     feps = min(EPS, float(np.finfo(np.float32).eps))
-    for lo in range(0, dc.shape[0], batch):
-        pr = dc[lo:lo + batch]
-        kt = ppts[pr[:, 0]]                                   # (B, w_e, 3)
-        kp = ppts[pr[:, 1]]                                   # (B, w_s, 3)
+    # A row's real points come first, its padding (point 0 again, charge 0) after them.
+    # Padded sources add 0 and padded targets are dropped, so each batch is cut to its
+    # widest real row; pairs run narrowest first so that a batch's rows are alike. The
+    # floor's scale still takes the maximum over the whole padded row, as near.py does.
+    nv = (s["pil"] >= 0).sum(axis=1)
+    width = np.maximum(nv[dc[:, 0]], nv[dc[:, 1]])
+    order = np.argsort(width, kind="stable")
+    n_pairs, lo = dc.shape[0], 0
+    while lo < n_pairs:
+        w_hi = int(width[order[min(lo + batch, n_pairs) - 1]])
+        hi = min(n_pairs, lo + max(1, min(batch, (1 << 22) // max(1, w_hi * w_hi))))
+        pr = dc[order[lo:hi]]
+        lo = hi
+        we, ws = max(1, int(nv[pr[:, 0]].max())), max(1, int(nv[pr[:, 1]].max()))
+        kt_row, kp_row = ppts[pr[:, 0]], ppts[pr[:, 1]]       # (B, w, 3), padding included
+        rs = np.sqrt(np.max(kp_row[..., 0] ** 2 + kp_row[..., 1] ** 2 + kp_row[..., 2] ** 2, axis=1))
+        re = np.sqrt(np.max(np.sum(kt_row ** 2, axis=-1), axis=1))
+        kt, kp = kt_row[:, :we], kp_row[:, :ws]               # (B, w_e, 3), (B, w_s, 3)
         dd = [kt[:, None, :, c] - kp[:, :, None, c] for c in range(3)]   # (B, w_s, w_e)
         d2 = dd[0] ** 2 + dd[1] ** 2 + dd[2] ** 2
-        rs = np.sqrt(np.max(kp[..., 0] ** 2 + kp[..., 1] ** 2 + kp[..., 2] ** 2, axis=1))
-        re = np.sqrt(np.max(np.sum(kt ** 2, axis=-1), axis=1))
         scale = ((re + rs) ** 2)[:, None, None]
         d2 = np.where(d2 > (16 * feps) ** 2 * scale, d2, 0.0)
-        q = pchg[pr[:, 1]]                                    # (B, w_s, R)
+        q = pchg[pr[:, 1], :ws]                               # (B, w_s, R)
         if field:
             kw = kern.k2g(d2)
             pot = np.stack([np.einsum("bse,bsr->ber", kw * dd[c], q) for c in range(3)], -1)
         else:
             kw = kern.k2(d2)
             pot = np.einsum("bse,bsr->ber", kw, q)
-        np.add.at(buf, pr[:, 0], pot)
+        np.add.at(buf[:, :we], pr[:, 0], pot)
     flat = buf.reshape((mb * w,) + buf.shape[2:])
     return flat[rev] / (4 * np.pi)
 

@@ -30,7 +30,13 @@ def helmholtz_G_np(k, imaginary):
     trig = np.sin if imaginary else np.cos
 
     def G(x, y):
-        r = np.linalg.norm(x[:, None, :] - y[None, :, :], axis=-1)
+        # |x - y| as np.linalg.norm(axis=-1) forms it, (dx^2 + dy^2) + dz^2, one
+        # component at a time instead of through an (n, m, 3) array
+        r = None
+        for c in range(3):
+            dc = x[:, c, None] - y[None, :, c]
+            r = dc * dc if r is None else r + dc * dc
+        np.sqrt(r, out=r)
         ok = r > 16 * np.finfo(r.dtype).eps * r.max(initial=0.0)
         return np.where(ok, trig(k * r) / np.where(ok, r, 1.0), 0.0)
     return G
@@ -43,12 +49,13 @@ def pinv_factors(A, eps_rel=1e-7):
     return U, s / (s * s + eps * eps), Vt
 
 
-def build_operators(p, G, eps_rel=1e-7):
+def build_operators(p, G, eps_rel=1e-7, m2l_out=None):
     """Unit-box operator set for kernel matrix function ``G`` (operators.py:330-403).
 
     Returns the members the leveled path uses. ``M2L_K_table`` has shape
     (343, n_s, n_s) in displacement order ``(dx+3)*49 + (dy+3)*7 + (dz+3)`` with
-    zero matrices at the 27 adjacent displacements.
+    zero matrices at the 27 adjacent displacements; ``m2l_out``, if given, is the
+    zeroed array it is written into.
     """
     equiv = surface_pts(p, R_EQUIV)
     check = surface_pts(p, R_CHECK)
@@ -59,7 +66,7 @@ def build_operators(p, G, eps_rel=1e-7):
     M2M_K = np.empty((8, n_s, n_s))
     for c in range(8):
         M2M_K[c] = G(parent_check, equiv + CHILD_OFFSETS[c])
-    M2L = np.zeros((343, n_s, n_s))
+    M2L = np.zeros((343, n_s, n_s)) if m2l_out is None else m2l_out
     for dxi in range(7):
         for dyi in range(7):
             for dzi in range(7):
@@ -82,11 +89,13 @@ def build_operators_leveled(p, max_depth, domain_extent, G, eps_rel=1e-7):
     ``M2M_K_lv[pl]`` (parent level pl) and ``L2L_K_lv[cl-1]`` (child level cl) are
     both taken from the CHILD level's assembly, as in the reference.
     """
+    n_s = surface_pts(p, R_EQUIV).shape[0]
+    m2l = np.zeros((max_depth + 1, 343, n_s, n_s))   # filled in place, level by level
     per = []
     for l in range(max_depth + 1):
         s = float(domain_extent) * 0.5 ** (l + 1)
         Gs = (lambda x, y, _s=s: G(x * _s, y * _s))
-        per.append(build_operators(p, Gs, eps_rel))
+        per.append(build_operators(p, Gs, eps_rel, m2l_out=m2l[l]))
 
     def stack_f(key):
         return tuple(np.stack([np.asarray(o[key][i]) for o in per]) for i in range(3))
@@ -96,5 +105,5 @@ def build_operators_leveled(p, max_depth, domain_extent, G, eps_rel=1e-7):
         F_up_lv=stack_f("F_up"), F_dn_lv=stack_f("F_dn"),
         M2M_K_lv=np.stack([per[pl + 1]["M2M_K"] for pl in range(max_depth)]),
         L2L_K_lv=np.stack([per[cl]["L2L_K"] for cl in range(1, max_depth + 1)]),
-        M2L_K_lv=np.stack([o["M2L_K_table"] for o in per]),
+        M2L_K_lv=m2l,
     )
