@@ -342,6 +342,9 @@ def calibrate_c1(budget_s, log=print):
     est, _, _ = OracleSampler(cfg, log).sample(budget_s)
     pos, q = make_problem(cfg)
     st = O.setup(pos, cfg["k"], p=cfg["p"], N_max=cfg["leaf"], max_depth=cfg["max_depth"])
+    for s in st:   # every padded near-field slot, as the reference evaluates them
+        if s is not None:
+            s["near_trim"] = False
     t0 = time.perf_counter()
     O.evaluate_complex(st, q, field=True)
     full = time.perf_counter() - t0

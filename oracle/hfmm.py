@@ -355,10 +355,13 @@ def eval_direct(s, kern, ppts, pchg, rev, field, batch=512):
     buf = np.zeros((mb, w, R, 3) if field else (mb, w, R))
     feps = min(EPS, float(np.finfo(np.float32).eps))
     # A row's real points come first, its padding (point 0 again, charge 0) after them.
-    # Padded sources add 0 and padded targets are dropped, so each batch is cut to its
-    # widest real row; pairs run narrowest first so that a batch's rows are alike. The
-    # floor's scale still takes the maximum over the whole padded row, as near.py does.
-    nv = (s["pil"] >= 0).sum(axis=1)
+    # Padded sources add 0 and padded targets are dropped, so with the state's "pil"
+    # each batch is cut to its widest real row (pairs run narrowest first so that a
+    # batch's rows are alike); the floor's scale still takes the maximum over the whole
+    # padded row, as near.py does. near_trim=False in the state (or no "pil") evaluates
+    # every padded slot, as the reference does: the CPU cost the benchmark times.
+    pil = s.get("pil") if s.get("near_trim", True) else None
+    nv = (pil >= 0).sum(axis=1) if pil is not None else np.full(mb, w)
     width = np.maximum(nv[dc[:, 0]], nv[dc[:, 1]])
     order = np.argsort(width, kind="stable")
     n_pairs, lo = dc.shape[0], 0
