@@ -31,8 +31,9 @@ namespace hfmm {
 
 namespace {
 
-constexpr int ROT_THREADS = 512;
-constexpr int ROT_MAXI = 12;     // local coefficients a thread holds: rows x columns
+constexpr int ROT_THREADS = 256;  // two CTAs per SM: one's barrier waits overlap the other's work
+constexpr int ROT_MAXI = 14;     // local coefficients a thread holds: rows x columns
+constexpr int ROT_MAXROWS = 7;   // (P+1)^2 <= 7 x 256 covers P <= 40
 constexpr int ROT_MAXCOL = 16;   // charge columns (targets x R) per CTA
 constexpr int ROT_MP_THREADS = 256;
 
@@ -104,8 +105,8 @@ __global__ void __launch_bounds__(ROT_MP_THREADS) k_rot_multipole(RotCall c) {
 // table value a thread loads feeds all of the tile's columns. ROWS = rows per thread
 // ((P+1)^2 <= ROWS x ROT_THREADS), NCM = the columns the registers hold for them.
 template <int ROWS>
-__global__ void __launch_bounds__(ROT_THREADS) k_rot_m2l(RotCall c) {
-    constexpr int NCM = ROT_MAXI / ROWS;
+__global__ void __launch_bounds__(ROT_THREADS, 2) k_rot_m2l(RotCall c) {
+    constexpr int NCM = (ROT_MAXI / ROWS) < 12 ? ROT_MAXI / ROWS : 12;
     extern __shared__ double2 sm[];
     __shared__ int32_t src[ROT_MAXCOL];
     const int NC = c.NC, NCOL = c.TT * c.R, NI = NC * NCOL, P = c.P;
@@ -275,7 +276,7 @@ void rot_m2l(hfmm_plan* P, int l, int R, int64_t fam_stride, cudaStream_t s) {
         throw Error{HFMM_ERR_STATE, "rotation M2L: set the rotation again after the plan was rebuilt"};
     // rows per thread, then targets per CTA: the columns a thread's registers hold
     const int rows = (int)ceil_div(NC, ROT_THREADS);
-    const int TT = rows <= 4 ? std::min(ROT_MAXCOL, ROT_MAXI / rows) / R : 0;
+    const int TT = rows <= ROT_MAXROWS ? std::min(std::min(ROT_MAXCOL, 12), ROT_MAXI / rows) / R : 0;
     if (TT < 1) throw Error{HFMM_ERR_ARG, "rotation M2L: order too high for one CTA"};
     for (int f = 0; f < P->n_fam; ++f) {
         LevelTables& T = P->tables[f][l];
@@ -316,10 +317,15 @@ void rot_m2l(hfmm_plan* P, int l, int R, int64_t fam_stride, cudaStream_t s) {
             HFMM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
             HFMM_LAUNCH(kern, grid, ROT_THREADS, smem, s, c);
         };
-        if (rows == 1) launch(k_rot_m2l<1>);
-        else if (rows == 2) launch(k_rot_m2l<2>);
-        else if (rows == 3) launch(k_rot_m2l<3>);
-        else launch(k_rot_m2l<4>);
+        switch (rows) {
+            case 1: launch(k_rot_m2l<1>); break;
+            case 2: launch(k_rot_m2l<2>); break;
+            case 3: launch(k_rot_m2l<3>); break;
+            case 4: launch(k_rot_m2l<4>); break;
+            case 5: launch(k_rot_m2l<5>); break;
+            case 6: launch(k_rot_m2l<6>); break;
+            default: launch(k_rot_m2l<7>); break;
+        }
     }
 }
 
