@@ -248,28 +248,49 @@ def level_operators(p, level, extent, k, imaginary, P):
 
 def enable(state, order):
     """Switch a plan's FP64 evaluate to the rotation-based M2L of ``order`` P (the
-    Helmholtz kernel; the dense tables stay in the plan for the other paths). Builds
-    the operators on the host (the coaxial coefficients' Gaunt table once per order,
-    about 20 s at P = 20) and uploads them."""
+    Helmholtz kernel, k > 0; the dense tables stay in the plan for the other paths).
+    Builds every level's operators on the host first (rotation blocks and the Gaunt
+    table once per order: about 4 s at P = 20, 25 s at P = 32) and uploads them only
+    when all are finite: at small k x box size with a high order the Neumann
+    functions y_nu(k t), nu <= 2P, overflow, and that raises ValueError with the plan
+    unchanged."""
     from . import _lib
     from ._lib import check
     if getattr(state, "kind", "helmholtz") != "helmholtz":
         raise ValueError("the rotation-based M2L is built for the Helmholtz kernel")
     P = int(order)
-    T = _packed_rotations(P)
-    uniq, slot = distances()
-    slot = np.ascontiguousarray(slot, np.int32)
-    check(_lib.lib.hfmm_plan_set_m2l_rotation(state.handle, P, T.ctypes.data, slot.ctypes.data,
-                                               len(uniq)))
+    if not 1 <= P <= 40:
+        raise ValueError("rotation order must be in [1, 40]")
+    if not float(state.k) > 0.0:
+        raise ValueError("the rotation-based M2L needs k > 0 (its expansions are spherical "
+                         "Bessel and Neumann functions of k r)")
     extent = state.info["domain_extent"]
+    for level in range(2, state.max_depth + 1):
+        # the largest Neumann value the shifts take: y_2P at the nearest V distance, 4 s
+        x = state.k * 4 * level_scale(extent, level)
+        if not np.isfinite(spherical_yn(2 * P, x)):
+            raise ValueError(f"rotation order {P} overflows at level {level} (y_{2 * P}"
+                             f"({x:.3g}) is not finite): use a lower order or the dense tables")
+    levels = []
     for fam in range(state.n_families):
         for level in range(2, state.max_depth + 1):
             Q, E, pref = level_operators(state.p, level, extent, state.k, fam == 1, P)
             C = np.ascontiguousarray(pack_coaxial(P, state.k, level_scale(extent, level), fam == 1))
             Q = np.ascontiguousarray(Q.astype(np.complex128))
             E = np.ascontiguousarray(E.astype(np.complex128))
-            check(_lib.lib.hfmm_plan_set_rotation_level(state.handle, fam, level, Q.ctypes.data,
-                                                         E.ctypes.data, C.ctypes.data, float(pref)))
+            if not (np.isfinite(C).all() and np.isfinite(Q).all() and np.isfinite(E).all()):
+                raise ValueError(f"rotation order {P} overflows at level {level} (k x box side "
+                                 f"{state.k * 2 * level_scale(extent, level):.3g}): use a lower "
+                                 f"order or the dense tables")
+            levels.append((fam, level, Q, E, C, pref))
+    T = _packed_rotations(P)
+    uniq, slot = distances()
+    slot = np.ascontiguousarray(slot, np.int32)
+    check(_lib.lib.hfmm_plan_set_m2l_rotation(state.handle, P, T.ctypes.data, slot.ctypes.data,
+                                               len(uniq)))
+    for fam, level, Q, E, C, pref in levels:
+        check(_lib.lib.hfmm_plan_set_rotation_level(state.handle, fam, level, Q.ctypes.data,
+                                                     E.ctypes.data, C.ctypes.data, float(pref)))
     state.rotation_order = P
 
 

@@ -101,3 +101,19 @@ def test_rotation_m2l_matches_the_dense_kifmm_operator(imag):
         ref = O.family_matrix(k, imag)(eq + dv, eq) @ x
         err = np.linalg.norm(y - ref) / np.linalg.norm(ref)
         assert err < (1e-12 if imag else bar), (d, err)
+
+
+def test_enable_refuses_before_touching_the_plan():
+    """No plan handle is needed: every refusal comes before the first library call."""
+    from types import SimpleNamespace
+    st = SimpleNamespace(kind="helmholtz", k=10.0, p=4, info={"domain_extent": 1.0},
+                         n_families=2, max_depth=5, handle=None)
+    for bad in (dict(kind="yukawa"), dict(k=0.0)):
+        with pytest.raises(ValueError):
+            rot.enable(SimpleNamespace(**{**vars(st), **bad}), 10)
+    for order in (0, 41):
+        with pytest.raises(ValueError):
+            rot.enable(st, order)
+    with pytest.raises(ValueError, match="overflows"):   # y_80(k 4 s) at k = 0.05
+        rot.enable(SimpleNamespace(**{**vars(st), "k": 0.05}), 40)
+    assert not hasattr(st, "rotation_order")
