@@ -85,7 +85,7 @@ SIGNATURES = [
     ("hfmm_batch_queued", _c_i32, [_c_vp]),
     ("hfmm_batch_queue_note", ctypes.c_char_p, [_c_vp]),
     ("hfmm_plan_set_m2l_queue", _c_i32, [_c_vp, _c_i32]),
-    ("hfmm_plan_set_m2l_rotation", _c_i32, [_c_vp, _c_i32, _c_vp, _c_vp, _c_i32]),
+    ("hfmm_plan_set_m2l_rotation", _c_i32, [_c_vp, _c_i32, _c_vp, _c_i32, _c_vp, _c_vp, _c_vp, _c_i32]),
     ("hfmm_plan_set_rotation_level", _c_i32, [_c_vp, _c_i32, _c_i32, _c_vp, _c_vp, _c_vp, _c_dbl]),
     ("hfmm_batch_set_problem", _c_i32, [_c_vp, _c_i32, _c_vp, _c_vp, _c_vp, _c_vp, _c_i32]),
     ("hfmm_batch_set_check", _c_i32, [_c_vp, _c_i32, _c_vp, _c_vp, _c_i32, _c_vp]),

@@ -228,8 +228,10 @@ struct hfmm_plan {
     hfmm::DevBuf<double> q_s;        // R x n sorted charges
     hfmm::DevBuf<double> check, equiv, loc, tmp;   // [fam][box][R][ld]
     hfmm::DevBuf<double> gemm_part;  // partial tiles of the main stream's split GEMMs
-    int rot_P = 0, rot_n_dist = 0;   // rotation-based M2L of the FP64 evaluate (0: dense tables)
-    hfmm::DevBuf<double> rot_T;      // rotation blocks per displacement slot (complex)
+    int rot_P = 0, rot_n_dist = 0, rot_n_theta = 0;   // rotation-based M2L of the FP64 evaluate (0: dense)
+    hfmm::DevBuf<double> rot_D;      // real y-rotation blocks per polar angle, then transposed
+    hfmm::DevBuf<int32_t> rot_theta; // polar angle index per slot
+    hfmm::DevBuf<double> rot_phase;  // e^{i m phi} per slot (complex)
     hfmm::DevBuf<int32_t> rot_dist;  // coaxial matrix per slot
     hfmm::DevBuf<double> rot_M;      // multipole work array of one level
     hfmm::DevBuf<double> pot;        // per sorted particle: [fam][R] potentials

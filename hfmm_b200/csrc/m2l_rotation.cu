@@ -18,9 +18,12 @@
 //      potentials are Re(pref E L) (E: n_s x (P+1)^2 complex), which the L2L GEMM and
 //      the decode then use as in the dense path.
 // The operators are built on the host in FP64 (hfmm_b200/rotation.py) and uploaded by
-// hfmm_plan_set_m2l_rotation / hfmm_plan_set_rotation_level (the rotation blocks
+// hfmm_plan_set_m2l_rotation / hfmm_plan_set_rotation_level (the y-rotation blocks
 // also transposed, Q, E and the coaxial matrices transposed on upload, for reads
-// coalesced over the thread index). Every stage is O(P^3) per
+// coalesced over the thread index). A slot's rotation R_y(-theta) R_z(-phi) factors
+// as T_n = D_n(theta) diag(e^{i m phi}) with D_n real: the gather applies the phases,
+// the two rotation stages multiply by real blocks shared by the slots of one polar
+// angle, and the rotation back applies the conjugate phases per row. Every stage is O(P^3) per
 // pair. Each target sums its slots in slot order, so results are deterministic.
 #include "hfmm_internal.cuh"
 
@@ -38,8 +41,10 @@ constexpr int ROT_MAXCOL = 16;   // charge columns (targets x R) per CTA
 constexpr int ROT_MP_THREADS = 256;
 
 struct RotCall {
-    const double2* T;          // [343][TS] rotation blocks per displacement slot, T_n[m][m'']
-    const double2* Tt;         // [343][TS] the same blocks transposed, T_n^T
+    const double* D;           // [n_theta][TS] real y-rotation blocks D_n[m][m''] per polar angle
+    const double* Dt;          // [n_theta][TS] the same blocks transposed, D_n^T
+    const int32_t* theta;      // [343] polar angle index of each slot (-1: adjacent slot)
+    const double2* phase;      // [343][2P+1] e^{i m phi} of each slot: T_n = D_n diag(phase)
     const int32_t* dist;       // [343] coaxial matrix index (-1: adjacent slot)
     const double2* QT;         // [n_s][NC]
     const double2* ET;         // [NC][n_s]
@@ -148,31 +153,40 @@ __global__ void __launch_bounds__(ROT_THREADS, 2) k_rot_m2l(RotCall c) {
         bool any = false;
         for (int tt = 0; tt < nt; ++tt) any |= src[tt] >= 0;
         if (!any) continue;     // the same answer for every thread of the CTA
+        const double2* __restrict__ ph = c.phase + (int64_t)e * (2 * P + 1) + P;   // ph[m]
         for (int i = threadIdx.x; i < NI; i += ROT_THREADS) {   // coalesced over q
             const int cc = i / NC, q = i - cc * NC;
             const int tt = cc / c.R, r = cc - tt * c.R;
             const int sb = src[tt];
-            X[q * NCOL + cc] = sb >= 0 ? c.M[((int64_t)sb * c.R + r) * NC + q] : make_double2(0.0, 0.0);
+            double2 v = make_double2(0.0, 0.0);
+            if (sb >= 0) {   // the z-rotation: coefficient (n, m) times e^{i m phi}
+                const int n = deg_of(q);
+                cmac(v, c.M[((int64_t)sb * c.R + r) * NC + q], __ldg(ph + (q - n * n - n)));
+            }
+            X[q * NCOL + cc] = v;
         }
         __syncthreads();
-        const int64_t toff = (int64_t)e * c.TS;
-        // rotate: Y[(n, m)] = sum_j T_n[m][j] X[(n, j - n)], T_n^T read along m (coalesced)
+        const int64_t toff = (int64_t)c.theta[e] * c.TS;
+        // rotate about y: Y[(n, m)] = sum_j D_n[m][j] X[(n, j - n)], D_n^T read along m
 #pragma unroll
         for (int k = 0; k < ROWS; ++k) {
             const int q = threadIdx.x + k * ROT_THREADS;
             if (q < NC) {
                 const int n = deg_of(q), m = q - n * n - n, w = 2 * n + 1;
-                const double2* __restrict__ Tt = c.Tt + toff + tri_off(n) + (m + n);
+                const double* __restrict__ Dt = c.Dt + toff + tri_off(n) + (m + n);
                 const double2* x = X + n * n * NCOL;
                 double2 acc[NCM];
 #pragma unroll
                 for (int cc = 0; cc < NCM; ++cc) acc[cc] = make_double2(0.0, 0.0);
                 for (int j = 0; j < w; ++j) {
-                    const double2 t = __ldg(Tt + j * w);
+                    const double t = __ldg(Dt + j * w);
                     const double2* xj = x + j * NCOL;
 #pragma unroll
                     for (int cc = 0; cc < NCM; ++cc)
-                        if (cc < NCOL) cmac(acc[cc], t, xj[cc]);
+                        if (cc < NCOL) {
+                            acc[cc].x = fma(t, xj[cc].x, acc[cc].x);
+                            acc[cc].y = fma(t, xj[cc].y, acc[cc].y);
+                        }
                 }
 #pragma unroll
                 for (int cc = 0; cc < NCM; ++cc)
@@ -211,21 +225,31 @@ __global__ void __launch_bounds__(ROT_THREADS, 2) k_rot_m2l(RotCall c) {
             }
         }
         __syncthreads();
-        // rotate back and accumulate: L[(n, m)] += sum_j conj(T_n[j][m]) X[(n, j - n)]
+        // rotate back and accumulate: L[(n, m)] += conj(ph[m]) sum_j D_n[j][m] X[(n, j - n)]
 #pragma unroll
         for (int k = 0; k < ROWS; ++k) {
             const int q = threadIdx.x + k * ROT_THREADS;
             if (q < NC) {
                 const int n = deg_of(q), m = q - n * n - n, w = 2 * n + 1;
-                const double2* __restrict__ Tn = c.T + toff + tri_off(n) + (m + n);
+                const double* __restrict__ Dn = c.D + toff + tri_off(n) + (m + n);
                 const double2* x = X + n * n * NCOL;
+                double2 acc[NCM];
+#pragma unroll
+                for (int cc = 0; cc < NCM; ++cc) acc[cc] = make_double2(0.0, 0.0);
                 for (int j = 0; j < w; ++j) {
-                    const double2 t = __ldg(Tn + j * w);
+                    const double t = __ldg(Dn + j * w);
                     const double2* xj = x + j * NCOL;
 #pragma unroll
                     for (int cc = 0; cc < NCM; ++cc)
-                        if (cc < NCOL) cmacc(L[k][cc], t, xj[cc]);
+                        if (cc < NCOL) {
+                            acc[cc].x = fma(t, xj[cc].x, acc[cc].x);
+                            acc[cc].y = fma(t, xj[cc].y, acc[cc].y);
+                        }
                 }
+                const double2 z = __ldg(ph + m);
+#pragma unroll
+                for (int cc = 0; cc < NCM; ++cc)
+                    if (cc < NCOL) cmacc(L[k][cc], z, acc[cc]);
             }
         }
     }
@@ -282,8 +306,10 @@ void rot_m2l(hfmm_plan* P, int l, int R, int64_t fam_stride, cudaStream_t s) {
         LevelTables& T = P->tables[f][l];
         if (!T.rot_Q.p) throw Error{HFMM_ERR_STATE, "rotation M2L: level operators missing"};
         RotCall c{};
-        c.T = reinterpret_cast<const double2*>(P->rot_T.p);
-        c.Tt = c.T + (int64_t)N_DISP * ((Pn + 1) * (4 * (Pn + 1) * (Pn + 1) - 1) / 3);
+        c.D = P->rot_D.p;
+        c.Dt = c.D + (int64_t)P->rot_n_theta * ((Pn + 1) * (4 * (Pn + 1) * (Pn + 1) - 1) / 3);
+        c.theta = P->rot_theta.p;
+        c.phase = reinterpret_cast<const double2*>(P->rot_phase.p);
         c.dist = P->rot_dist.p;
         c.QT = reinterpret_cast<const double2*>(T.rot_Q.p);
         c.ET = reinterpret_cast<const double2*>(T.rot_E.p);
@@ -335,7 +361,8 @@ using namespace hfmm;
 
 extern "C" {
 
-int hfmm_plan_set_m2l_rotation(hfmm_plan* P, int32_t order, const double* T_host,
+int hfmm_plan_set_m2l_rotation(hfmm_plan* P, int32_t order, const double* D_host, int32_t n_theta,
+                               const int32_t* theta_host, const double* phase_host,
                                const int32_t* dist_host, int32_t n_dist) {
     if (!P) return fail(HFMM_ERR_ARG, "plan is NULL");
     if (order == 0) {   // back to the dense M2L tables
@@ -343,26 +370,34 @@ int hfmm_plan_set_m2l_rotation(hfmm_plan* P, int32_t order, const double* T_host
         return HFMM_OK;
     }
     if (order < 1 || order > 40) return fail(HFMM_ERR_ARG, "rotation order must be in [1, 40]");
-    if (!T_host || !dist_host || n_dist < 1) return fail(HFMM_ERR_ARG, "rotations and distances are required");
+    if (!D_host || n_theta < 1 || !theta_host || !phase_host || !dist_host || n_dist < 1)
+        return fail(HFMM_ERR_ARG, "rotations, phases and distances are required");
     try {
         const size_t TS = (size_t)(order + 1) * (4 * (order + 1) * (order + 1) - 1) / 3;
-        std::vector<int32_t> d(dist_host, dist_host + N_DISP);
-        for (int e = 0; e < N_DISP; ++e)
+        const size_t NZ = 2 * (size_t)order + 1;
+        std::vector<int32_t> d(dist_host, dist_host + N_DISP), th(theta_host, theta_host + N_DISP);
+        for (int e = 0; e < N_DISP; ++e) {
             if (d[e] >= n_dist) return fail(HFMM_ERR_ARG, "distance index out of range");
-        // the blocks as given, then each block transposed (T_n^T), complex as re, im pairs
-        std::vector<double> tt(N_DISP * TS * 2);
-        for (size_t e = 0; e < (size_t)N_DISP; ++e)
+            if (d[e] >= 0 && (th[e] < 0 || th[e] >= n_theta))   // every V slot needs its rotation
+                return fail(HFMM_ERR_ARG, "polar angle index out of range");
+        }
+        // the blocks as given, then each block transposed (D_n^T)
+        std::vector<double> dt((size_t)n_theta * TS);
+        for (size_t a = 0; a < (size_t)n_theta; ++a)
             for (int n = 0, off = 0; n <= order; off += (2 * n + 1) * (2 * n + 1), ++n) {
-                const size_t w = 2 * n + 1, b = e * TS + off;
-                for (size_t a = 0; a < w; ++a)
-                    for (size_t j = 0; j < w; ++j)
-                        for (int z = 0; z < 2; ++z)
-                            tt[(b + j * w + a) * 2 + z] = T_host[(b + a * w + j) * 2 + z];
+                const size_t w = 2 * n + 1, b = a * TS + off;
+                for (size_t i = 0; i < w; ++i)
+                    for (size_t j = 0; j < w; ++j) dt[b + j * w + i] = D_host[b + i * w + j];
             }
-        P->rot_T.alloc(2 * N_DISP * TS * 2);
-        HFMM_CUDA(cudaMemcpy(P->rot_T.p, T_host, N_DISP * TS * 2 * sizeof(double), cudaMemcpyHostToDevice));
-        HFMM_CUDA(cudaMemcpy(P->rot_T.p + N_DISP * TS * 2, tt.data(), N_DISP * TS * 2 * sizeof(double),
+        P->rot_D.alloc(2 * (size_t)n_theta * TS);
+        HFMM_CUDA(cudaMemcpy(P->rot_D.p, D_host, (size_t)n_theta * TS * sizeof(double), cudaMemcpyHostToDevice));
+        HFMM_CUDA(cudaMemcpy(P->rot_D.p + (size_t)n_theta * TS, dt.data(), (size_t)n_theta * TS * sizeof(double),
                              cudaMemcpyHostToDevice));
+        P->rot_theta.alloc(N_DISP);
+        HFMM_CUDA(cudaMemcpy(P->rot_theta.p, th.data(), N_DISP * sizeof(int32_t), cudaMemcpyHostToDevice));
+        P->rot_phase.alloc(N_DISP * NZ * 2);
+        HFMM_CUDA(cudaMemcpy(P->rot_phase.p, phase_host, N_DISP * NZ * 2 * sizeof(double), cudaMemcpyHostToDevice));
+        P->rot_n_theta = n_theta;
         P->rot_dist.alloc(N_DISP);
         HFMM_CUDA(cudaMemcpy(P->rot_dist.p, d.data(), N_DISP * sizeof(int32_t), cudaMemcpyHostToDevice));
         P->rot_P = order;

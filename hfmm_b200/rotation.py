@@ -25,9 +25,16 @@ The formula is pinned against numerical projection in tests/test_rotation_cpu.py
 Rotation blocks T_n[m, m''] = int Y_{nm''}(s) conj(Y_nm(R s)) d Omega are integrated
 exactly (Gauss-Legendre x uniform azimuth, enough points for degree 2P).
 
-Cost per V pair, family and charge column: two rotations of sum (2n+1)^2 and one
-coaxial shift of sum (P+1-|m|)^2 complex multiply-adds, O(P^3): at P = 20 about
-31,000, against n_s^2 = 87,616 multiply-adds of the dense p = 8 table. Accuracy is
+Each slot's rotation is R_y(-theta) R_z(-phi) (theta, phi the displacement's polar
+angle and azimuth), whose blocks factor as T_n = D_n(theta) diag(e^{i m phi}) with D_n
+real; the shift along z commutes with rotations about z, so this gives the same
+operator as any other rotation taking d to z. The 316 slots share the D tables of
+their distinct polar angles.
+
+Cost per V pair, family and charge column: two real rotations of sum (2n+1)^2 and one
+coaxial shift of sum (P+1-|m|)^2 real x complex multiply-adds plus the phases, O(P^3):
+at P = 20 about 30,900 (61,700 FMA), against n_s^2 = 87,616 multiply-adds of the dense
+p = 8 table. Accuracy is
 set by P: at p = 8 the nearest face displacement (2, 0, 0) converges slowest
 (relative 2.9e-6 at P = 20, 1.1e-6 at 24, 3.8e-7 at 28); the sin family is exact to
 rounding at any P used here.
@@ -42,8 +49,9 @@ from scipy.special import spherical_jn, spherical_yn
 
 from .operators import surface_pts, level_scale, R_EQUIV
 
-__all__ = ["gaunt", "rotation_blocks", "coaxial", "level_operators", "direction_blocks",
-           "n_coeff", "pack_rotations", "pack_coaxial", "enable", "disable"]
+__all__ = ["gaunt", "rotation_blocks", "coaxial", "level_operators", "direction_angles",
+           "slot_rotation", "packed_dmatrices", "pack_phases", "n_coeff", "pack_coaxial",
+           "enable", "disable"]
 
 
 def n_coeff(P):
@@ -187,30 +195,62 @@ def displacements():
     return np.array([(i // 49 - 3, (i // 7) % 7 - 3, i % 7 - 3) for i in range(343)], float)
 
 
-def direction_blocks(P):
-    """Rotation blocks of every non-adjacent slot (None for the others); the slot's
-    displacement d = target - source (the source's multipole is shifted by d)."""
-    out = []
-    for d in displacements():
-        out.append(rotation_blocks(P, rotation_to_z(d)) if np.abs(d).max() > 1 else None)
-    return out
+def _rot_y(b):
+    c, s = math.cos(b), math.sin(b)
+    return np.array([[c, 0.0, s], [0.0, 1.0, 0.0], [-s, 0.0, c]])
 
 
-def pack_rotations(P, blocks):
-    """[343][sum (2n+1)^2] complex128 as interleaved re, im (zeros for adjacent slots)."""
-    size = sum((2 * n + 1) ** 2 for n in range(P + 1))
-    out = np.zeros((343, size), np.complex128)
-    for e, T in enumerate(blocks):
-        if T is None:
+def _rot_z(a):
+    c, s = math.cos(a), math.sin(a)
+    return np.array([[c, -s, 0.0], [s, c, 0.0], [0.0, 0.0, 1.0]])
+
+
+def direction_angles():
+    """The rotation of each non-adjacent slot's displacement d = target - source onto z
+    as R_y(-theta) R_z(-phi) (polar angle theta, azimuth phi of d). Its blocks factor as
+    T_n = D_n(theta) diag(e^{i m phi}) with D_n real (a y-rotation), so the slots share
+    the D tables of their distinct polar angles. Returns (theta of each distinct polar
+    angle, each slot's theta index (-1: adjacent), each slot's phi)."""
+    d = displacements()
+    keys, theta = {}, []
+    tidx, phi = np.full(343, -1, np.int32), np.zeros(343)
+    for e in range(343):
+        dx, dy, dz = (int(v) for v in d[e])
+        if max(abs(dx), abs(dy), abs(dz)) <= 1:
             continue
-        out[e] = np.concatenate([t.ravel() for t in T])
-    return out
+        d2 = dx * dx + dy * dy + dz * dz
+        key = ((dz > 0) - (dz < 0), Fraction(dz * dz, d2))   # cos(theta) = dz / |d|
+        if key not in keys:
+            keys[key] = len(theta)
+            theta.append(math.acos(dz / math.sqrt(d2)))
+        tidx[e] = keys[key]
+        phi[e] = math.atan2(dy, dx)
+    return np.array(theta), tidx, phi
+
+
+def slot_rotation(e, P):
+    """The blocks T_n of slot e from its factors (what the device applies)."""
+    theta, tidx, phi = direction_angles()
+    D = rotation_blocks(P, _rot_y(-theta[tidx[e]]))
+    return [D[n].real * np.exp(1j * np.arange(-n, n + 1) * phi[e])[None, :] for n in range(P + 1)]
 
 
 @lru_cache(maxsize=4)
-def _packed_rotations(P):
-    """pack_rotations of direction_blocks(P), kept per order (it depends on nothing else)."""
-    return np.ascontiguousarray(pack_rotations(P, direction_blocks(P)))
+def packed_dmatrices(P):
+    """[n_theta][sum (2n+1)^2] real: D_n(theta) of every distinct polar angle, each block
+    row-major [m][m'']."""
+    theta, _, _ = direction_angles()
+    return np.ascontiguousarray(np.stack([np.concatenate([t.real.ravel() for t in
+                                                          rotation_blocks(P, _rot_y(-th))])
+                                          for th in theta]))
+
+
+def pack_phases(P):
+    """[343][2P+1] complex: e^{i m phi} of each slot, m = -P..P (zeros for adjacent slots)."""
+    _, tidx, phi = direction_angles()
+    out = np.exp(1j * np.outer(phi, np.arange(-P, P + 1)))
+    out[tidx < 0] = 0.0
+    return np.ascontiguousarray(out)
 
 
 def distances():
@@ -283,10 +323,14 @@ def enable(state, order):
                                  f"{state.k * 2 * level_scale(extent, level):.3g}): use a lower "
                                  f"order or the dense tables")
             levels.append((fam, level, Q, E, C, pref))
-    T = _packed_rotations(P)
+    D = packed_dmatrices(P)
+    _, tidx, _ = direction_angles()
+    tidx = np.ascontiguousarray(tidx, np.int32)
+    Z = pack_phases(P)
     uniq, slot = distances()
     slot = np.ascontiguousarray(slot, np.int32)
-    check(_lib.lib.hfmm_plan_set_m2l_rotation(state.handle, P, T.ctypes.data, slot.ctypes.data,
+    check(_lib.lib.hfmm_plan_set_m2l_rotation(state.handle, P, D.ctypes.data, D.shape[0],
+                                               tidx.ctypes.data, Z.ctypes.data, slot.ctypes.data,
                                                len(uniq)))
     for fam, level, Q, E, C, pref in levels:
         check(_lib.lib.hfmm_plan_set_rotation_level(state.handle, fam, level, Q.ctypes.data,
@@ -298,5 +342,5 @@ def disable(state):
     """Back to the dense M2L tables."""
     from . import _lib
     from ._lib import check
-    check(_lib.lib.hfmm_plan_set_m2l_rotation(state.handle, 0, None, None, 0))
+    check(_lib.lib.hfmm_plan_set_m2l_rotation(state.handle, 0, None, 0, None, None, None, 0))
     state.rotation_order = 0

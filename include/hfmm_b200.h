@@ -321,18 +321,21 @@ int hfmm_plan_set_m2l_queue(hfmm_plan* plan, int32_t on);
  * kernels/laplace/transf.py:143-250; its Helmholtz path uses KIFMM tables,
  * kifmm/phases.py:176-237): per V pair, the source box's multipole coefficients of
  * order `order` are rotated into the frame whose z axis is the displacement, shifted
- * along z and rotated back, O(order^3). T_host: [343][sum_{n<=order} (2n+1)^2] complex
- * (re, im interleaved) rotation blocks per displacement slot ((dx+3)*49 + (dy+3)*7 +
- * (dz+3)), zero for adjacent slots; dist_host[343]: each slot's coaxial matrix index
- * (-1 adjacent), n_dist of them. order 0 returns to the dense M2L tables. Then, per
- * family and level, hfmm_plan_set_rotation_level with Q [(order+1)^2][n_s] complex
- * (multipole from equivalent density), E [n_s][(order+1)^2] complex (check potential
- * from local coefficients, times pref, real part) and C [n_dist][2 order+1][order+1]
- * [order+1] real (the coaxial shifts: C[d][m + order][n'][n] takes multipole (n, m) to
- * local (n', m)). The library keeps its own transposed copies. hfmm_b200/rotation.py
- * builds all of them. Only the FP64 evaluate uses it; after hfmm_plan_rebuild set it
- * again. */
-int hfmm_plan_set_m2l_rotation(hfmm_plan* plan, int32_t order, const double* T_host,
+ * along z and rotated back, O(order^3). A displacement slot's ((dx+3)*49 + (dy+3)*7 +
+ * (dz+3)) rotation R_y(-theta) R_z(-phi) has blocks T_n = D_n(theta) diag(e^{i m phi}):
+ * D_host [n_theta][sum_{n<=order} (2n+1)^2] real holds D_n, row-major per block, for
+ * each distinct polar angle; theta_host[343] each slot's angle index (-1 adjacent);
+ * phase_host [343][2 order+1] complex (re, im interleaved) e^{i m phi}, m = -order..order;
+ * dist_host[343] each slot's coaxial matrix index (-1 adjacent), n_dist of them. order 0
+ * returns to the dense M2L tables. Then, per family and level,
+ * hfmm_plan_set_rotation_level with Q [(order+1)^2][n_s] complex (multipole from
+ * equivalent density), E [n_s][(order+1)^2] complex (check potential from local
+ * coefficients, times pref, real part) and C [n_dist][2 order+1][order+1][order+1] real
+ * (the coaxial shifts: C[d][m + order][n'][n] takes multipole (n, m) to local (n', m)).
+ * The library keeps its own transposed copies. hfmm_b200/rotation.py builds all of
+ * them. Only the FP64 evaluate uses it; after hfmm_plan_rebuild set it again. */
+int hfmm_plan_set_m2l_rotation(hfmm_plan* plan, int32_t order, const double* D_host, int32_t n_theta,
+                               const int32_t* theta_host, const double* phase_host,
                                const int32_t* dist_host, int32_t n_dist);
 int hfmm_plan_set_rotation_level(hfmm_plan* plan, int32_t family, int32_t level, const double* Q_host,
                                  const double* E_host, const double* C_host, double pref);

@@ -61,7 +61,7 @@ def test_rotation_refuses_other_kernels_and_bad_orders():
     st.close()
     st = hfmm_b200.setup(pos, 3.0, p=4, N_max=32)
     with pytest.raises(ValueError):
-        _lib.check(_lib.lib.hfmm_plan_set_m2l_rotation(st.handle, 41, None, None, 0))
+        _lib.check(_lib.lib.hfmm_plan_set_m2l_rotation(st.handle, 41, None, 0, None, None, None, 0))
     with pytest.raises(hfmm_b200.HFMMError):   # level operators before the order
         _lib.check(_lib.lib.hfmm_plan_set_rotation_level(st.handle, 0, 2, None, None, None, 1.0))
     st.close()

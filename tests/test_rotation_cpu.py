@@ -71,6 +71,28 @@ def test_rotation_blocks_are_unitary_and_rotate():
     assert np.allclose(f, g, atol=1e-12)
 
 
+def test_slot_rotations_factor_into_real_y_rotations_and_phases():
+    """Every V slot: R_y(-theta) R_z(-phi) takes the displacement to z, and its blocks
+    are D_n(theta) diag(e^{i m phi}) with D_n real, the tables the device reads."""
+    P = 5
+    theta, tidx, phi = rot.direction_angles()
+    D, Z = rot.packed_dmatrices(P), rot.pack_phases(P)
+    d = rot.displacements()
+    far = np.abs(d).max(1) > 1
+    assert (tidx[far] >= 0).all() and (tidx[~far] == -1).all() and len(theta) < 61
+    for e in np.nonzero(far)[0]:
+        R = rot._rot_y(-theta[tidx[e]]) @ rot._rot_z(-phi[e])
+        assert np.allclose(R @ d[e] / np.linalg.norm(d[e]), [0, 0, 1], atol=1e-14)
+        full, sr = rot.rotation_blocks(P, R), rot.slot_rotation(e, P)
+        off = 0
+        for n in range(P + 1):
+            w = 2 * n + 1
+            Dn = D[tidx[e], off:off + w * w].reshape(w, w)
+            off += w * w
+            assert np.abs(Dn * Z[e, P - n:P + n + 1][None, :] - full[n]).max() < 1e-13
+            assert np.abs(sr[n] - full[n]).max() < 1e-13
+
+
 def _apply(P, Q, E, pref, T, C, x):
     M = Q @ x
     Mb = np.concatenate([T[n] @ M[n * n:(n + 1) ** 2] for n in range(P + 1)])
@@ -95,7 +117,7 @@ def test_rotation_m2l_matches_the_dense_kifmm_operator(imag):
     x = np.random.default_rng(1).normal(size=eq.shape[0])
     for d, bar in (((3, 1, 0), 1e-8), ((2, 2, 2), 1e-8), ((2, 0, 0), 1e-4)):
         dv = 2 * s * np.array(d, float)
-        T = rot.rotation_blocks(P, rot.rotation_to_z(dv))
+        T = rot.slot_rotation((d[0] + 3) * 49 + (d[1] + 3) * 7 + d[2] + 3, P)   # D_n diag(phase)
         C = rot.coaxial(P, k, np.linalg.norm(dv), imag)
         y = _apply(P, Q, E, pref, T, C, x)
         ref = O.family_matrix(k, imag)(eq + dv, eq) @ x
@@ -117,3 +139,11 @@ def test_enable_refuses_before_touching_the_plan():
     with pytest.raises(ValueError, match="overflows"):   # y_80(k 4 s) at k = 0.05
         rot.enable(SimpleNamespace(**{**vars(st), "k": 0.05}), 40)
     assert not hasattr(st, "rotation_order")
+
+
+def test_disable_goes_through_the_library_signature():
+    """disable() reaches the C entry point with its full argument list; a NULL plan is
+    refused there before anything touches a device."""
+    from types import SimpleNamespace
+    with pytest.raises(ValueError, match="plan is NULL"):   # HFMM_ERR_ARG
+        rot.disable(SimpleNamespace(handle=None))
