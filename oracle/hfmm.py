@@ -154,7 +154,8 @@ def kifmm_setup(positions, p, N_max, max_depth, kernel, eps_rel=1e-7):
         X = Xn if Xn.shape[0] else None
     dc = near_pairs(U, lvls, is_leaf)
     _, pil = assign_particles(t["sort_idx"], m_id, lvls, counts, is_leaf, md, maxleaf)
-    ops = build_operators_leveled(p, md, float(t["domain_extent"]), kernel.G_np, eps_rel)
+    ops = build_operators_leveled(p, md, float(t["domain_extent"]), kernel.G_np, eps_rel,
+                                  m2l_from_level=2)   # V pairs start at level 2
     return dict(positions=x, pil=pil, dir_cnct=dc, V=V, U=U, W=W, X=X, m_id=m_id, p_id=p_id,
                 lvls=lvls, counts=counts, is_leaf=is_leaf, sort_idx=t["sort_idx"],
                 domain_extent=float(t["domain_extent"]), pmin=t["pmin"], ops=ops,
@@ -177,7 +178,7 @@ def setup(positions, k, p=4, N_max=16, max_depth=None):
         return real, None
     ki = HelmholtzComponent(k, True)
     imag_ops = build_operators_leveled(int(p), real["max_depth"], float(real["domain_extent"]),
-                                       ki.G_np, eps_rel=1e-12)
+                                       ki.G_np, eps_rel=1e-12, m2l_from_level=2)
     return real, dict(real, ops=imag_ops, kernel=ki)
 
 

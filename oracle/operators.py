@@ -49,13 +49,13 @@ def pinv_factors(A, eps_rel=1e-7):
     return U, s / (s * s + eps * eps), Vt
 
 
-def build_operators(p, G, eps_rel=1e-7, m2l_out=None):
+def build_operators(p, G, eps_rel=1e-7, m2l_out=None, with_m2l=True):
     """Unit-box operator set for kernel matrix function ``G`` (operators.py:330-403).
 
     Returns the members the leveled path uses. ``M2L_K_table`` has shape
     (343, n_s, n_s) in displacement order ``(dx+3)*49 + (dy+3)*7 + (dz+3)`` with
     zero matrices at the 27 adjacent displacements; ``m2l_out``, if given, is the
-    zeroed array it is written into.
+    zeroed array it is written into; ``with_m2l=False`` leaves it zero.
     """
     equiv = surface_pts(p, R_EQUIV)
     check = surface_pts(p, R_CHECK)
@@ -67,7 +67,7 @@ def build_operators(p, G, eps_rel=1e-7, m2l_out=None):
     for c in range(8):
         M2M_K[c] = G(parent_check, equiv + CHILD_OFFSETS[c])
     M2L = np.zeros((343, n_s, n_s)) if m2l_out is None else m2l_out
-    for dxi in range(7):
+    for dxi in range(7 if with_m2l else 0):
         for dyi in range(7):
             for dzi in range(7):
                 dx, dy, dz = dxi - 3, dyi - 3, dzi - 3
@@ -83,11 +83,13 @@ def build_operators(p, G, eps_rel=1e-7, m2l_out=None):
                 equiv_pts=equiv, check_pts=check, n_s=n_s, p=p)
 
 
-def build_operators_leveled(p, max_depth, domain_extent, G, eps_rel=1e-7):
+def build_operators_leveled(p, max_depth, domain_extent, G, eps_rel=1e-7, m2l_from_level=0):
     """Per-level tables (operators.py:572-641).
 
     ``M2M_K_lv[pl]`` (parent level pl) and ``L2L_K_lv[cl-1]`` (child level cl) are
-    both taken from the CHILD level's assembly, as in the reference.
+    both taken from the CHILD level's assembly, as in the reference. M2L tables of the
+    levels below ``m2l_from_level`` are left zero: ``setup`` passes 2, the first level
+    with V pairs; the reference builds them and never reads them.
     """
     n_s = surface_pts(p, R_EQUIV).shape[0]
     m2l = np.zeros((max_depth + 1, 343, n_s, n_s))   # filled in place, level by level
@@ -95,7 +97,7 @@ def build_operators_leveled(p, max_depth, domain_extent, G, eps_rel=1e-7):
     for l in range(max_depth + 1):
         s = float(domain_extent) * 0.5 ** (l + 1)
         Gs = (lambda x, y, _s=s: G(x * _s, y * _s))
-        per.append(build_operators(p, Gs, eps_rel, m2l_out=m2l[l]))
+        per.append(build_operators(p, Gs, eps_rel, m2l_out=m2l[l], with_m2l=l >= m2l_from_level))
 
     def stack_f(key):
         return tuple(np.stack([np.asarray(o[key][i]) for o in per]) for i in range(3))
