@@ -18,6 +18,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <exception>
 #include <memory>
 #include <mutex>
 
@@ -394,11 +395,35 @@ struct CritStream {
 };
 }  // namespace
 
+// On an error part-way through an evaluate, the side streams may still run work that
+// was enqueued before it (the near field writes the outputs, the compressed M2Ls the
+// local expansions). While the exception unwinds, the far-field stream waits for all
+// of it, and CritStream's join then carries that wait to the caller's stream: no
+// kernel of the call outlives its error return on the caller's stream.
+struct SideJoin {
+    hfmm_plan* P;
+    cudaStream_t s;
+    int unwinding;
+    SideJoin(hfmm_plan* p, cudaStream_t st) : P(p), s(st), unwinding(std::uncaught_exceptions()) {}
+    ~SideJoin() {
+        if (std::uncaught_exceptions() <= unwinding) return;
+        auto join = [&](cudaStream_t side, cudaEvent_t ev) {
+            if (side && ev && side != s && cudaEventRecord(ev, side) == cudaSuccess)
+                cudaStreamWaitEvent(s, ev, 0);
+        };
+        join(P->nf_side, P->nf_join);
+        for (int k = 0; k < hfmm_plan::CX_STREAMS; ++k) join(P->cx_side[k], P->cx_join[k]);
+    }
+};
+
 void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double* phi, double* E,
                    cudaStream_t s_caller, bool mixed, int phase) {
+    const bool up = phase & EVAL_UP, down = phase & EVAL_DOWN;
+    if (down && P->rot_P > 0 && !(mixed && P->mixed_ready))
+        rot_check(P);   // before anything is enqueued
     CritStream crit(P, s_caller);
     cudaStream_t s = crit.s;
-    const bool up = phase & EVAL_UP, down = phase & EVAL_DOWN;
+    SideJoin side_join(P, s);   // destroyed before crit: the sides join s, then s the caller
     const int R = q_im ? 2 : 1;
     const int NF = P->n_fam;
     const bool field = E != nullptr;

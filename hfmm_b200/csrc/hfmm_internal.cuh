@@ -300,6 +300,7 @@ void gemm_f64(const GemmCall& c, int* d_err, cudaStream_t s);
 int sm_count();   // multiprocessors of the current device (read once)
 // rotation-based M2L of level l into the check potentials (m2l_rotation.cu)
 void rot_m2l(hfmm_plan* P, int l, int R, int64_t fam_stride, cudaStream_t s);
+void rot_check(const hfmm_plan* P);   // throws when the rotation M2L cannot run
 size_t rot_workspace_doubles(const hfmm_plan* P);
 constexpr int64_t GEMM_PART_CAP = 768LL * 64 * 64;   // doubles: 768 partial 64 x 64 tiles
 

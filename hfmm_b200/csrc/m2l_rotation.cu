@@ -294,10 +294,17 @@ size_t rot_workspace_doubles(const hfmm_plan* P) {
     return (size_t)widest * 2 * (P->rot_P + 1) * (P->rot_P + 1) * 2;
 }
 
-void rot_m2l(hfmm_plan* P, int l, int R, int64_t fam_stride, cudaStream_t s) {
-    const int Pn = P->rot_P, NC = (Pn + 1) * (Pn + 1);
+void rot_check(const hfmm_plan* P) {
     if (P->rot_M.n < rot_workspace_doubles(P))   // a rebuilt tree with a wider level
         throw Error{HFMM_ERR_STATE, "rotation M2L: set the rotation again after the plan was rebuilt"};
+    for (int f = 0; f < P->n_fam; ++f)
+        for (int l = 2; l <= P->md; ++l)
+            if (!P->tables[f][l].rot_Q.p) throw Error{HFMM_ERR_STATE, "rotation M2L: level operators missing"};
+}
+
+void rot_m2l(hfmm_plan* P, int l, int R, int64_t fam_stride, cudaStream_t s) {
+    const int Pn = P->rot_P, NC = (Pn + 1) * (Pn + 1);
+    rot_check(P);
     // rows per thread, then targets per CTA: the columns a thread's registers hold
     const int rows = (int)ceil_div(NC, ROT_THREADS);
     const int TT = rows <= ROT_MAXROWS ? std::min(std::min(ROT_MAXCOL, 12), ROT_MAXI / rows) / R : 0;
