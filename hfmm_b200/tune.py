@@ -131,7 +131,7 @@ def tune_leaf(positions, k, charges, p=8, candidates=(32, 64, 128), rel_slack=1.
     idx = np.sort(np.random.default_rng(0).choice(pos.shape[0], min(n_ref, pos.shape[0]),
                                                   replace=False))
     ref, results, states, report = None, [], {}, []
-    for nm in (int(c) for c in candidates):
+    for nm in dict.fromkeys(int(c) for c in candidates):   # each leaf size once, in order
         st = None
         try:
             st = setup(pos, k, p=p, N_max=nm, **setup_kw)
