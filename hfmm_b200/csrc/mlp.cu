@@ -3,7 +3,7 @@
 // (k x box size per level, box and leaf-occupancy statistics of the tree, the
 // requested tolerance) to the expansion order p and the depth offset. No
 // counterpart in the reference, which takes p and the leaf size from the caller
-// (HFMM.py:55-80); the judge of its choice is the direct-sum check of
+// (HFMM.py:55-80); its choice is checked against the direct sum of
 // test.py:11-18.
 //
 // Parameters, one flat FP32 array (row-major, input index first):
