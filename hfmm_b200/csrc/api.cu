@@ -298,7 +298,7 @@ MixedCall cx_call(hfmm_plan* P, int l, int f, int R) {
     mc.out_fam_stride = 0;
     mc.nb = P->nb;
     mc.err = P->d_err.p;
-    if (R == 2 && T.grid && g_m2l_grid) {   // sources from the dense grid by TMA
+    if (R == 2 && T.grid && g_m2l_grid.load()) {   // sources from the dense grid by TMA
         mc.grid = 1;
         mc.tile_tgt = P->gx_tiles[l].tgt.p;
         mc.ntiles = P->gx_tiles[l].ntiles;
@@ -620,7 +620,7 @@ void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double*
                 gemm_1(K_CMP, l, f, P->equiv.p + f * fs, P->ld, level_base(T.xc.p, l, T.ckld), T.ckld,
                        s);
                 const int64_t nbl = P->level_hi[l] - P->level_lo[l];
-                if (R == 2 && T.grid && g_m2l_grid)   // complete level: into the dense grid
+                if (R == 2 && T.grid && g_m2l_grid.load())   // complete level: into the dense grid
                     split_tf32_grid(T.xc.p, P->m_id.p + P->level_lo[l], nbl, T.grid, T.ckld,
                                     T.xg_hi.p, T.xg_lo.p, s);
                 else
@@ -645,13 +645,13 @@ void evaluate_fp64(hfmm_plan* P, const double* q_re, const double* q_im, double*
     // The plan's own queued M2L (every level and family in one persistent launch, the
     // largest items first) in place of the per-level launches on side streams; the test
     // switches of the M2L kernels (grid mode off) take the per-level path.
-    PlanQueue* pq = (up && use_cx && g_m2l_grid && P->queue_m2l) ? static_cast<PlanQueue*>(P->cxq[R - 1])
+    PlanQueue* pq = (up && use_cx && g_m2l_grid.load() && P->queue_m2l) ? static_cast<PlanQueue*>(P->cxq[R - 1])
                                                                  : nullptr;
     if (pq) {
         {
             PhaseTimer pt(X, s, 4);
             m2l_queue(pq->calls.p, pq->maps.p, pq->items.p, pq->n_items, pq->next.p, R, sm_count(), s,
-                      g_m2l_starve);
+                      g_m2l_starve.load());
         }
         for (int l = 2; l <= P->md; ++l)
             for (int f = 0; f < NF; ++f) {

@@ -339,7 +339,7 @@ int hfmm_batch_capture(hfmm_batch* B) {
                 int sms = 148;
                 HFMM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, B->device));
                 m2l_queue(B->q_calls.p, B->q_maps.p, B->q_items.p, B->n_items, B->q_next.p, B->queue_R,
-                          sms, s0, g_m2l_starve);
+                          sms, s0, g_m2l_starve.load());
                 HFMM_CUDA(cudaEventRecord(B->events[0], s0));
                 for (int s = 1; s < S; ++s) HFMM_CUDA(cudaStreamWaitEvent(B->streams[s], B->events[0], 0));
             }

@@ -439,11 +439,11 @@ void m2l_queue(const MixedCall* calls, const MixedMaps* maps, const M2LItem* ite
     HFMM_CUDA(cudaMemsetAsync(next, 0, sizeof(int), s));
     if (R == 1) {
         HFMM_CUDA(cudaFuncSetAttribute(k_m2l_queue<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        HFMM_LAUNCH(k_m2l_queue<1>, grid, THREADS, smem, s, calls, maps, items, n_items, next, g_m2l_wait_ns,
+        HFMM_LAUNCH(k_m2l_queue<1>, grid, THREADS, smem, s, calls, maps, items, n_items, next, g_m2l_wait_ns.load(),
                     starve);
     } else {
         HFMM_CUDA(cudaFuncSetAttribute(k_m2l_queue<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        HFMM_LAUNCH(k_m2l_queue<2>, grid, THREADS, smem, s, calls, maps, items, n_items, next, g_m2l_wait_ns,
+        HFMM_LAUNCH(k_m2l_queue<2>, grid, THREADS, smem, s, calls, maps, items, n_items, next, g_m2l_wait_ns.load(),
                     starve);
     }
 }

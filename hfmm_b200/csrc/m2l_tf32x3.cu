@@ -547,17 +547,17 @@ void check_register_split() {
         throw Error{HFMM_ERR_STATE, "m2l_tf32x3: the warp roles' register split exceeds the launch's registers"};
 }
 
-uint64_t g_m2l_wait_ns = 0;
-int g_m2l_grid = 1;
-int g_m2l_starve = 0;
+std::atomic<uint64_t> g_m2l_wait_ns{0};
+std::atomic<int> g_m2l_grid{1};
+std::atomic<int> g_m2l_starve{0};
 
 size_t m2l_tf32x3_smem() { return (size_t)STAGES * STAGE_BYTES + sizeof(Ctl) + 1024; }
 
 void m2l_tf32x3(const MixedMaps& maps, const MixedCall& call, cudaStream_t s) {
     if (call.ntiles == 0) return;
     MixedCall c = call;
-    c.wait_ns = g_m2l_wait_ns;
-    c.starve = g_m2l_starve;
+    c.wait_ns = g_m2l_wait_ns.load();
+    c.starve = g_m2l_starve.load();
     if (!c.ldk) c.ldk = c.ld;
     if (!c.ldm) c.ldm = c.ld;
     if (c.ldk % BK || c.ldm % BK)

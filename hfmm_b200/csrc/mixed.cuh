@@ -4,6 +4,8 @@
 
 #include <cuda.h>
 
+#include <atomic>
+
 #include <string>
 #include <vector>
 
@@ -44,9 +46,10 @@ struct MixedCall {
 };
 
 // Wait limit and starvation switch of the next M2L launches (hfmm_debug_m2l_wait):
-// a test makes a bounded wait run out on purpose and checks the error status.
-extern uint64_t g_m2l_wait_ns;
-extern int g_m2l_starve;
+// a test makes a bounded wait run out on purpose and checks the error status. Atomic:
+// a hook call may come from another thread than the evaluate that reads it.
+extern std::atomic<uint64_t> g_m2l_wait_ns;
+extern std::atomic<int> g_m2l_starve;
 
 void make_table_map(CUtensorMap* map, const float* base, int ld, int count, int ldm = 0);
 void split_tf32(const double* src, float* hi, float* lo, int64_t n, cudaStream_t s);
@@ -56,7 +59,7 @@ void split_tf32_grid(const double* src, const uint64_t* m_id, int64_t n_boxes, i
                      float* hi, float* lo, cudaStream_t s);
 void make_grid_map(CUtensorMap* map, const float* base, int ckld, int G);
 // process-wide: 1 (default) lets complete levels use grid mode, 0 forces the gather
-extern int g_m2l_grid;
+extern std::atomic<int> g_m2l_grid;
 void split_transpose_tables(const double* at, float* hi, float* lo, int ld, int count);
 void m2l_tf32x3(const MixedMaps& maps, const MixedCall& c, cudaStream_t s);
 
