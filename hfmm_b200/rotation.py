@@ -71,24 +71,35 @@ def _fact(n):
 
 @lru_cache(maxsize=None)
 def wigner_3j(j1, j2, j3, m1, m2, m3):
-    """The Wigner 3j symbol by the Racah formula in exact integer arithmetic."""
+    """The Wigner 3j symbol by the Racah formula in exact integer arithmetic: the
+    alternating sum over k of 1 / prod(a_i!) is formed over the common denominator
+    prod(max_k a_i)! (each a_i is linear in k), and the square of the result is
+    rounded to a double once."""
     if m1 + m2 + m3 != 0 or j3 < abs(j1 - j2) or j3 > j1 + j2:
         return 0.0
     if abs(m1) > j1 or abs(m2) > j2 or abs(m3) > j3:
         return 0.0
     f = _fact
-    tri = Fraction(f(j1 + j2 - j3) * f(j1 - j2 + j3) * f(-j1 + j2 + j3), f(j1 + j2 + j3 + 1))
-    pre = tri * f(j1 + m1) * f(j1 - m1) * f(j2 + m2) * f(j2 - m2) * f(j3 + m3) * f(j3 - m3)
-    s = Fraction(0)
+    pre_num = (f(j1 + j2 - j3) * f(j1 - j2 + j3) * f(-j1 + j2 + j3)
+               * f(j1 + m1) * f(j1 - m1) * f(j2 + m2) * f(j2 - m2) * f(j3 + m3) * f(j3 - m3))
+    pre_den = f(j1 + j2 + j3 + 1)
+    terms = []
     for k in range(0, j1 + j2 + j3 + 1):
         a = (k, j3 - j2 + k + m1, j3 - j1 + k - m2, j1 + j2 - j3 - k, j1 - k - m1, j2 - k + m2)
-        if min(a) < 0:
-            continue
-        s += Fraction((-1) ** k, f(a[0]) * f(a[1]) * f(a[2]) * f(a[3]) * f(a[4]) * f(a[5]))
+        if min(a) >= 0:
+            terms.append((k, a))
+    den = 1
+    for i in range(6):
+        den *= f(max(a[i] for _, a in terms))
+    num = 0
+    for k, a in terms:
+        d = f(a[0]) * f(a[1]) * f(a[2]) * f(a[3]) * f(a[4]) * f(a[5])
+        num += (den // d) if k % 2 == 0 else -(den // d)
     sign = -1.0 if (j1 - j2 - m3) % 2 else 1.0
-    # sqrt(pre) * s with pre, s exact: the product's square is exact, its sign is s's
-    val = math.sqrt(pre * s * s)
-    return sign * (val if s >= 0 else -val)
+    # sqrt(pre) * s: the square pre s^2 = pre_num num^2 / (pre_den den^2) is exact and
+    # Python's integer division rounds it correctly; the sign is num's
+    val = math.sqrt((pre_num * num * num) / (pre_den * den * den))
+    return sign * (val if num >= 0 else -val)
 
 
 def gaunt(l1, m1, l2, m2, l3, m3):
@@ -103,7 +114,7 @@ def gaunt(l1, m1, l2, m2, l3, m3):
 def _coax_table(P):
     """W[m + P, n', n, nu] = 4 pi i^(n'+nu-n) G(n' m; nu 0; n m) sqrt((2 nu+1)/(4 pi)) (real)."""
     W = np.zeros((2 * P + 1, P + 1, P + 1, 2 * P + 1))
-    for m in range(-P, P + 1):
+    for m in range(0, P + 1):   # the coefficients of -m equal those of m (n' + nu + n even)
         for n2 in range(abs(m), P + 1):
             for n in range(abs(m), P + 1):
                 for nu in range(abs(n - n2), n + n2 + 1, 2):
@@ -113,6 +124,7 @@ def _coax_table(P):
                     e = (n2 + nu - n) % 4   # i^e: 0 -> 1, 2 -> -1 (odd e has g = 0)
                     W[m + P, n2, n, nu] = (1.0 if e == 0 else -1.0) * 4 * math.pi * g * \
                         math.sqrt((2 * nu + 1) / (4 * math.pi))
+    W[:P] = W[:P:-1]
     return W
 
 
