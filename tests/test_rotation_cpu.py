@@ -37,6 +37,25 @@ def test_coaxial_coefficients_match_projection(regular):
         assert abs(C[m + P, n2, n] - num) <= 1e-11 * max(1.0, abs(num)), (n, m, n2)
 
 
+def test_wigner_3j_known_values_and_orthogonality():
+    """Tabulated symbols ((j j 0; m -m 0) = (-1)^(j-m) / sqrt(2j+1) and two (j1 j2 j3; 0 0 0))
+    and the orthogonality sum over m1, m2 of products with equal (j1, j2)."""
+    w = rot.wigner_3j
+    for j in range(6):
+        for m in range(-j, j + 1):
+            assert abs(w(j, j, 0, m, -m, 0) - (-1) ** (j - m) / np.sqrt(2 * j + 1)) < 1e-15
+    assert abs(w(1, 1, 2, 0, 0, 0) - np.sqrt(2 / 15)) < 1e-15
+    assert abs(w(2, 2, 2, 0, 0, 0) + np.sqrt(2 / 35)) < 1e-15
+    assert w(1, 1, 1, 0, 0, 0) == 0.0 and w(2, 3, 7, 0, 0, 0) == 0.0   # parity, triangle
+    for j1, j2 in ((3, 5), (7, 4), (12, 9)):
+        for j3 in range(abs(j1 - j2), j1 + j2 + 1):
+            for j3b in (j3, min(j3 + 1, j1 + j2)):
+                m3 = min(j3, j3b) // 2
+                tot = sum(w(j1, j2, j3, m1, -m1 - m3, m3) * w(j1, j2, j3b, m1, -m1 - m3, m3)
+                          for m1 in range(-j1, j1 + 1) if abs(m1 + m3) <= j2)
+                assert abs(tot - (j3 == j3b) / (2 * j3 + 1)) < 1e-14, (j1, j2, j3, j3b)
+
+
 @pytest.mark.parametrize("P", [0, 1, 7, 24, 40])
 def test_harmonics_recurrence_matches_scipy(P):
     rng = np.random.default_rng(P)
