@@ -31,6 +31,7 @@ is timed on a bounded, phase-by-phase sample of the same workload and scaled by
 the exact work counts of the full problem (see ``oracle_estimate``).
 """
 import argparse
+import importlib.util
 import json
 import os
 import subprocess
@@ -1032,7 +1033,9 @@ def run_reference(a, cfg, rank, world):
             "e2e": {"value": v, "unit": "points/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0},
             "note": "reference JAX not installable offline; its NumPy restatement (the oracle) "
-                    "timed instead"}
+                    "timed instead",
+            # the probe behind the note, on the host this arm ran on
+            "jax_importable": importlib.util.find_spec("jax") is not None}
 
 
 def main():
