@@ -55,3 +55,31 @@ def test_near_field_with_and_without_padding_cut():
         cut = O.hfmm.eval_direct(s, s["kernel"], ppts, pchg, rev, field)
         full = O.hfmm.eval_direct(dict(s, near_trim=False), s["kernel"], ppts, pchg, rev, field)
         assert O.relative_error(cut, full) < 1e-14
+
+
+def test_clock_sampler_summary_from_nvidia_smi_rows():
+    """The clocks record of the JSON line from nvidia-smi rows (index, sm, max sm,
+    power, active reasons, then the four reason columns): median SM clock, highest
+    max, the reasons seen active, malformed rows skipped."""
+    import bench
+
+    class _Proc:
+        def terminate(self): pass
+        def wait(self, timeout=None): return 0
+        def kill(self): pass
+
+    class _Thread:
+        def join(self, timeout=None): pass
+
+    cs = bench.ClockSampler(0)
+    cs.proc, cs.t = _Proc(), _Thread()
+    row = lambda sm, pc: ["0", str(sm), "1965", "900.1", "0x0", "Not Active", "Not Active",
+                          "Not Active", pc]
+    cs.rows = [row(1965, "Not Active"), row(1890, "Active"), row(1965, "Not Active"),
+               ["garbage"], ["0", "[N/A]", "1965", "1", "x", "Not Active", "Not Active",
+                             "Not Active", "Not Active"]]
+    out = cs.stop()
+    assert out["sm_mhz"] == 1965.0 and out["sm_max_mhz"] == 1965.0
+    assert out["reasons"] == ["sw_power_cap"] and out["samples"] == 5
+    cs2 = bench.ClockSampler(0)
+    assert cs2.stop() is None            # never started
